@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 form-factor path (one JSON line on rank 0).
+
+Workload (the closed enclosure): an inward icosphere of 20 480 FP32 triangles
+(subdivision 5, radius 1) holding two perpendicular 1x1 plates of 20x20 cells
+(800 triangles each), N = 22 080 faces, 1000 front-side Malley rays per face
+(R = 22 080 000 rays per step), per-(source face, hit face) uint32 counts in
+an N x N matrix (1.95 GB) resident on the device.  Synthetic and seeded; each
+step draws fresh rays (Philox epoch = step index).
+
+A step is one ffb_form_factor_counts call: zero the count matrix, fused
+emission + grid trace + shared-memory histogram + flush.  The 1.95 GB zeroing
+writes more than the 126 MB L2 every step, so no step starts with the previous
+step's lines in L2.
+
+  value  rays/s with the scene, grid and matrix resident (CUDA events on the
+         context stream around K steps, max over ranks)
+  e2e    rays/s through the C ABI with host buffers: host ray counts in, the
+         count matrix copied to pinned host memory every step
+  --impl reference  the reference's own CPU path (zgrid_cpu caster + malley_cpu
+         emission, compiled from its sources into oracle/_ref) on a bounded
+         sample of the same workload, all host cores
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = ("enclosure: inward icosphere s5 (20480 tri) + 2 perpendicular 20x20 plates (1600 tri), "
+            "N=22080, 1000 front rays/face, N^2 uint32 counts")
+METRIC = "rays/s"
+FLOPS_PER_TEST = 42  # math/triangle.cpp:40-78 with u, v, n, uu, uv, vv, D precomputed per face
+SEED = 0x5EED
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rays-per-face", type=int, default=1000)
+    ap.add_argument("--cpu-sample-every", type=int, default=0, help="reference sample: every k-th source face")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default="", help="grid dims nx,ny,nz (default: automatic)")
+    return ap.parse_args()
+
+
+def workload(rays_per_face):
+    from form_factors_b200 import scenes
+    faces = scenes.enclosure(5, 20)
+    n = len(faces)
+    front = np.full(n, rays_per_face, np.int32)
+    rear = np.zeros(n, np.int32)
+    return faces, front, rear
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = [num(r[2]) for r in rows if num(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# the reference CPU path (oracle/_ref), bounded sample
+# ---------------------------------------------------------------------------
+def reference_sampler(faces, rays_per_face, every):
+    """Returns (run_step, describe): run_step() casts one bounded sample with
+    the reference's malley_cpu emission and zgrid_cpu caster on all cores and
+    returns (rays, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ctypes as C
+    from oracle_lib import Reference
+    if not Reference.available():
+        return None, "oracle/_ref/libffref.so not built (reference sources absent when the tree was built)"
+    ref = Reference()
+    n = len(faces)
+    cores = os.cpu_count() or 1
+    if every <= 0:
+        every = max(1, int(round(n * rays_per_face / (0.25e6 * cores))))  # ~1-4 s per step
+    mask = np.zeros(n, np.uint8)
+    mask[::every] = 1
+    # front weight 1, rear 0, total 1, n_rays = rays_per_face: exactly
+    # rays_per_face front rays per sampled face (malley_emission.cpp:50-54)
+    w = np.zeros(2 * n, np.float32)
+    w[0::2] = 1.0
+    prep = C.c_double()
+    h = ref.lib.ffref_step_open(Reference.ZGRID_CPU, n, np.ascontiguousarray(faces, np.float32), C.byref(prep))
+    if not h:
+        return None, "reference zgrid_cpu prepare failed"
+    hist = np.zeros(n, np.uint32)
+
+    def run():
+        te, tc = C.c_double(), C.c_double()
+        t0 = time.perf_counter()
+        k = ref.lib.ffref_step_run(h, rays_per_face, w, 1.0, mask, cores, hist.ctypes.data, C.byref(te),
+                                   C.byref(tc))
+        return k, time.perf_counter() - t0
+
+    desc = ("reference zgrid_cpu cast + malley_cpu emission (oracle/_ref) of every %d-th source face "
+            "(%d faces, %d rays) against the full %d-face scene, cast on %d threads" %
+            (every, int(mask.sum()), int(mask.sum()) * rays_per_face, n, cores))
+    return run, desc, cores
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    faces, front, rear = workload(args.rays_per_face)
+    out = reference_sampler(faces, args.rays_per_face, args.cpu_sample_every)
+    if out[0] is None:
+        print(json.dumps({"impl": "reference", "unavailable": out[1]}))
+        return
+    run, desc, cores = out
+    for _ in range(args.warmup):
+        run()
+    rays = 0
+    secs = 0.0
+    for _ in range(args.steps):
+        k, s = run()
+        rays += k
+        secs += s
+    v = rays / secs
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def fp32_peak(device):
+    import ctypes as C
+    from form_factors_b200 import build
+    lib = C.CDLL(build.PROBE_LIB)
+    lib.ffb_probe_fp32_ops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    v = C.c_double()
+    best = 0.0
+    for _ in range(3):
+        if lib.ffb_probe_fp32_ops(device, 20, C.byref(v)) == 0:
+            best = max(best, v.value)
+    return best
+
+
+def traffic_per_launch():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get("k_form_factors_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    from form_factors_b200 import build, native
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    build.build()
+    faces, front, rear = workload(args.rays_per_face)
+    n = len(faces)
+    rays_per_step = int(front.sum() + rear.sum())
+    ctx = native.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.scene_set(faces)
+    dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
+    t0 = time.perf_counter()
+    ctx.grid_build(dims=dims)
+    torch.cuda.synchronize()
+    grid_s = time.perf_counter() - t0
+    info = ctx.grid_info()
+    counts = torch.empty(n * n, dtype=torch.int32, device="cuda")  # uint32 bit patterns
+
+    def step(i, out=counts):
+        # replicas: each rank solves the same scene with its own Philox epoch
+        ctx.form_factor_counts(front, rear, SEED, epoch=1000 * rank + i, out=out, n_rows=n)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.2)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * rays_per_step / (ms_step * 1e-3)
+
+    # kernel-only time and counters of the fused kernel (one launch per step)
+    kms, tests, cells, hits = [], 0, 0, 0
+    for i in range(3):
+        step(10_000 + i)
+        s = ctx.stats()
+        kms.append(s.kernel_ms)
+        tests += s.tests
+        cells += s.cells
+        hits += s.hits
+    k_ms = statistics.median(kms)
+    tests_per_launch = tests / 3
+    achieved = tests_per_launch * FLOPS_PER_TEST / (k_ms * 1e-3)
+    peak = fp32_peak(local)
+
+    # end to end through the C ABI with host buffers
+    host_counts = torch.empty(n * n, dtype=torch.int32, pin_memory=True)
+    e2e_steps = max(2, min(args.steps, 5))
+    step(20_000, out=host_counts)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        step(20_001 + i, out=host_counts)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    n_chunks = sum((int(f) + 1023) // 1024 for f in (front + rear))  # hash-histogram chunks of 1024 rays
+    h2d = 16 * n_chunks
+    d2h = 4 * n * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out = reference_sampler(faces, args.rays_per_face, args.cpu_sample_every)
+        if out[0] is not None:
+            run, desc, cores = out
+            run()
+            k, s = run()
+            cpu = {"value": k / s, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc}
+        else:
+            cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": out[1]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "faces": n, "rays_per_step": rays_per_step,
+                       "grid": [info.nx, info.ny, info.nz], "grid_refs": int(info.n_refs),
+                       "grid_build_ms": 1e3 * grid_s, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed each step by zeroing the 1.95 GB count matrix"},
+            "e2e": {"value": world * rays_per_step / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "GFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic_per_launch(),
+                         "kernel": "k_form_factors", "kernel_ms": k_ms,
+                         "work": "%d FP32 ops per ray/triangle test x %.4g tests per launch" % (
+                             FLOPS_PER_TEST, tests_per_launch),
+                         "peak_source": "measured live: FMUL+FADD issue probe (libffb200_probe.so)"},
+            "tests_per_ray": tests / (3 * rays_per_step), "cells_per_ray": cells / (3 * rays_per_step),
+            "hit_fraction": hits / (3 * rays_per_step),
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

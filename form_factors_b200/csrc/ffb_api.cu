@@ -1,0 +1,778 @@
+// ffb_api.cu -- the C ABI of libffb200.so (declared in include/ffb.h).
+//
+// Host orchestration of the B200 form-factor path: resident scene and grid
+// per context, one CUDA stream per context, grow-only device scratch, pinned
+// staging for host arguments.  No CPU fallback: every result is computed by
+// the kernels of ffb_grid.cuh / ffb_trace.cuh.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ffb.h"
+#include "ffb_trace.cuh"
+
+using namespace ffb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define FFB_CUDA(call)                                                                                   \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess)                                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? FFB_ERR_NO_MEMORY : FFB_ERR_CUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                    \
+  } while (0)
+
+#define FFB_TRY(expr)   \
+  do {                  \
+    int r_ = (expr);    \
+    if (r_ < 0)         \
+      return r_;        \
+  } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+};
+
+constexpr int kDenseMaxRows = 8192;  // dense shared-memory row up to 32 KB
+constexpr int kHashCap = 2048;       // hash table slots (16 KB)
+constexpr int kDenseChunk = 4096;    // rays per chunk with a dense row
+constexpr int kHashChunk = kHashCap / 2;
+
+}  // namespace
+
+struct ffb_ctx {
+  int device = 0;
+  int n_sm = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  unsigned long long budget = 0;  // 0 = unlimited
+  unsigned long long bytes = 0;   // device bytes held in DevBufs
+
+  // scene
+  int n_faces = -1;  // -1: no scene
+  DevBuf faces, tri, box_lo, box_hi, frames, scene_ord;
+  int frames_mode = -1;  // emission flags the frames were built for
+
+  // grid
+  bool grid_ok = false;
+  ffb_grid_info info{};
+  DevBuf cell_start, cell_fill, ref_tri, empty_dist, scan_sums;
+
+  // per-call scratch
+  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev;
+  std::vector<unsigned char> host_stage_dummy;
+  void* pinned = nullptr;
+  size_t pinned_cap = 0;
+  cudaEvent_t pinned_free = nullptr;  // recorded after the last copy out of `pinned`
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;
+};
+
+namespace {
+
+int ensure(ffb_ctx* c, DevBuf& b, size_t need)
+{
+  if (need <= b.cap)
+    return FFB_OK;
+  size_t want = std::max(need, b.cap + b.cap / 2);
+  if (c->budget && c->bytes - b.cap + want > c->budget) {
+    want = need;
+    if (c->bytes - b.cap + want > c->budget)
+      return fail(FFB_ERR_NO_MEMORY, "device budget of %llu bytes exceeded (need %zu more)", c->budget, want);
+  }
+  if (b.ptr) {
+    cudaFreeAsync(b.ptr, c->stream);
+    c->bytes -= b.cap;
+    b.ptr = nullptr;
+    b.cap = 0;
+  }
+  cudaError_t e = cudaMallocAsync(&b.ptr, want, c->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FFB_ERR_NO_MEMORY, "cudaMallocAsync(%zu): %s", want, cudaGetErrorString(e));
+  }
+  b.cap = want;
+  c->bytes += want;
+  return FFB_OK;
+}
+
+void release(ffb_ctx* c, DevBuf& b)
+{
+  if (b.ptr) {
+    cudaFreeAsync(b.ptr, c->stream);
+    c->bytes -= b.cap;
+  }
+  b.ptr = nullptr;
+  b.cap = 0;
+}
+
+template <class T>
+T* dptr(DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
+
+bool is_device_ptr(const void* p)
+{
+  if (!p)
+    return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Pinned staging buffer; waits for the previous copy out of it first.
+int stage(ffb_ctx* c, size_t bytes, void** out)
+{
+  if (c->pinned_free)
+    FFB_CUDA(cudaEventSynchronize(c->pinned_free));
+  if (bytes > c->pinned_cap) {
+    if (c->pinned)
+      cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    size_t want = std::max(bytes, c->pinned_cap * 2);
+    FFB_CUDA(cudaMallocHost(&c->pinned, want));
+    c->pinned_cap = want;
+  }
+  *out = c->pinned;
+  return FFB_OK;
+}
+
+// Copies host data into device buffer `b` through the pinned stage.
+int upload(ffb_ctx* c, DevBuf& b, const void* host, size_t bytes)
+{
+  FFB_TRY(ensure(c, b, std::max<size_t>(bytes, 16)));
+  if (!bytes)
+    return FFB_OK;
+  void* st;
+  FFB_TRY(stage(c, bytes, &st));
+  memcpy(st, host, bytes);
+  FFB_CUDA(cudaMemcpyAsync(b.ptr, st, bytes, cudaMemcpyHostToDevice, c->stream));
+  FFB_CUDA(cudaEventRecord(c->pinned_free, c->stream));
+  return FFB_OK;
+}
+
+int grid_blocks(long long n, int threads, int max_blocks = 1 << 20)
+{
+  long long b = (n + threads - 1) / threads;
+  return (int)std::max<long long>(1, std::min<long long>(b, max_blocks));
+}
+
+GridView make_view(ffb_ctx* c)
+{
+  GridView g;
+  const ffb_grid_info& I = c->info;
+  g.lo = make_float3(I.lo[0], I.lo[1], I.lo[2]);
+  g.hi = make_float3(I.hi[0], I.hi[1], I.hi[2]);
+  g.cs = make_float3(I.cell[0], I.cell[1], I.cell[2]);
+  g.inv_cs = make_float3(1.f / I.cell[0], 1.f / I.cell[1], 1.f / I.cell[2]);
+  g.nx = I.nx;
+  g.ny = I.ny;
+  g.nz = I.nz;
+  g.slack = 2.f * I.margin;
+  g.cell_start = dptr<uint32_t>(c->cell_start);
+  g.ref_tri = dptr<int32_t>(c->ref_tri);
+  g.tri = dptr<TriRec>(c->tri);
+  g.empty_dist = I.skip_empty ? dptr<uint8_t>(c->empty_dist) : nullptr;
+  return g;
+}
+
+int check_ctx(ffb_ctx* c)
+{
+  if (!c)
+    return fail(FFB_ERR_ARG, "null context");
+  FFB_CUDA(cudaSetDevice(c->device));
+  return FFB_OK;
+}
+
+int ensure_frames(ffb_ctx* c, int flags)
+{
+  int mode = flags & FFB_EMIT_REF_NORMAL;
+  if (c->frames_mode == mode)
+    return FFB_OK;
+  FFB_TRY(ensure(c, c->frames, sizeof(float) * 20 * (size_t)std::max(c->n_faces, 1)));
+  if (c->n_faces > 0)
+    k_face_frames<<<grid_blocks(c->n_faces, 256), 256, 0, c->stream>>>(dptr<float>(c->faces), c->n_faces, mode,
+                                                                       dptr<float>(c->frames));
+  FFB_CUDA(cudaGetLastError());
+  c->frames_mode = mode;
+  return FFB_OK;
+}
+
+// Exclusive scan of n uint32 counts into out[0..n] (out[n] = total).
+int scan(ffb_ctx* c, const uint32_t* in, int n, uint32_t* out)
+{
+  int nb = (n + kScanTile - 1) / kScanTile;
+  FFB_TRY(ensure(c, c->scan_sums, sizeof(uint32_t) * (size_t)std::max(nb, 1)));
+  uint32_t* sums = dptr<uint32_t>(c->scan_sums);
+  k_scan_reduce<<<nb, kScanBlock, 0, c->stream>>>(in, n, sums);
+  k_scan_sums<<<1, kScanBlock, 0, c->stream>>>(sums, nb);
+  k_scan_apply<<<nb, kScanBlock, 0, c->stream>>>(in, n, sums, out);
+  FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
+}
+
+void timing_begin(ffb_ctx* c)
+{
+  cudaEventRecord(c->ev0, c->stream);
+}
+
+void timing_end(ffb_ctx* c)
+{
+  cudaEventRecord(c->ev1, c->stream);
+  c->timed = true;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Context
+// ===========================================================================
+extern "C" int ffb_ctx_create(int device, ffb_ctx** out)
+{
+  if (!out)
+    return fail(FFB_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(FFB_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= n)
+    return fail(FFB_ERR_ARG, "device %d out of range (%d devices)", device, n);
+  cudaDeviceProp prop;
+  FFB_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(FFB_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major,
+                prop.minor);
+  FFB_CUDA(cudaSetDevice(device));
+  ffb_ctx* c = new ffb_ctx;
+  c->device = device;
+  c->n_sm = prop.multiProcessorCount;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pinned_free, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(FFB_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return FFB_OK;
+}
+
+extern "C" void ffb_ctx_destroy(ffb_ctx* c)
+{
+  if (!c)
+    return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DevBuf* bufs[] = {&c->faces, &c->tri, &c->box_lo, &c->box_hi, &c->frames, &c->scene_ord, &c->cell_start,
+                    &c->cell_fill, &c->ref_tri, &c->empty_dist, &c->scan_sums, &c->chunks, &c->rows,
+                    &c->cursor, &c->stats, &c->tmp_in, &c->tmp_out, &c->tmp_out2, &c->offsets, &c->front_dev};
+  for (DevBuf* b : bufs)
+    release(c, *b);
+  cudaStreamSynchronize(c->stream);
+  if (c->pinned)
+    cudaFreeHost(c->pinned);
+  if (c->pinned_free) cudaEventDestroy(c->pinned_free);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+extern "C" int ffb_ctx_set_stream(ffb_ctx* c, void* stream)
+{
+  FFB_TRY(check_ctx(c));
+  // finish work on the old stream before switching (buffers are shared)
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return FFB_OK;
+}
+
+extern "C" void* ffb_ctx_stream(ffb_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int ffb_ctx_set_budget(ffb_ctx* c, unsigned long long bytes)
+{
+  if (!c)
+    return fail(FFB_ERR_ARG, "null context");
+  c->budget = bytes;
+  return FFB_OK;
+}
+
+extern "C" unsigned long long ffb_ctx_bytes(ffb_ctx* c) { return c ? c->bytes : 0; }
+
+extern "C" const char* ffb_last_error(void) { return g_last_error.c_str(); }
+
+// ===========================================================================
+// Scene and grid
+// ===========================================================================
+extern "C" int ffb_scene_set(ffb_ctx* c, const float* faces9, int n_faces)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_faces < 0 || (n_faces > 0 && !faces9))
+    return fail(FFB_ERR_ARG, "bad scene (n_faces=%d)", n_faces);
+  c->grid_ok = false;
+  c->frames_mode = -1;
+  c->n_faces = n_faces;
+  if (n_faces == 0)
+    return FFB_OK;
+  const size_t bytes = sizeof(float) * 9 * (size_t)n_faces;
+  if (is_device_ptr(faces9)) {
+    FFB_TRY(ensure(c, c->faces, bytes));
+    FFB_CUDA(cudaMemcpyAsync(c->faces.ptr, faces9, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    FFB_TRY(upload(c, c->faces, faces9, bytes));
+  }
+  FFB_TRY(ensure(c, c->tri, sizeof(TriRec) * (size_t)n_faces));
+  FFB_TRY(ensure(c, c->box_lo, sizeof(float4) * (size_t)n_faces));
+  FFB_TRY(ensure(c, c->box_hi, sizeof(float4) * (size_t)n_faces));
+  FFB_TRY(ensure(c, c->scene_ord, sizeof(uint32_t) * 6));
+  uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+  FFB_TRY(upload(c, c->scene_ord, init, sizeof init));
+  k_face_prepare<<<grid_blocks(n_faces, 256), 256, 0, c->stream>>>(
+      dptr<float>(c->faces), n_faces, dptr<TriRec>(c->tri), dptr<float4>(c->box_lo), dptr<float4>(c->box_hi),
+      dptr<uint32_t>(c->scene_ord));
+  FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
+}
+
+extern "C" int ffb_grid_build(ffb_ctx* c, const ffb_grid_params* params)
+{
+  FFB_TRY(check_ctx(c));
+  c->grid_ok = false;
+  if (c->n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "grid build without a scene (or with an empty scene)");
+  ffb_grid_params P = {0, 0, 0, 2.f, 1};
+  if (params)
+    P = *params;
+  if (P.cells_per_face <= 0.f)
+    P.cells_per_face = 2.f;
+  if (P.nx < 0 || P.ny < 0 || P.nz < 0 || P.nx > kMaxDim || P.ny > kMaxDim || P.nz > kMaxDim)
+    return fail(FFB_ERR_TOO_LARGE, "grid dims %dx%dx%d outside [0, %d]", P.nx, P.ny, P.nz, kMaxDim);
+
+  uint32_t ord[6];
+  FFB_CUDA(cudaMemcpyAsync(ord, c->scene_ord.ptr, sizeof ord, cudaMemcpyDeviceToHost, c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  float smin[3], smax[3];
+  for (int a = 0; a < 3; ++a) {
+    smin[a] = ord2f(ord[a]);
+    smax[a] = ord2f(ord[3 + a]);
+  }
+  ffb_grid_info I{};
+  bool any = ord[0] != 0xFFFFFFFFu && smin[0] <= smax[0];
+  if (!any) {  // nothing can be hit: a single empty cell
+    for (int a = 0; a < 3; ++a) {
+      smin[a] = 0.f;
+      smax[a] = 1.f;
+    }
+  }
+  float max_ext = 0.f, max_abs = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    max_ext = std::max(max_ext, smax[a] - smin[a]);
+    max_abs = std::max(max_abs, std::max(std::fabs(smin[a]), std::fabs(smax[a])));
+  }
+  // margin: far above the rounding of a computed hit point (a few ulps of the
+  // coordinates) and far below a cell
+  const float margin = max_ext * 0x1p-12f + max_abs * 0x1p-17f + 1e-30f;
+  double ext[3];
+  for (int a = 0; a < 3; ++a) {
+    I.lo[a] = smin[a] - 2.f * margin;
+    I.hi[a] = smax[a] + 2.f * margin;
+    ext[a] = (double)I.hi[a] - (double)I.lo[a];
+  }
+  int dims[3] = {P.nx, P.ny, P.nz};
+  if (!any) {
+    dims[0] = dims[1] = dims[2] = 1;
+  } else if (!P.nx || !P.ny || !P.nz) {
+    double mx = std::max(ext[0], std::max(ext[1], ext[2]));
+    double e2[3], vol = 1.0;
+    for (int a = 0; a < 3; ++a) {
+      e2[a] = std::max(ext[a], mx / 32.0);
+      vol *= e2[a];
+    }
+    double target = (double)P.cells_per_face * c->n_faces;
+    double s = std::cbrt(target / vol);
+    for (int a = 0; a < 3; ++a) {
+      if (!dims[a])
+        dims[a] = (int)std::min<double>(kMaxDim, std::max(1.0, std::round(ext[a] * s)));
+    }
+  }
+  I.nx = dims[0];
+  I.ny = dims[1];
+  I.nz = dims[2];
+  for (int a = 0; a < 3; ++a)
+    I.cell[a] = (float)(ext[a] / dims[a]);
+  // the last boundary lo + n*cs must reach hi: nudge the cell size up if the
+  // float product falls short
+  for (int a = 0; a < 3; ++a) {
+    while (I.lo[a] + (float)dims[a] * I.cell[a] < I.hi[a])
+      I.cell[a] = std::nextafter(I.cell[a], INFINITY);
+    I.hi[a] = I.lo[a] + (float)dims[a] * I.cell[a];
+  }
+  I.margin = margin;
+  I.skip_empty = P.skip_empty ? 1 : 0;
+  const long long n_cells = (long long)I.nx * I.ny * I.nz;
+
+  FFB_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (size_t)(n_cells + 1)));
+  FFB_TRY(ensure(c, c->cell_fill, sizeof(uint32_t) * (size_t)n_cells));
+  FFB_CUDA(cudaMemsetAsync(c->cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
+  BinGeom bg;
+  bg.lo = make_float3(I.lo[0], I.lo[1], I.lo[2]);
+  bg.cs = make_float3(I.cell[0], I.cell[1], I.cell[2]);
+  bg.inv_cs = make_float3(1.f / I.cell[0], 1.f / I.cell[1], 1.f / I.cell[2]);
+  bg.nx = I.nx;
+  bg.ny = I.ny;
+  bg.nz = I.nz;
+  bg.margin = margin;
+  const int nb = grid_blocks(c->n_faces, 128);
+  k_grid_count<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(c->faces), dptr<float4>(c->box_lo),
+                                          dptr<float4>(c->box_hi), c->n_faces, dptr<uint32_t>(c->cell_fill));
+  FFB_CUDA(cudaGetLastError());
+  FFB_TRY(scan(c, dptr<uint32_t>(c->cell_fill), (int)n_cells, dptr<uint32_t>(c->cell_start)));
+  uint32_t total = 0;
+  FFB_CUDA(cudaMemcpyAsync(&total, dptr<uint32_t>(c->cell_start) + n_cells, sizeof total, cudaMemcpyDeviceToHost,
+                           c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  FFB_TRY(ensure(c, c->ref_tri, sizeof(int32_t) * (size_t)std::max<uint32_t>(total, 1)));
+  FFB_CUDA(cudaMemsetAsync(c->cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
+  k_grid_fill<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(c->faces), dptr<float4>(c->box_lo),
+                                         dptr<float4>(c->box_hi), c->n_faces, dptr<uint32_t>(c->cell_start),
+                                         dptr<uint32_t>(c->cell_fill), dptr<int32_t>(c->ref_tri));
+  k_cell_sort<<<grid_blocks(n_cells, 128), 128, 0, c->stream>>>(dptr<uint32_t>(c->cell_start), (int)n_cells,
+                                                                dptr<int32_t>(c->ref_tri));
+  FFB_CUDA(cudaGetLastError());
+  if (I.skip_empty) {
+    FFB_TRY(ensure(c, c->empty_dist, (size_t)n_cells));
+    uint8_t* d = dptr<uint8_t>(c->empty_dist);
+    k_empty_init<<<grid_blocks(n_cells, 256), 256, 0, c->stream>>>(dptr<uint32_t>(c->cell_start), (int)n_cells, d);
+    k_empty_pass<<<grid_blocks((long long)I.ny * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 0);
+    k_empty_pass<<<grid_blocks((long long)I.nx * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 1);
+    k_empty_pass<<<grid_blocks((long long)I.nx * I.ny, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 2);
+    FFB_CUDA(cudaGetLastError());
+  }
+  // live faces: those with a non-empty binning box
+  I.n_refs = total;
+  I.n_live_faces = 0;
+  {
+    std::vector<float4> lo((size_t)c->n_faces), hi((size_t)c->n_faces);
+    FFB_CUDA(cudaMemcpyAsync(lo.data(), c->box_lo.ptr, sizeof(float4) * lo.size(), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FFB_CUDA(cudaMemcpyAsync(hi.data(), c->box_hi.ptr, sizeof(float4) * hi.size(), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+    for (int f = 0; f < c->n_faces; ++f)
+      I.n_live_faces += lo[f].x <= hi[f].x;
+  }
+  c->info = I;
+  c->grid_ok = true;
+  return FFB_OK;
+}
+
+extern "C" int ffb_grid_info_get(ffb_ctx* c, ffb_grid_info* out)
+{
+  if (!c || !out)
+    return fail(FFB_ERR_ARG, "null argument");
+  if (!c->grid_ok)
+    return fail(FFB_ERR_NO_GRID, "no grid built");
+  *out = c->info;
+  return FFB_OK;
+}
+
+// ===========================================================================
+// Casts
+// ===========================================================================
+namespace {
+
+// Resolves an input array: device pointers pass through, host data is copied
+// into `tmp`.
+int input_ptr(ffb_ctx* c, const void* p, size_t bytes, DevBuf& tmp, const void** out)
+{
+  if (is_device_ptr(p)) {
+    *out = p;
+    return FFB_OK;
+  }
+  FFB_TRY(ensure(c, tmp, std::max<size_t>(bytes, 16)));
+  if (bytes)
+    FFB_CUDA(cudaMemcpyAsync(tmp.ptr, p, bytes, cudaMemcpyHostToDevice, c->stream));
+  *out = tmp.ptr;
+  return FFB_OK;
+}
+
+// Resolves an output array: device pointers pass through, host outputs get a
+// device temporary copied back by finish_output.
+int output_ptr(ffb_ctx* c, void* p, size_t bytes, DevBuf& tmp, void** out, bool* host)
+{
+  *host = p && !is_device_ptr(p);
+  if (!p || !*host) {
+    *out = p;
+    return FFB_OK;
+  }
+  FFB_TRY(ensure(c, tmp, std::max<size_t>(bytes, 16)));
+  *out = tmp.ptr;
+  return FFB_OK;
+}
+
+int finish_output(ffb_ctx* c, void* host, const void* dev, size_t bytes)
+{
+  if (bytes)
+    FFB_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  return FFB_OK;
+}
+
+int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_face, float* hit_point, bool brute)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_rays < 0 || (n_rays > 0 && (!rays6 || !hit_face)))
+    return fail(FFB_ERR_ARG, "bad cast arguments");
+  if (c->n_faces < 0)
+    return fail(FFB_ERR_NO_SCENE, "cast without a scene");
+  if (!brute && !c->grid_ok)
+    return fail(FFB_ERR_NO_GRID, "cast before ffb_grid_build");
+  if (n_rays == 0)
+    return FFB_OK;
+  const void* d_rays;
+  void *d_hit, *d_pt;
+  bool host_hit, host_pt;
+  FFB_TRY(input_ptr(c, rays6, sizeof(float) * 6 * (size_t)n_rays, c->tmp_in, &d_rays));
+  FFB_TRY(output_ptr(c, hit_face, sizeof(int32_t) * (size_t)n_rays, c->tmp_out, &d_hit, &host_hit));
+  FFB_TRY(output_ptr(c, hit_point, sizeof(float) * 3 * (size_t)n_rays, c->tmp_out2, &d_pt, &host_pt));
+  FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
+  FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
+  timing_begin(c);
+  if (brute || c->n_faces == 0) {
+    k_cast_brute<<<grid_blocks(n_rays, kTraceThreads), kTraceThreads, 0, c->stream>>>(
+        dptr<TriRec>(c->tri), c->n_faces, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit, (float*)d_pt);
+  } else {
+    GridView g = make_view(c);
+    int blocks = grid_blocks(n_rays, kTraceThreads, c->n_sm * 16);
+    if (g.empty_dist)
+      k_cast<true><<<blocks, kTraceThreads, 0, c->stream>>>(g, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit,
+                                                             (float*)d_pt, dptr<unsigned long long>(c->stats));
+    else
+      k_cast<false><<<blocks, kTraceThreads, 0, c->stream>>>(g, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit,
+                                                              (float*)d_pt, dptr<unsigned long long>(c->stats));
+  }
+  timing_end(c);
+  FFB_CUDA(cudaGetLastError());
+  if (host_hit)
+    FFB_TRY(finish_output(c, hit_face, d_hit, sizeof(int32_t) * (size_t)n_rays));
+  if (host_pt)
+    FFB_TRY(finish_output(c, hit_point, d_pt, sizeof(float) * 3 * (size_t)n_rays));
+  if (host_hit || host_pt || !is_device_ptr(rays6))
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  return FFB_OK;
+}
+
+}  // namespace
+
+extern "C" int ffb_cast(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_face, float* hit_point)
+{
+  return cast_impl(c, rays6, n_rays, hit_face, hit_point, false);
+}
+
+extern "C" int ffb_cast_bruteforce(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_face,
+                                   float* hit_point)
+{
+  return cast_impl(c, rays6, n_rays, hit_face, hit_point, true);
+}
+
+// ===========================================================================
+// Emission and form factors
+// ===========================================================================
+namespace {
+
+int check_counts(ffb_ctx* c, const int32_t* front, const int32_t* rear, long long* total)
+{
+  if (c->n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!front || !rear)
+    return fail(FFB_ERR_ARG, "null ray counts");
+  long long t = 0;
+  for (int f = 0; f < c->n_faces; ++f) {
+    if (front[f] < 0 || rear[f] < 0)
+      return fail(FFB_ERR_ARG, "negative ray count at face %d", f);
+    t += (long long)front[f] + rear[f];
+  }
+  *total = t;
+  return FFB_OK;
+}
+
+}  // namespace
+
+extern "C" int ffb_emit(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
+                        int flags, float* rays6)
+{
+  FFB_TRY(check_ctx(c));
+  long long total = 0;
+  FFB_TRY(check_counts(c, front, rear, &total));
+  if (total == 0)
+    return FFB_OK;
+  if (!rays6)
+    return fail(FFB_ERR_ARG, "null ray output");
+  FFB_TRY(ensure_frames(c, flags));
+  std::vector<long long> offs((size_t)c->n_faces + 1);
+  offs[0] = 0;
+  for (int f = 0; f < c->n_faces; ++f)
+    offs[f + 1] = offs[f] + front[f] + rear[f];
+  FFB_TRY(upload(c, c->offsets, offs.data(), sizeof(long long) * offs.size()));
+  // front counts after the offsets in the same stage would race the stage;
+  // upload() waits for the previous copy, so sequential uploads are safe
+  FFB_TRY(upload(c, c->front_dev, front, sizeof(int32_t) * (size_t)c->n_faces));
+  void* d_rays;
+  bool host_out;
+  FFB_TRY(output_ptr(c, rays6, sizeof(float) * 6 * (size_t)total, c->tmp_out, &d_rays, &host_out));
+  k_emit<<<grid_blocks(total, 256, c->n_sm * 32), 256, 0, c->stream>>>(
+      dptr<float>(c->frames), dptr<long long>(c->offsets), dptr<int32_t>(c->front_dev), c->n_faces, (long)total,
+      (uint32_t)seed, (uint32_t)(seed >> 32), epoch, (float*)d_rays);
+  FFB_CUDA(cudaGetLastError());
+  if (host_out) {
+    FFB_TRY(finish_output(c, rays6, d_rays, sizeof(float) * 6 * (size_t)total));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return FFB_OK;
+}
+
+extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                      uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
+                                      uint32_t* counts)
+{
+  FFB_TRY(check_ctx(c));
+  if (!c->grid_ok)
+    return fail(FFB_ERR_NO_GRID, "form factors before ffb_grid_build");
+  long long total = 0;
+  FFB_TRY(check_counts(c, front, rear, &total));
+  if (!counts)
+    return fail(FFB_ERR_ARG, "null counts");
+  if (!face_to_row && n_rows != c->n_faces)
+    return fail(FFB_ERR_ARG, "identity rows need n_rows == n_faces (%d != %d)", n_rows, c->n_faces);
+  if (n_rows <= 0)
+    return fail(FFB_ERR_ARG, "n_rows must be positive");
+  if (face_to_row) {
+    for (int f = 0; f < c->n_faces; ++f)
+      if (face_to_row[f] < 0 || face_to_row[f] >= n_rows)
+        return fail(FFB_ERR_ARG, "face_to_row[%d] = %d outside [0, %d)", f, face_to_row[f], n_rows);
+  }
+  FFB_TRY(ensure_frames(c, flags));
+  const bool hash = n_rows > kDenseMaxRows;
+  const int chunk = hash ? kHashChunk : kDenseChunk;
+  std::vector<Chunk> chunks;
+  chunks.reserve((size_t)(total / chunk + c->n_faces));
+  for (int f = 0; f < c->n_faces; ++f) {
+    const int nf = front[f] + rear[f];
+    for (int j0 = 0; j0 < nf; j0 += chunk)
+      chunks.push_back(Chunk{f, j0, std::min(chunk, nf - j0), front[f]});
+  }
+  const size_t mat = (size_t)n_rows * n_rows;
+  void* d_counts;
+  bool host_out;
+  FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * mat, c->tmp_out, &d_counts, &host_out));
+  FFB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * mat, c->stream));
+  FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
+  FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
+  if (!chunks.empty()) {
+    FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
+    if (face_to_row)
+      FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)c->n_faces));
+    FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
+    FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
+    TraceParams p;
+    p.g = make_view(c);
+    p.frames = dptr<float>(c->frames);
+    p.chunks = dptr<Chunk>(c->chunks);
+    p.n_chunks = (int)chunks.size();
+    p.face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
+    p.n_cols = n_rows;
+    p.counts = (uint32_t*)d_counts;
+    p.key0 = (uint32_t)seed;
+    p.key1 = (uint32_t)(seed >> 32);
+    p.epoch = epoch;
+    p.chunk_cursor = dptr<uint32_t>(c->cursor);
+    p.stats = dptr<unsigned long long>(c->stats);
+    p.hash_cap = kHashCap;
+    const size_t smem = hash ? sizeof(uint32_t) * 2 * kHashCap : sizeof(uint32_t) * (size_t)n_rows;
+    void (*kern)(TraceParams);
+    if (hash)
+      kern = p.g.empty_dist ? k_form_factors<true, true> : k_form_factors<true, false>;
+    else
+      kern = p.g.empty_dist ? k_form_factors<false, true> : k_form_factors<false, false>;
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, smem));
+    const int blocks = std::max(1, std::min<int>(per_sm * c->n_sm, (int)chunks.size()));
+    timing_begin(c);
+    kern<<<blocks, kTraceThreads, smem, c->stream>>>(p);
+    timing_end(c);
+    FFB_CUDA(cudaGetLastError());
+  }
+  if (host_out) {
+    FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * mat));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return FFB_OK;
+}
+
+extern "C" int ffb_normalise(ffb_ctx* c, const uint32_t* counts, const int32_t* outgoing, int n_rows, float* ff)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_rows <= 0 || !counts || !outgoing || !ff)
+    return fail(FFB_ERR_ARG, "bad normalise arguments");
+  const size_t mat = (size_t)n_rows * n_rows;
+  const void* d_counts;
+  void* d_ff;
+  bool host_out;
+  FFB_TRY(input_ptr(c, counts, sizeof(uint32_t) * mat, c->tmp_in, &d_counts));
+  FFB_TRY(upload(c, c->front_dev, outgoing, sizeof(int32_t) * (size_t)n_rows));
+  FFB_TRY(output_ptr(c, ff, sizeof(float) * mat, c->tmp_out2, &d_ff, &host_out));
+  k_normalise<<<grid_blocks((long long)mat, 256, c->n_sm * 16), 256, 0, c->stream>>>(
+      (const uint32_t*)d_counts, dptr<int32_t>(c->front_dev), n_rows, (float*)d_ff);
+  FFB_CUDA(cudaGetLastError());
+  if (host_out) {
+    FFB_TRY(finish_output(c, ff, d_ff, sizeof(float) * mat));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return FFB_OK;
+}
+
+extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)
+{
+  FFB_TRY(check_ctx(c));
+  if (!out)
+    return fail(FFB_ERR_ARG, "null output");
+  memset(out, 0, sizeof *out);
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->stats.ptr) {
+    unsigned long long s[kStatSlots];
+    FFB_CUDA(cudaMemcpy(s, c->stats.ptr, sizeof s, cudaMemcpyDeviceToHost));
+    out->tests = s[kStatTests];
+    out->cells = s[kStatCells];
+    out->rays = s[kStatRays];
+    out->hits = s[kStatHits];
+  }
+  if (c->timed)
+    cudaEventElapsedTime(&out->kernel_ms, c->ev0, c->ev1);
+  return FFB_OK;
+}

@@ -1,0 +1,221 @@
+"""ctypes binding of libffb200.so (the C ABI of include/ffb.h).
+
+Arguments may be numpy arrays (host memory; the library stages them) or
+objects exposing ``data_ptr()`` such as CUDA torch tensors (device memory,
+used in place).  Loading fails loudly when the library is missing: there is
+no CPU fallback for any call.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libffb200.so")
+HEADER = os.path.join(ROOT, "include", "ffb.h")
+
+FFB_OK = 0
+FFB_EMIT_REF_NORMAL = 1
+ERRORS = {
+    -301: "FFB_ERR_ARG", -302: "FFB_ERR_CUDA", -303: "FFB_ERR_NO_SCENE", -304: "FFB_ERR_NO_GRID",
+    -305: "FFB_ERR_NO_MEMORY", -306: "FFB_ERR_TOO_LARGE", -307: "FFB_ERR_NO_DEVICE",
+}
+
+
+class FFBError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "error"), code, msg))
+        self.code = code
+
+
+class GridParams(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("cells_per_face", C.c_float),
+                ("skip_empty", C.c_int)]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("lo", C.c_float * 3), ("hi", C.c_float * 3), ("cell", C.c_float * 3), ("nx", C.c_int),
+                ("ny", C.c_int), ("nz", C.c_int), ("n_live_faces", C.c_int), ("n_refs", C.c_longlong),
+                ("margin", C.c_float), ("skip_empty", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("tests", C.c_ulonglong), ("cells", C.c_ulonglong), ("rays", C.c_ulonglong),
+                ("hits", C.c_ulonglong), ("kernel_ms", C.c_float)]
+
+
+_lib = None
+
+
+def declared_symbols(header=HEADER):
+    """Function names declared in a C header (every `ffb_*(` prototype)."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ffb_\w+)\s*\(", text)))
+
+
+def load(path=LIB_PATH):
+    """Loads libffb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("%s is missing: run form_factors_b200.build.build() (or __graft_entry__.build())" % path)
+    lib = C.CDLL(path)
+    vp, i32, i64, u64, u32 = C.c_void_p, C.c_int, C.c_longlong, C.c_uint64, C.c_uint32
+    sig = {
+        "ffb_ctx_create": (i32, [i32, C.POINTER(vp)]),
+        "ffb_ctx_destroy": (None, [vp]),
+        "ffb_ctx_set_stream": (i32, [vp, vp]),
+        "ffb_ctx_stream": (vp, [vp]),
+        "ffb_ctx_set_budget": (i32, [vp, C.c_ulonglong]),
+        "ffb_ctx_bytes": (C.c_ulonglong, [vp]),
+        "ffb_last_error": (C.c_char_p, []),
+        "ffb_scene_set": (i32, [vp, vp, i32]),
+        "ffb_grid_build": (i32, [vp, C.POINTER(GridParams)]),
+        "ffb_grid_info_get": (i32, [vp, C.POINTER(GridInfo)]),
+        "ffb_cast": (i32, [vp, vp, i64, vp, vp]),
+        "ffb_cast_bruteforce": (i32, [vp, vp, i64, vp, vp]),
+        "ffb_emit": (i32, [vp, vp, vp, u64, u32, i32, vp]),
+        "ffb_form_factor_counts": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp]),
+        "ffb_normalise": (i32, [vp, vp, vp, i32, vp]),
+        "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    """Address of a numpy array or a tensor (data_ptr), or None."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    raise TypeError("unsupported buffer type %r" % type(a))
+
+
+def _check(code):
+    if code < 0:
+        raise FFBError(code, load().ffb_last_error().decode(errors="replace"))
+    return code
+
+
+class Context:
+    """One device, one stream, a resident scene and grid (see include/ffb.h)."""
+
+    def __init__(self, device=0):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.ffb_ctx_create(int(device), C.byref(h)))
+        self._h = h
+        self._lib = lib
+        self.n_faces = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ffb_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr):
+        _check(self._lib.ffb_ctx_set_stream(self._h, stream_ptr))
+
+    def set_budget(self, nbytes):
+        _check(self._lib.ffb_ctx_set_budget(self._h, int(nbytes)))
+
+    def device_bytes(self):
+        return int(self._lib.ffb_ctx_bytes(self._h))
+
+    def scene_set(self, faces):
+        n = int(faces.shape[0]) if faces is not None else 0
+        if isinstance(faces, np.ndarray):
+            faces = np.ascontiguousarray(faces, np.float32).reshape(-1, 9)
+            n = len(faces)
+        _check(self._lib.ffb_scene_set(self._h, _ptr(faces) if n else None, n))
+        self.n_faces = n
+
+    def grid_build(self, dims=None, cells_per_face=2.0, skip_empty=True):
+        p = GridParams(0, 0, 0, float(cells_per_face), int(bool(skip_empty)))
+        if dims is not None:
+            p.nx, p.ny, p.nz = [int(d) for d in dims]
+        _check(self._lib.ffb_grid_build(self._h, C.byref(p)))
+
+    def grid_info(self):
+        info = GridInfo()
+        _check(self._lib.ffb_grid_info_get(self._h, C.byref(info)))
+        return info
+
+    def cast(self, rays, hit=None, points=None, want_points=True, brute=False):
+        """rays: (n, 6) float32 host array or device tensor.  Returns (hit, points)."""
+        n = int(rays.shape[0]) if not isinstance(rays, np.ndarray) else len(rays.reshape(-1, 6))
+        if isinstance(rays, np.ndarray):
+            rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        if hit is None:
+            hit = np.empty(n, np.int32)
+        if points is None and want_points:
+            points = np.empty((n, 3), np.float32)
+        fn = self._lib.ffb_cast_bruteforce if brute else self._lib.ffb_cast
+        _check(fn(self._h, _ptr(rays), n, _ptr(hit), _ptr(points)))
+        return hit, points
+
+    def emit(self, front, rear, seed, epoch=0, flags=0, out=None):
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        total = int(front.sum(dtype=np.int64) + rear.sum(dtype=np.int64))
+        if out is None:
+            out = np.empty((total, 6), np.float32)
+        _check(self._lib.ffb_emit(self._h, _ptr(front), _ptr(rear), int(seed), int(epoch), int(flags), _ptr(out)))
+        return out
+
+    def form_factor_counts(self, front, rear, seed, epoch=0, flags=0, face_to_row=None, n_rows=None, out=None):
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        if face_to_row is not None:
+            face_to_row = np.ascontiguousarray(face_to_row, np.int32)
+        if n_rows is None:
+            n_rows = self.n_faces if face_to_row is None else int(face_to_row.max()) + 1
+        if out is None:
+            out = np.empty((n_rows, n_rows), np.uint32)
+        _check(self._lib.ffb_form_factor_counts(self._h, _ptr(front), _ptr(rear), int(seed), int(epoch), int(flags),
+                                                _ptr(face_to_row), int(n_rows), _ptr(out)))
+        return out
+
+    def normalise(self, counts, outgoing, out=None):
+        outgoing = np.ascontiguousarray(outgoing, np.int32)
+        n = len(outgoing)
+        if isinstance(counts, np.ndarray):
+            counts = np.ascontiguousarray(counts, np.uint32)
+        if out is None:
+            out = np.empty((n, n), np.float32)
+        _check(self._lib.ffb_normalise(self._h, _ptr(counts), _ptr(outgoing), n, _ptr(out)))
+        return out
+
+    def stats(self):
+        s = Stats()
+        _check(self._lib.ffb_stats_get(self._h, C.byref(s)))
+        return s

@@ -1,0 +1,134 @@
+/*
+ * ffb.h -- C ABI of libffb200.so, the B200 (sm_100a) form-factor path.
+ *
+ * Plain pointers and sizes only.  Every function returns FFB_OK (0) or a
+ * negative FFB_ERR_* code and never exits or resets the device; the message
+ * of the last failure on the calling thread is in ffb_last_error().
+ *
+ * Pointer arguments marked "host or device" are classified with
+ * cudaPointerGetAttributes: device (or managed) memory is used in place;
+ * host memory is staged through the context's buffers.  A call whose outputs
+ * are all in device memory only enqueues work on the context stream and
+ * returns (CUDA-graph capturable); a call with a host output synchronises the
+ * stream before it returns.
+ *
+ * Geometry layouts are the reference's (math/types.h:36-76):
+ *   face  = 9 floats, three vertices            (math::triangle_t, 36 B)
+ *   ray   = 6 floats, origin then END POINT     (math::ray_t, 24 B; the
+ *           direction is end - origin, ray_caster/naive_cpu.cpp, math/triangle.cpp:41)
+ *
+ * The C++ system_t types of ffb_systems.h wrap these calls behind the
+ * reference's own ray_caster / emission / form_factors interfaces.
+ */
+#ifndef FFB_H
+#define FFB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFB_OK 0
+#define FFB_ERR_ARG (-301)       /* invalid argument */
+#define FFB_ERR_CUDA (-302)      /* CUDA runtime failure (see ffb_last_error) */
+#define FFB_ERR_NO_SCENE (-303)  /* no scene, or a scene with no faces */
+#define FFB_ERR_NO_GRID (-304)   /* cast before ffb_grid_build */
+#define FFB_ERR_NO_MEMORY (-305) /* device allocation failed or over the context budget */
+#define FFB_ERR_TOO_LARGE (-306) /* a size beyond a documented limit */
+#define FFB_ERR_NO_DEVICE (-307) /* no CUDA device / not an sm_100 device */
+
+/* Emission flag: rotate +z towards the raw cross-product normal, as the
+ * reference's emission/malley_cpu.cpp:125-129 does.  Without it the normal is
+ * normalised first (cosine-weighted directions for any triangle size). */
+#define FFB_EMIT_REF_NORMAL 1
+
+typedef struct ffb_ctx ffb_ctx;
+
+typedef struct {
+  int nx, ny, nz;          /* cells per axis, each <= 256; 0 = choose from cells_per_face */
+  float cells_per_face;    /* automatic sizing target (cells ~ this * faces); <= 0 means 2 */
+  int skip_empty;          /* 1 = jump through empty space (distance map), 0 = plain DDA */
+} ffb_grid_params;
+
+typedef struct {
+  float lo[3], hi[3];      /* grid box */
+  float cell[3];           /* cell size */
+  int nx, ny, nz;
+  int n_live_faces;        /* faces that can be hit (finite, non-degenerate) */
+  long long n_refs;        /* triangle references in all cells */
+  float margin;            /* binning margin, world units */
+  int skip_empty;
+} ffb_grid_info;
+
+typedef struct {
+  unsigned long long tests; /* ray/triangle tests executed */
+  unsigned long long cells; /* grid cells visited */
+  unsigned long long rays;  /* rays traced */
+  unsigned long long hits;  /* rays that hit a face */
+  float kernel_ms;          /* device time of the trace kernel (CUDA events) */
+} ffb_stats;
+
+/* Context: one device, one stream, resident scene and grid.
+ * Replaces the state of ray_caster::system_create (ray_caster/system.cpp:65-90). */
+int ffb_ctx_create(int device, ffb_ctx** out);
+void ffb_ctx_destroy(ffb_ctx* ctx);
+/* Use `stream` (a cudaStream_t) instead of the context's own; NULL restores it. */
+int ffb_ctx_set_stream(ffb_ctx* ctx, void* stream);
+void* ffb_ctx_stream(ffb_ctx* ctx);
+/* Device-memory budget of the context in bytes (0 = unlimited). */
+int ffb_ctx_set_budget(ffb_ctx* ctx, unsigned long long bytes);
+unsigned long long ffb_ctx_bytes(ffb_ctx* ctx);
+const char* ffb_last_error(void);
+
+/* Scene upload and per-face precompute (host or device faces9).
+ * ray_caster::system_set_scene, ray_caster/system.h:95.  n_faces == 0 is
+ * accepted (the reference accepts an empty scene); ffb_grid_build then
+ * fails with FFB_ERR_NO_SCENE as ray_caster prepare does (zgrid_cpu.cpp:59). */
+int ffb_scene_set(ffb_ctx* ctx, const float* faces9, int n_faces);
+
+/* Device grid build (counting sort of triangle references into cells).
+ * ray_caster::system_prepare, ray_caster/system.h:98; zgrid_cpu.cpp:57-68.
+ * params may be NULL (automatic). */
+int ffb_grid_build(ffb_ctx* ctx, const ffb_grid_params* params);
+int ffb_grid_info_get(ffb_ctx* ctx, ffb_grid_info* out);
+
+/* Nearest hit per ray through the grid.  rays6: host or device; hit_face:
+ * host or device, face index or -1; hit_point: host, device or NULL, the
+ * reference's hit point for hits and NaN for misses.  Equal bit for bit to
+ * ray_caster/naive_cpu.cpp:65-97.  ray_caster::system_cast, ray_caster/system.h:102. */
+int ffb_cast(ffb_ctx* ctx, const float* rays6, long long n_rays, int32_t* hit_face, float* hit_point);
+
+/* Same result by brute force (every ray against every face), the naive
+ * definition without the grid; needs only ffb_scene_set. */
+int ffb_cast_bruteforce(ffb_ctx* ctx, const float* rays6, long long n_rays, int32_t* hit_face, float* hit_point);
+
+/* Malley emission rays, packed face by face, front then rear
+ * (emission/malley_cpu.cpp:142-189), ray j of face f drawn from
+ * Philox4x32-10 keyed by (seed, epoch, f, j).  front/rear: host int32[n_faces]
+ * ray counts; rays6: host or device, 6 * sum(front + rear) floats. */
+int ffb_emit(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
+             float* rays6);
+
+/* Fused emission + grid trace + count: counts[row(f) * n_rows + row(h)] +=
+ * number of rays of face f whose nearest hit is face h, where row() is
+ * face_to_row (host int32[n_faces], values in [0, n_rows)) or the identity
+ * when face_to_row is NULL (then n_rows must equal n_faces).  counts: host or
+ * device uint32[n_rows * n_rows], overwritten.  The per-face (row) form of
+ * cpuFactorsCalculator/cpu_system.cpp:162-190. */
+int ffb_form_factor_counts(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
+                           int flags, const int32_t* face_to_row, int n_rows, uint32_t* counts);
+
+/* ff[m * n_rows + j] = (float)counts[m * n_rows + j] * (1.f / (float)outgoing[m]),
+ * the row normalisation of cpuFactorsCalculator/cpu_system.cpp:193-195.
+ * counts and ff: host or device; outgoing: host int32[n_rows]. */
+int ffb_normalise(ffb_ctx* ctx, const uint32_t* counts, const int32_t* outgoing, int n_rows, float* ff);
+
+/* Counters and kernel time of the last ffb_cast / ffb_form_factor_counts
+ * (synchronises the stream). */
+int ffb_stats_get(ffb_ctx* ctx, ffb_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFB_H */
