@@ -231,8 +231,11 @@ def ours(args):
     n = len(faces)
     rays_per_step = int(front.sum() + rear.sum())
     ctx = native.Context(local)
-    stream = torch.cuda.current_stream()
+    # a real (non-default) stream shared by the library and the timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
+    assert ctx.stream_ptr() == stream.cuda_stream
     ctx.scene_set(faces)
     dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
     t0 = time.perf_counter()

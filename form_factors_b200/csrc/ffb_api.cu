@@ -55,10 +55,8 @@ struct DevBuf {
   size_t cap = 0;
 };
 
-constexpr int kDenseMaxRows = 8192;  // dense shared-memory row up to 32 KB
-constexpr int kHashCap = 2048;       // hash table slots (16 KB)
-constexpr int kDenseChunk = 4096;    // rays per chunk with a dense row
-constexpr int kHashChunk = kHashCap / 2;
+constexpr int kChunkRays = 256;  // rays per work chunk of the fused kernel
+constexpr int kMaxRows = 65535;  // matrix index row * n + col stays below 0xFFFFFFFF
 
 }  // namespace
 
@@ -78,10 +76,10 @@ struct ffb_ctx {
   // grid
   bool grid_ok = false;
   ffb_grid_info info{};
-  DevBuf cell_start, cell_fill, ref_tri, empty_dist, scan_sums;
+  DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist, scan_sums;
 
   // per-call scratch
-  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev;
+  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor;
   std::vector<unsigned char> host_stage_dummy;
   void* pinned = nullptr;
   size_t pinned_cap = 0;
@@ -194,7 +192,7 @@ GridView make_view(ffb_ctx* c)
   g.slack = 2.f * I.margin;
   g.cell_start = dptr<uint32_t>(c->cell_start);
   g.ref_tri = dptr<int32_t>(c->ref_tri);
-  g.tri = dptr<TriRec>(c->tri);
+  g.ref_rec = dptr<TriRec>(c->ref_rec);
   g.empty_dist = I.skip_empty ? dptr<uint8_t>(c->empty_dist) : nullptr;
   return g;
 }
@@ -290,9 +288,10 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
     return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->faces, &c->tri, &c->box_lo, &c->box_hi, &c->frames, &c->scene_ord, &c->cell_start,
-                    &c->cell_fill, &c->ref_tri, &c->empty_dist, &c->scan_sums, &c->chunks, &c->rows,
-                    &c->cursor, &c->stats, &c->tmp_in, &c->tmp_out, &c->tmp_out2, &c->offsets, &c->front_dev};
+  DevBuf* bufs[] = {&c->faces,     &c->tri,       &c->box_lo,   &c->box_hi,     &c->frames,    &c->scene_ord,
+                    &c->cell_start, &c->cell_fill, &c->ref_tri,  &c->ref_rec,    &c->empty_dist, &c->scan_sums,
+                    &c->chunks,    &c->rows,      &c->cursor,   &c->stats,      &c->tmp_in,    &c->tmp_out,
+                    &c->tmp_out2,  &c->offsets,   &c->front_dev, &c->ray_cursor};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
@@ -465,6 +464,9 @@ extern "C" int ffb_grid_build(ffb_ctx* c, const ffb_grid_params* params)
                                          dptr<uint32_t>(c->cell_fill), dptr<int32_t>(c->ref_tri));
   k_cell_sort<<<grid_blocks(n_cells, 128), 128, 0, c->stream>>>(dptr<uint32_t>(c->cell_start), (int)n_cells,
                                                                 dptr<int32_t>(c->ref_tri));
+  FFB_TRY(ensure(c, c->ref_rec, sizeof(TriRec) * (size_t)std::max<uint32_t>(total, 1)));
+  k_ref_gather<<<grid_blocks(total, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+      dptr<int32_t>(c->ref_tri), total, dptr<TriRec>(c->tri), dptr<TriRec>(c->ref_rec));
   FFB_CUDA(cudaGetLastError());
   if (I.skip_empty) {
     FFB_TRY(ensure(c, c->empty_dist, (size_t)n_cells));
@@ -569,13 +571,15 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
         dptr<TriRec>(c->tri), c->n_faces, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit, (float*)d_pt);
   } else {
     GridView g = make_view(c);
-    int blocks = grid_blocks(n_rays, kTraceThreads, c->n_sm * 16);
-    if (g.empty_dist)
-      k_cast<true><<<blocks, kTraceThreads, 0, c->stream>>>(g, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit,
-                                                             (float*)d_pt, dptr<unsigned long long>(c->stats));
-    else
-      k_cast<false><<<blocks, kTraceThreads, 0, c->stream>>>(g, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit,
-                                                              (float*)d_pt, dptr<unsigned long long>(c->stats));
+    FFB_TRY(ensure(c, c->ray_cursor, sizeof(unsigned long long)));
+    FFB_CUDA(cudaMemsetAsync(c->ray_cursor.ptr, 0, sizeof(unsigned long long), c->stream));
+    auto kern = g.empty_dist ? k_cast<true> : k_cast<false>;
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
+    const int blocks = grid_blocks(n_rays, kTraceThreads, std::max(1, per_sm) * c->n_sm);
+    kern<<<blocks, kTraceThreads, 0, c->stream>>>(g, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit,
+                                                  (float*)d_pt, dptr<unsigned long long>(c->stats),
+                                                  dptr<unsigned long long>(c->ray_cursor));
   }
   timing_end(c);
   FFB_CUDA(cudaGetLastError());
@@ -677,15 +681,15 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
       if (face_to_row[f] < 0 || face_to_row[f] >= n_rows)
         return fail(FFB_ERR_ARG, "face_to_row[%d] = %d outside [0, %d)", f, face_to_row[f], n_rows);
   }
+  if (n_rows > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
   FFB_TRY(ensure_frames(c, flags));
-  const bool hash = n_rows > kDenseMaxRows;
-  const int chunk = hash ? kHashChunk : kDenseChunk;
   std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / chunk + c->n_faces));
+  chunks.reserve((size_t)(total / kChunkRays + c->n_faces));
   for (int f = 0; f < c->n_faces; ++f) {
     const int nf = front[f] + rear[f];
-    for (int j0 = 0; j0 < nf; j0 += chunk)
-      chunks.push_back(Chunk{f, j0, std::min(chunk, nf - j0), front[f]});
+    for (int j0 = 0; j0 < nf; j0 += kChunkRays)
+      chunks.push_back(Chunk{f, j0, std::min(kChunkRays, nf - j0), front[f]});
   }
   const size_t mat = (size_t)n_rows * n_rows;
   void* d_counts;
@@ -713,18 +717,15 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
     p.epoch = epoch;
     p.chunk_cursor = dptr<uint32_t>(c->cursor);
     p.stats = dptr<unsigned long long>(c->stats);
-    p.hash_cap = kHashCap;
-    const size_t smem = hash ? sizeof(uint32_t) * 2 * kHashCap : sizeof(uint32_t) * (size_t)n_rows;
-    void (*kern)(TraceParams);
-    if (hash)
-      kern = p.g.empty_dist ? k_form_factors<true, true> : k_form_factors<true, false>;
-    else
-      kern = p.g.empty_dist ? k_form_factors<false, true> : k_form_factors<false, false>;
+    void (*kern)(TraceParams) = p.g.empty_dist ? k_form_factors<true> : k_form_factors<false>;
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, smem));
-    const int blocks = std::max(1, std::min<int>(per_sm * c->n_sm, (int)chunks.size()));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
+    // persistent blocks: a full wave, fewer when there are fewer chunks than warps
+    const long long wave = (long long)std::max(per_sm, 1) * c->n_sm;
+    const long long by_work = ((long long)chunks.size() + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
     timing_begin(c);
-    kern<<<blocks, kTraceThreads, smem, c->stream>>>(p);
+    kern<<<blocks, kTraceThreads, 0, c->stream>>>(p);
     timing_end(c);
     FFB_CUDA(cudaGetLastError());
   }

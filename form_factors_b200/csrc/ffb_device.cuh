@@ -60,39 +60,72 @@ __device__ inline TriRec make_trirec(float3 p0, float3 p1, float3 p2)
 }
 
 // ---------------------------------------------------------------------------
-// The ray/triangle test of math/triangle.cpp:40-78 on a precomputed record.
-// o is the ray origin, dir = end - origin.  Returns true for
-// TRIANGLE_INTERSECTION_UNIQUE and writes the intersection point.
-// The first half (a, b, r) needs only q0 and q1; q2 and q3 are read only for
-// rays that reach the parametric test.
+// Division-free decisions that are exact for the reference's comparisons.
+// For q = num / den rounded to nearest:
+//  * q < 0 holds exactly when num and den have opposite signs, num != 0 and
+//    the quotient does not round to -0; |num| > |den| * 2^-100 rules out the
+//    underflow, so "surely negative" below implies q < 0.
+//  * q > 1 holds when num and den share a sign and |num| > |den| * (1 + 2^-20):
+//    the exact quotient then exceeds 1 by far more than half an ulp.
+// Anything not decided this way goes through the IEEE division.  NaN inputs
+// fail every comparison and always take the division path.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool tri_hit(const float4* __restrict__ rec, float3 o, float3 dir, float3& pt)
+__device__ __forceinline__ bool surely_negative(float num, float den)
 {
-  const float4 q0 = __ldg(rec + 0);
-  const float4 q1 = __ldg(rec + 1);
+  return ((num < 0.f) != (den < 0.f)) && num != 0.f && fabsf(num) > fabsf(den) * 0x1p-100f;
+}
+
+__device__ __forceinline__ bool surely_above_one(float num, float den)
+{
+  return ((num < 0.f) == (den < 0.f)) && fabsf(num) > fabsf(den) * 0x1.000010p+0f;
+}
+
+// ---------------------------------------------------------------------------
+// The ray/triangle test of math/triangle.cpp:40-78 on a precomputed record
+// held in registers.  o is the ray origin, dir = end - origin.  Returns true
+// for TRIANGLE_INTERSECTION_UNIQUE and writes the intersection point.  Every
+// value that decides the result is computed with the reference's operations
+// in the reference's order; the sign shortcuts above only skip divisions
+// whose outcome is already known.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool tri_hit_regs(const float4 q0, const float4 q1, const float4 q2, const float4 q3,
+                                             float3 o, float3 dir, float3& pt)
+{
   float3 w0 = f3(o.x - q0.x, o.y - q0.y, o.z - q0.z);
   float a = -(q1.x * w0.x + q1.y * w0.y + q1.z * w0.z);
   float b = q1.x * dir.x + q1.y * dir.y + q1.z * dir.z;
   if (fabsf(b) < FFB_EPS_ABOVE_1E8)
     return false;
+  if (surely_negative(a, b))  // r = a / b < 0
+    return false;
   float r = a / b;
   if (r < 0.f)
     return false;
   float3 p = f3(o.x + r * dir.x, o.y + r * dir.y, o.z + r * dir.z);
-  const float4 q2 = __ldg(rec + 2);
-  const float4 q3 = __ldg(rec + 3);
   float3 w = f3(p.x - q0.x, p.y - q0.y, p.z - q0.z);
   float wu = w.x * q2.x + w.y * q2.y + w.z * q2.z;
   float wv = w.x * q3.x + w.y * q3.y + w.z * q3.z;
   const float uu = q0.w, uv = q1.w, vv = q2.w, D = q3.w;
-  float s = (uv * wv - vv * wu) / D;
+  const float ns = uv * wv - vv * wu;
+  if (surely_negative(ns, D) || surely_above_one(ns, D))  // s < 0 || s > 1
+    return false;
+  const float nt = uv * wu - uu * wv;
+  if (surely_negative(nt, D))  // t < 0: rejected whatever s decides
+    return false;
+  float s = ns / D;
   if (s < 0.f || s > 1.f)
     return false;
-  float t = (uv * wu - uu * wv) / D;
+  float t = nt / D;
   if (t < 0.f || (s + t) > 1.f)
     return false;
   pt = p;
   return true;
+}
+
+// Same test on a record in memory (global or shared).
+__device__ __forceinline__ bool tri_hit(const float4* rec, float3 o, float3 dir, float3& pt)
+{
+  return tri_hit_regs(rec[0], rec[1], rec[2], rec[3], o, dir, pt);
 }
 
 // Squared distance of the reference caster (naive_cpu.cpp:83-84).
@@ -205,6 +238,7 @@ __device__ inline void rotate_towards(float3 s, float3 t, float* m)
 
 // Ray j of a face (emission/malley_cpu.cpp:159-184) with Philox draws keyed
 // by (seed, epoch, face, j).  Writes origin o and end point e.
+// fr points at the face's 20-float frame in global memory.
 __device__ __forceinline__ void emit_ray(const float* __restrict__ fr, uint32_t face, uint32_t j, int front,
                                          uint32_t key0, uint32_t key1, uint32_t epoch, float3& o, float3& e)
 {
@@ -215,9 +249,9 @@ __device__ __forceinline__ void emit_ray(const float* __restrict__ fr, uint32_t 
     a = 1.f - a;
     b = 1.f - b;
   }
-  float3 p0 = f3(fr[0], fr[1], fr[2]);
-  float3 e1 = f3(fr[3], fr[4], fr[5]);
-  float3 e2 = f3(fr[6], fr[7], fr[8]);
+  float3 p0 = f3(__ldg(fr + 0), __ldg(fr + 1), __ldg(fr + 2));
+  float3 e1 = f3(__ldg(fr + 3), __ldg(fr + 4), __ldg(fr + 5));
+  float3 e2 = f3(__ldg(fr + 6), __ldg(fr + 7), __ldg(fr + 8));
   float3 origin = add3(add3(p0, mul3(e1, a)), mul3(e2, b));
   float r = u01(x.z);
   float rad = sqrtf(r);
@@ -226,7 +260,10 @@ __device__ __forceinline__ void emit_ray(const float* __restrict__ fr, uint32_t 
   float3 mv = f3(rad * cphi, rad * sphi, sqrtf(1.f - r));
   if ((int)j >= front)
     mv.z = -mv.z;
-  const float* m = fr + 9;
+  float m[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+    m[k] = __ldg(fr + 9 + k);
   float3 d = f3((m[0] * mv.x + m[3] * mv.y) + m[6] * mv.z,
                 (m[1] * mv.x + m[4] * mv.y) + m[7] * mv.z,
                 (m[2] * mv.x + m[5] * mv.y) + m[8] * mv.z);

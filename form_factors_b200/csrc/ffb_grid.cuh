@@ -29,7 +29,7 @@ struct GridView {
   float slack;          // 2 * margin, world units
   const uint32_t* __restrict__ cell_start;  // ncells + 1
   const int32_t* __restrict__ ref_tri;      // triangle index per reference
-  const TriRec* __restrict__ tri;           // triangle records
+  const TriRec* __restrict__ ref_rec;       // triangle record per reference (a copy of tri[ref_tri[i]])
   const uint8_t* __restrict__ empty_dist;   // Chebyshev distance to the nearest occupied cell, or null
 };
 
@@ -238,6 +238,15 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ cell_start, int n_cells
   }
 }
 
+// Per-reference copy of the triangle records: a cell's candidates are
+// contiguous and a test needs no index load before its record.
+__global__ void k_ref_gather(const int32_t* __restrict__ ref_tri, uint32_t n_refs, const TriRec* __restrict__ tri,
+                             TriRec* __restrict__ ref_rec)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_refs; i += gridDim.x * blockDim.x)
+    ref_rec[i] = tri[ref_tri[i]];
+}
+
 // ---------------------------------------------------------------------------
 // Exclusive scan of uint32 counts (n + 1 outputs, out[n] = total) in three
 // passes: per-block sums, a single-block scan of the sums, per-block scan.
@@ -394,130 +403,225 @@ __device__ __forceinline__ float boundary_t(float lo, int edge, float cs, float 
   return t == t ? t : INFINITY;
 }
 
-template <bool kSkip>
-__device__ __forceinline__ int trace_grid(const GridView& g, float3 o, float3 e, float3& hit_pt, uint32_t& n_tests,
-                                          uint32_t& n_cells)
+// Slab clip of the ray o + t*d, t >= 0, against [lo, hi] on one axis.
+__device__ __forceinline__ bool slab(float d, float o, float lo, float hi, float& inv, float& t0, float& t1)
 {
-  const float3 dir = sub3(e, o);
-  float t0 = 0.f, t1 = INFINITY;
-  float inv[3];
-  const float oo[3] = {o.x, o.y, o.z};
-  const float dd[3] = {dir.x, dir.y, dir.z};
-  const float lo[3] = {g.lo.x, g.lo.y, g.lo.z};
-  const float hi[3] = {g.hi.x, g.hi.y, g.hi.z};
+  if (d == 0.f) {
+    inv = INFINITY;
+    return o >= lo && o <= hi;
+  }
+  inv = 1.f / d;
+  const float ta = (lo - o) * inv, tb = (hi - o) * inv;
+  t0 = fmaxf(t0, fminf(ta, tb));
+  t1 = fminf(t1, fmaxf(ta, tb));
+  return true;
+}
+
+__device__ __forceinline__ int cell_of(float p, float lo, float ics, int n)
+{
+  return min(max((int)floorf((p - lo) * ics), 0), n - 1);
+}
+
+__device__ __forceinline__ int sgn(float d) { return d > 0.f ? 1 : (d < 0.f ? -1 : 0); }
+
+// Next boundary parameter on an axis for cell c and step s (inf when s == 0).
+__device__ __forceinline__ float next_t(int s, int c, float lo, float cs, float o, float inv)
+{
+  return s == 0 ? INFINITY : boundary_t(lo, c + (s > 0), cs, o, inv);
+}
+
+// Landing cell on one axis after a jump to parameter tj: never against the
+// ray, never beyond the empty cube of half-width `jump`.
+__device__ __forceinline__ int land(int s, int c, int jump, float o, float d, float tj, float lo, float ics)
+{
+  if (s == 0)
+    return c;
+  const int ci = (int)floorf(((o + tj * d) - lo) * ics);
+  return s > 0 ? min(max(ci, c), c + jump) : max(min(ci, c), c - jump);
+}
+
+// ---------------------------------------------------------------------------
+// Nearest hit through the grid as a per-lane state machine.  One call does
+// one unit of work: test one triangle reference of the current cell, or (when
+// the cell is exhausted) decide termination and move to the next cell or jump
+// over empty space.  Lanes of a warp stay in step whatever the cell
+// occupancy, and a lane whose ray finishes can start another ray at once
+// (persistent refill).
+//
+// Stopping rule: after a cell, stop when the best squared distance is below
+// the squared distance at which the ray leaves that cell, reduced by twice
+// the binning margin; any triangle not yet tested lies in unvisited cells and
+// cannot compute a smaller distance.
+// ---------------------------------------------------------------------------
+#ifndef FFB_MAILBOX
+#define FFB_MAILBOX 0
+#endif
+
+struct Tracer {
+  float3 o, dir, inv;
+  float t1, dlen, best;
+  float tnx, tny, tnz;
+  float3 best_pt;
+  int cx, cy, cz;
+  int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
+  int jump;          // empty-space distance of the current cell
+  uint32_t i, en;    // pending references of the current cell
+  int iters;         // cells left before the hard stop
+#if FFB_MAILBOX > 0
+  int mb[FFB_MAILBOX];  // faces tested most recently (a face repeats in neighbouring cells)
+#endif
+};
+
+template <bool kSkip>
+__device__ __forceinline__ void tracer_enter(Tracer& T, const GridView& g)
+{
+  const int cell = (T.cz * g.ny + T.cy) * g.nx + T.cx;
+  T.jump = kSkip ? (int)__ldg(g.empty_dist + cell) : 0;
+  if (T.jump == 0) {
+    T.i = __ldg(g.cell_start + cell);
+    T.en = __ldg(g.cell_start + cell + 1);
+  } else {
+    T.i = T.en = 0;
+  }
+}
+
+// Sets up a ray; false when it misses the grid box (no hit possible).
+template <bool kSkip>
+__device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float3 o, float3 e, uint32_t& n_cells)
+{
+  T.o = o;
+  T.dir = sub3(e, o);
+  float t0 = 0.f;
+  T.t1 = INFINITY;
+  if (!slab(T.dir.x, o.x, g.lo.x, g.hi.x, T.inv.x, t0, T.t1) || !slab(T.dir.y, o.y, g.lo.y, g.hi.y, T.inv.y, t0, T.t1) ||
+      !slab(T.dir.z, o.z, g.lo.z, g.hi.z, T.inv.z, t0, T.t1) || !(t0 <= T.t1))
+    return false;
+  T.cx = cell_of(o.x + t0 * T.dir.x, g.lo.x, g.inv_cs.x, g.nx);
+  T.cy = cell_of(o.y + t0 * T.dir.y, g.lo.y, g.inv_cs.y, g.ny);
+  T.cz = cell_of(o.z + t0 * T.dir.z, g.lo.z, g.inv_cs.z, g.nz);
+  T.tnx = next_t(sgn(T.dir.x), T.cx, g.lo.x, g.cs.x, o.x, T.inv.x);
+  T.tny = next_t(sgn(T.dir.y), T.cy, g.lo.y, g.cs.y, o.y, T.inv.y);
+  T.tnz = next_t(sgn(T.dir.z), T.cz, g.lo.z, g.cs.z, o.z, T.inv.z);
+  T.dlen = sqrtf(dot3(T.dir, T.dir));
+  T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
+  T.best_ref = -1;
+  T.iters = g.nx + g.ny + g.nz + 3;
+#if FFB_MAILBOX > 0
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (dd[a] == 0.f) {
-      inv[a] = INFINITY;
-      if (!(oo[a] >= lo[a] && oo[a] <= hi[a]))
-        return -1;
-    } else {
-      inv[a] = 1.f / dd[a];
-      float ta = (lo[a] - oo[a]) * inv[a], tb = (hi[a] - oo[a]) * inv[a];
-      t0 = fmaxf(t0, fminf(ta, tb));
-      t1 = fminf(t1, fmaxf(ta, tb));
+  for (int k = 0; k < FFB_MAILBOX; ++k)
+    T.mb[k] = -1;
+#endif
+  ++n_cells;
+  tracer_enter<kSkip>(T, g);
+  return true;
+}
+
+// Tests the next pending reference of the current cell and merges a hit
+// into (best, best_ref, best_pt): the smallest squared distance wins and,
+// among equal distances, the lowest face index, which equals the reference's
+// strict '<' scan in index order.
+__device__ __forceinline__ void tracer_test(Tracer& T, const GridView& g, uint32_t& n_tests)
+{
+  const uint32_t i = T.i++;
+#if FFB_MAILBOX > 0
+  const int f = __ldg(g.ref_tri + i);
+  bool seen = false;
+#pragma unroll
+  for (int k = 0; k < FFB_MAILBOX; ++k)
+    seen |= T.mb[k] == f;
+  if (seen)
+    return;  // same face, same ray: the same test result as before
+#pragma unroll
+  for (int k = FFB_MAILBOX - 1; k > 0; --k)
+    T.mb[k] = T.mb[k - 1];
+  T.mb[0] = f;
+#endif
+  ++n_tests;
+  const float4* rec = reinterpret_cast<const float4*>(g.ref_rec + i);
+  float3 pt;
+  if (tri_hit_regs(__ldg(rec), __ldg(rec + 1), __ldg(rec + 2), __ldg(rec + 3), T.o, T.dir, pt)) {
+    const float d = dist2(pt, T.o);
+    if (d < T.best) {
+      T.best = d;
+      T.best_ref = (int)i;
+      T.best_pt = pt;
+    } else if (d == T.best && T.best_ref >= 0) {
+      // equal distance: the lower face index wins (a repeated reference of
+      // the same face compares equal and changes nothing)
+      if (__ldg(g.ref_tri + i) < __ldg(g.ref_tri + T.best_ref)) {
+        T.best_ref = (int)i;
+        T.best_pt = pt;
+      }
     }
   }
-  if (!(t0 <= t1))
-    return -1;
-  const float cs[3] = {g.cs.x, g.cs.y, g.cs.z};
-  const float ics[3] = {g.inv_cs.x, g.inv_cs.y, g.inv_cs.z};
-  const int nn[3] = {g.nx, g.ny, g.nz};
-  int c[3], st[3];
-  float tn[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float p = oo[a] + t0 * dd[a];
-    int ci = (int)floorf((p - lo[a]) * ics[a]);
-    c[a] = min(max(ci, 0), nn[a] - 1);
-    st[a] = dd[a] > 0.f ? 1 : (dd[a] < 0.f ? -1 : 0);
-    tn[a] = st[a] == 0 ? INFINITY : boundary_t(lo[a], c[a] + (st[a] > 0), cs[a], oo[a], inv[a]);
+}
+
+// Face index of the finished ray's nearest hit, or -1.
+__device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
+{
+  return T.best_ref >= 0 ? __ldg(g.ref_tri + T.best_ref) : -1;
+}
+
+// The current cell is exhausted: stop, or move to the next cell.  Returns
+// false when the ray is finished.
+template <bool kSkip>
+__device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells)
+{
+  const float tx = fminf(fminf(T.tnx, T.tny), T.tnz);
+  if (T.best_ref >= 0) {
+    const float L = fminf(tx, T.t1) * T.dlen - g.slack;
+    if (L > 0.f && T.best < L * L)
+      return false;
   }
-  const float dlen = sqrtf(dot3(dir, dir));
-  float best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
-  int best_idx = -1;
-  float3 best_pt = f3(0.f, 0.f, 0.f);
-  const int max_iter = g.nx + g.ny + g.nz + 4;
-  for (int it = 0; it < max_iter; ++it) {
-    const int cell = (c[2] * g.ny + c[1]) * g.nx + c[0];
-    ++n_cells;
-    int jump = 0;
-    if (kSkip)
-      jump = g.empty_dist[cell];
-    if (!kSkip || jump == 0) {
-      const uint32_t b = g.cell_start[cell], en = g.cell_start[cell + 1];
-      for (uint32_t i = b; i < en; ++i) {
-        const int f = g.ref_tri[i];
-        float3 pt;
-        ++n_tests;
-        if (tri_hit(reinterpret_cast<const float4*>(g.tri + f), o, dir, pt)) {
-          const float d = dist2(pt, o);
-          if (d < best || (d == best && f < best_idx)) {
-            best = d;
-            best_idx = f;
-            best_pt = pt;
-          }
-        }
-      }
+  if (!(tx < T.t1) || --T.iters <= 0)
+    return false;
+  const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
+  if (kSkip && T.jump >= 2) {
+    // every cell within Chebyshev distance jump-1 is empty: leave that cube
+    const int jump = T.jump;
+    float tj = INFINITY;
+    if (sx) tj = fminf(tj, boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x));
+    if (sy) tj = fminf(tj, boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y));
+    if (sz) tj = fminf(tj, boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z));
+    if (!(tj < T.t1))
+      return false;
+    const int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
+    const int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
+    const int nz = land(sz, T.cz, jump, T.o.z, T.dir.z, tj, g.lo.z, g.inv_cs.z);
+    if (nx != T.cx || ny != T.cy || nz != T.cz) {
+      T.cx = nx;
+      T.cy = ny;
+      T.cz = nz;
+      if ((unsigned)nx >= (unsigned)g.nx || (unsigned)ny >= (unsigned)g.ny || (unsigned)nz >= (unsigned)g.nz)
+        return false;
+      T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
+      T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
+      T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
+      ++n_cells;
+      tracer_enter<kSkip>(T, g);
+      return true;
     }
-    const float tx = fminf(fminf(tn[0], tn[1]), tn[2]);
-    if (best_idx >= 0) {
-      const float L = fminf(tx, t1) * dlen - g.slack;
-      if (L > 0.f && best < L * L)
-        break;
-    }
-    if (!(tx < t1))
-      break;
-    if (kSkip && jump >= 2) {
-      // every cell within Chebyshev distance jump-1 is empty: leave that cube
-      float tj = INFINITY;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        if (st[a] != 0) {
-          int edge = st[a] > 0 ? c[a] + jump : c[a] - jump + 1;
-          tj = fminf(tj, boundary_t(lo[a], edge, cs[a], oo[a], inv[a]));
-        }
-      }
-      if (!(tj < t1))
-        break;
-      int nc[3];
-      bool moved = false;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        float p = oo[a] + tj * dd[a];
-        int ci = (int)floorf((p - lo[a]) * ics[a]);
-        // never move against the ray or beyond the cube
-        if (st[a] > 0) ci = min(max(ci, c[a]), c[a] + jump);
-        else if (st[a] < 0) ci = max(min(ci, c[a]), c[a] - jump);
-        else ci = c[a];
-        nc[a] = ci;
-        moved |= ci != c[a];
-      }
-      if (moved) {
-        bool out = false;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          c[a] = nc[a];
-          out |= c[a] < 0 || c[a] >= nn[a];
-          tn[a] = st[a] == 0 ? INFINITY : boundary_t(lo[a], c[a] + (st[a] > 0), cs[a], oo[a], inv[a]);
-        }
-        if (out)
-          break;
-        continue;
-      }
-    }
-    // one DDA step along the axis whose boundary comes first
-    int a = (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2);
-    if (st[a] == 0)
-      break;
-    c[a] += st[a];
-    if (c[a] < 0 || c[a] >= nn[a])
-      break;
-    tn[a] = boundary_t(lo[a], c[a] + (st[a] > 0), cs[a], oo[a], inv[a]);
   }
-  if (best_idx >= 0)
-    hit_pt = best_pt;
-  return best_idx;
+  // one DDA step along the axis whose boundary comes first
+  if (T.tnx <= T.tny && T.tnx <= T.tnz) {
+    T.cx += sx;
+    if ((unsigned)T.cx >= (unsigned)g.nx)
+      return false;
+    T.tnx = next_t(sx, T.cx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
+  } else if (T.tny <= T.tnz) {
+    T.cy += sy;
+    if ((unsigned)T.cy >= (unsigned)g.ny)
+      return false;
+    T.tny = next_t(sy, T.cy, g.lo.y, g.cs.y, T.o.y, T.inv.y);
+  } else {
+    T.cz += sz;
+    if ((unsigned)T.cz >= (unsigned)g.nz)
+      return false;
+    T.tnz = next_t(sz, T.cz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
+  }
+  ++n_cells;
+  tracer_enter<kSkip>(T, g);
+  return true;
 }
 
 }  // namespace ffb

@@ -1,6 +1,6 @@
 // ffb_trace.cuh -- the hot kernels: fused emission + nearest-hit trace +
-// per-source histogram (form-factor counts), ray-batch casts (grid and brute
-// force) and ray materialisation.
+// per-(source, hit) histogram (form-factor counts), ray-batch casts (grid and
+// brute force) and ray materialisation.
 #pragma once
 
 #include "ffb_grid.cuh"
@@ -16,7 +16,7 @@ struct Chunk {
   int32_t front;
 };
 
-// Statistics slots (uint64 each), accumulated once per block.
+// Statistics slots (uint64 each), accumulated once per warp.
 enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatSlots = 4 };
 
 struct TraceParams {
@@ -30,13 +30,22 @@ struct TraceParams {
   uint32_t key0, key1, epoch;
   uint32_t* __restrict__ chunk_cursor;        // work counter, zero before the launch
   unsigned long long* __restrict__ stats;     // kStatSlots, or null
-  int hash_cap;                               // hash mode: slots (power of two)
 };
 
 constexpr int kTraceThreads = 128;
+constexpr int kWarpsPerBlock = kTraceThreads / 32;
+// Blocks per SM the trace kernels are compiled for: 8 blocks of 128 threads
+// cap registers at 64 per thread (32 warps per SM to hide L1/L2 latency).
+#ifndef FFB_MIN_BLOCKS
+#define FFB_MIN_BLOCKS 8
+#endif
+constexpr int kWarpHashLog2 = 9;
+constexpr int kWarpHash = 1 << kWarpHashLog2;  // histogram slots per warp
+constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
 
-__device__ __forceinline__ void block_stats(unsigned long long* stats, uint32_t tests, uint32_t cells,
-                                            uint32_t rays, uint32_t hits)
+__device__ __forceinline__ void warp_stats(unsigned long long* stats, uint32_t tests, uint32_t cells, uint32_t rays,
+                                           uint32_t hits)
 {
   if (!stats)
     return;
@@ -45,128 +54,166 @@ __device__ __forceinline__ void block_stats(unsigned long long* stats, uint32_t 
   for (int k = 0; k < 4; ++k) {
     unsigned long long x = v[k];
     for (int o = 16; o > 0; o >>= 1)
-      x += __shfl_xor_sync(0xffffffffu, x, o);
+      x += __shfl_xor_sync(kFull, x, o);
     if ((threadIdx.x & 31) == 0 && x)
       atomicAdd(stats + k, x);
   }
 }
 
-__device__ __forceinline__ uint32_t hash_slot(int key, int cap)
+// Adds 1 to the bin of `key` in a warp's open-addressing table.  Returns true
+// when the key took a new slot.  Keys are matrix indices row * n_cols + col.
+__device__ __forceinline__ bool warp_hash_add(uint32_t* keys, uint32_t* vals, uint32_t key, uint32_t* counts)
 {
-  return ((uint32_t)key * 2654435761u) & (uint32_t)(cap - 1);
+  uint32_t s = (key * 2654435761u) >> (32 - kWarpHashLog2);
+  volatile uint32_t* vk = keys;
+  for (int probe = 0; probe < kWarpHash; ++probe) {
+    uint32_t cur = vk[s];
+    if (cur == kEmptyKey) {
+      cur = atomicCAS(keys + s, kEmptyKey, key);
+      if (cur == kEmptyKey) {
+        atomicAdd(vals + s, 1u);
+        return true;
+      }
+    }
+    if (cur == key) {
+      atomicAdd(vals + s, 1u);
+      return false;
+    }
+    s = (s + 1) & (kWarpHash - 1);
+  }
+  atomicAdd(counts + key, 1u);  // full table; unreachable: flushed at half load
+  return false;
+}
+
+// Adds every occupied bin of a warp's table to the global matrix and clears it.
+__device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, uint32_t* counts, int lane)
+{
+  __syncwarp();
+  for (int i = lane; i < kWarpHash; i += 32) {
+    const uint32_t k = keys[i];
+    if (k != kEmptyKey) {
+      atomicAdd(counts + k, vals[i]);
+      keys[i] = kEmptyKey;
+      vals[i] = 0;
+    }
+  }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
-// Fused form-factor kernel.  Persistent blocks take chunks from a global
-// cursor.  For each chunk the block generates its rays (Philox, keyed by
-// seed/epoch/face/j), traces them through the grid and counts hit columns in
-// a shared-memory histogram of the chunk's source row, then flushes the
-// non-zero bins to the global uint32 matrix with atomic adds (several chunks
-// may share a row).  kHash selects an open-addressing table (keys = column)
-// for matrices too wide for a dense shared-memory row.
+// Fused form-factor kernel.  Persistent warps, no block barriers.  Each warp
+// keeps a current chunk (consecutive rays of one face) and hands its rays to
+// lanes as they fall idle (one ballot per refill, one global atomic per
+// chunk), so a warp may hold rays of several faces at once.  Each lane runs
+// the grid traversal state machine one unit of work per iteration.  A finished
+// hit adds one to the warp's shared-memory hash histogram keyed by the matrix
+// index row(f) * n_cols + row(h); the warp flushes the table to the global
+// uint32 matrix with atomic adds when it is half full and at the end.
 // ---------------------------------------------------------------------------
-template <bool kHash, bool kSkip>
-__global__ void __launch_bounds__(kTraceThreads) k_form_factors(TraceParams p)
+template <bool kSkip>
+__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(TraceParams p)
 {
-  extern __shared__ uint32_t smem[];
-  __shared__ int s_chunk;
-  uint32_t* hist = smem;                                  // dense: n_cols bins
-  int* keys = reinterpret_cast<int*>(smem);               // hash: hash_cap keys
-  uint32_t* vals = smem + (kHash ? p.hash_cap : 0);       // hash: hash_cap values
-  const int bins = kHash ? p.hash_cap : p.n_cols;
-  for (int i = threadIdx.x; i < bins; i += blockDim.x) {
-    if (kHash) {
-      keys[i] = -1;
-      vals[i] = 0;
-    } else {
-      hist[i] = 0;
-    }
+  __shared__ uint32_t s_keys[kWarpsPerBlock][kWarpHash];
+  __shared__ uint32_t s_vals[kWarpsPerBlock][kWarpHash];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* keys = s_keys[warp];
+  uint32_t* vals = s_vals[warp];
+  for (int i = lane; i < kWarpHash; i += 32) {
+    keys[i] = kEmptyKey;
+    vals[i] = 0;
   }
+  __syncwarp();
+  const unsigned lane_below = (1u << lane) - 1u;
+  int fill = 0;  // occupied slots (warp-uniform)
+  // current chunk (warp-uniform)
+  int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0;
+  bool exhausted = false;
+  // lane state
+  Tracer T;
+  bool active = false;
+  int my_row = 0;
   uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0;
   for (;;) {
-    if (threadIdx.x == 0)
-      s_chunk = (int)atomicAdd(p.chunk_cursor, 1u);
-    __syncthreads();
-    const int k = s_chunk;
-    if (k >= p.n_chunks)
+    unsigned need = __ballot_sync(kFull, !active);
+    while (need && !exhausted) {
+      if (c_left == 0) {
+        int k = 0;
+        if (lane == 0)
+          k = (int)atomicAdd(p.chunk_cursor, 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= p.n_chunks) {
+          exhausted = true;
+          break;
+        }
+        const Chunk ch = p.chunks[k];
+        c_face = ch.face;
+        c_j = ch.j0;
+        c_left = ch.count;
+        c_front = ch.front;
+        c_row = p.face_to_row ? __ldg(p.face_to_row + ch.face) : ch.face;
+      }
+      const int take = min(__popc(need), c_left);
+      const int rank = __popc(need & lane_below);
+      const bool mine = ((need >> lane) & 1u) && rank < take;
+      if (mine) {
+        float3 o, e;
+        emit_ray(p.frames + 20 * (size_t)c_face, (uint32_t)c_face, (uint32_t)(c_j + rank), c_front, p.key0, p.key1,
+                 p.epoch, o, e);
+        ++n_rays;
+        my_row = c_row;
+        active = tracer_begin<kSkip>(T, p.g, o, e, n_cells);
+      }
+      need &= ~__ballot_sync(kFull, mine);
+      c_j += take;
+      c_left -= take;
+    }
+    if (exhausted && !__any_sync(kFull, active))
       break;
-    const Chunk ch = p.chunks[k];
-    const float* fr = p.frames + 20 * (size_t)ch.face;
-    float frame[18];
-#pragma unroll
-    for (int e = 0; e < 18; ++e)
-      frame[e] = __ldg(fr + e);
-    const int row = p.face_to_row ? __ldg(p.face_to_row + ch.face) : ch.face;
-    for (int j = ch.j0 + threadIdx.x; j < ch.j0 + ch.count; j += blockDim.x) {
-      float3 o, e;
-      emit_ray(frame, (uint32_t)ch.face, (uint32_t)j, ch.front, p.key0, p.key1, p.epoch, o, e);
-      float3 pt;
-      const int h = trace_grid<kSkip>(p.g, o, e, pt, n_tests, n_cells);
-      ++n_rays;
-      if (h >= 0) {
-        ++n_hits;
-        const int col = p.face_to_row ? __ldg(p.face_to_row + h) : h;
-        if (!kHash) {
-          atomicAdd(hist + col, 1u);
-        } else {
-          uint32_t s = hash_slot(col, p.hash_cap);
-          bool done = false;
-          for (int probe = 0; probe < p.hash_cap; ++probe) {
-            int cur = keys[s];
-            if (cur == -1)
-              cur = atomicCAS(keys + s, -1, col);
-            if (cur == -1 || cur == col) {
-              atomicAdd(vals + s, 1u);
-              done = true;
-              break;
-            }
-            s = (s + 1) & (uint32_t)(p.hash_cap - 1);
-          }
-          if (!done)  // table full (not reachable with cap >= 2 * chunk rays)
-            atomicAdd(p.counts + (size_t)row * p.n_cols + col, 1u);
-        }
+    int hit = -1;
+    if (active) {
+      if (T.i < T.en) {
+        tracer_test(T, p.g, n_tests);
+      } else if (!tracer_advance<kSkip>(T, p.g, n_cells)) {
+        active = false;
+        hit = tracer_result(T, p.g);
       }
     }
-    __syncthreads();
-    uint32_t* out_row = p.counts + (size_t)row * p.n_cols;
-    for (int i = threadIdx.x; i < bins; i += blockDim.x) {
-      if (kHash) {
-        const int key = keys[i];
-        if (key >= 0) {
-          atomicAdd(out_row + key, vals[i]);
-          keys[i] = -1;
-          vals[i] = 0;
-        }
-      } else {
-        const uint32_t v = hist[i];
-        if (v) {
-          atomicAdd(out_row + i, v);
-          hist[i] = 0;
-        }
-      }
+    bool fresh = false;
+    if (hit >= 0) {
+      ++n_hits;
+      const int col = p.face_to_row ? __ldg(p.face_to_row + hit) : hit;
+      fresh = warp_hash_add(keys, vals, (uint32_t)my_row * (uint32_t)p.n_cols + (uint32_t)col, p.counts);
     }
-    __syncthreads();
+    fill += __popc(__ballot_sync(kFull, fresh));
+    if (fill > kWarpHash / 2) {
+      warp_hash_flush(keys, vals, p.counts, lane);
+      fill = 0;
+    }
   }
-  block_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
+  warp_hash_flush(keys, vals, p.counts, lane);
+  warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
 }
 
 // ---------------------------------------------------------------------------
 // Ray-batch cast through the grid (the ray_caster interface): rays are
 // {origin, end point} as in math::ray_t.  hit_face gets the face index or -1;
-// hit_point (optional) gets the point, NaN for a miss.
+// hit_point (optional) gets the point, NaN for a miss.  Persistent warps take
+// rays from a global cursor (one atomic per refill) as lanes fall idle.
 // ---------------------------------------------------------------------------
 template <bool kSkip>
-__global__ void __launch_bounds__(kTraceThreads) k_cast(GridView g, const float* __restrict__ rays6, long n_rays,
-                                                         int32_t* __restrict__ hit_face, float* __restrict__ hit_point,
-                                                         unsigned long long* __restrict__ stats)
+__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
+    k_cast(GridView g, const float* __restrict__ rays6, long n_rays, int32_t* __restrict__ hit_face,
+           float* __restrict__ hit_point, unsigned long long* __restrict__ stats,
+           unsigned long long* __restrict__ cursor)
 {
+  const int lane = threadIdx.x & 31;
+  const unsigned lane_below = (1u << lane) - 1u;
   uint32_t n_tests = 0, n_cells = 0, n_done = 0, n_hits = 0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_rays; i += (long)gridDim.x * blockDim.x) {
-    const float* r = rays6 + 6 * i;
-    const float3 o = f3(__ldg(r + 0), __ldg(r + 1), __ldg(r + 2));
-    const float3 e = f3(__ldg(r + 3), __ldg(r + 4), __ldg(r + 5));
-    float3 pt = f3(NAN, NAN, NAN);
-    const int h = trace_grid<kSkip>(g, o, e, pt, n_tests, n_cells);
+  Tracer T;
+  bool active = false;
+  long id = -1;
+  bool exhausted = false;
+  auto finish = [&](long i, int h, float3 pt) {
     hit_face[i] = h;
     if (hit_point) {
       if (h < 0)
@@ -177,12 +224,46 @@ __global__ void __launch_bounds__(kTraceThreads) k_cast(GridView g, const float*
     }
     ++n_done;
     n_hits += h >= 0;
+  };
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !active);
+    if (need && !exhausted) {
+      unsigned long long base = 0;
+      if (lane == 0)
+        base = atomicAdd(cursor, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= (unsigned long long)n_rays)
+        exhausted = true;
+      if ((need >> lane) & 1u) {
+        const unsigned long long r = base + __popc(need & lane_below);
+        if (r < (unsigned long long)n_rays) {
+          id = (long)r;
+          const float* q = rays6 + 6 * r;
+          const float3 o = f3(__ldg(q + 0), __ldg(q + 1), __ldg(q + 2));
+          const float3 e = f3(__ldg(q + 3), __ldg(q + 4), __ldg(q + 5));
+          active = tracer_begin<kSkip>(T, g, o, e, n_cells);
+          if (!active)
+            finish(id, -1, o);
+        }
+      }
+    }
+    if (exhausted && !__any_sync(kFull, active))
+      break;
+    if (active) {
+      if (T.i < T.en) {
+        tracer_test(T, g, n_tests);
+      } else if (!tracer_advance<kSkip>(T, g, n_cells)) {
+        active = false;
+        finish(id, tracer_result(T, g), T.best_pt);
+      }
+    }
   }
-  block_stats(stats, n_tests, n_cells, n_done, n_hits);
+  warp_stats(stats, n_tests, n_cells, n_done, n_hits);
 }
 
 // Brute force: every ray against every face (the naive_cpu definition),
-// faces staged through shared memory in tiles.
+// faces staged through shared memory in tiles, in index order with a strict
+// '<' as the reference scans them.
 constexpr int kBruteTile = 128;
 
 __global__ void __launch_bounds__(kTraceThreads) k_cast_brute(const TriRec* __restrict__ tri, int n_faces,
@@ -212,33 +293,13 @@ __global__ void __launch_bounds__(kTraceThreads) k_cast_brute(const TriRec* __re
     if (live) {
       for (int k = 0; k < m; ++k) {
         float3 pt;
-        const float4* rec = reinterpret_cast<const float4*>(tile + k);
-        // shared-memory copy of tri_hit (no __ldg on shared memory)
-        const float4 q0 = rec[0], q1 = rec[1];
-        float3 w0 = f3(o.x - q0.x, o.y - q0.y, o.z - q0.z);
-        float a = -(q1.x * w0.x + q1.y * w0.y + q1.z * w0.z);
-        float b = q1.x * dir.x + q1.y * dir.y + q1.z * dir.z;
-        if (fabsf(b) < FFB_EPS_ABOVE_1E8)
-          continue;
-        float r = a / b;
-        if (r < 0.f)
-          continue;
-        pt = f3(o.x + r * dir.x, o.y + r * dir.y, o.z + r * dir.z);
-        const float4 q2 = rec[2], q3 = rec[3];
-        float3 w = f3(pt.x - q0.x, pt.y - q0.y, pt.z - q0.z);
-        float wu = w.x * q2.x + w.y * q2.y + w.z * q2.z;
-        float wv = w.x * q3.x + w.y * q3.y + w.z * q3.z;
-        float s = (q1.w * wv - q2.w * wu) / q3.w;
-        if (s < 0.f || s > 1.f)
-          continue;
-        float t = (q1.w * wu - q0.w * wv) / q3.w;
-        if (t < 0.f || (s + t) > 1.f)
-          continue;
-        const float d = dist2(pt, o);
-        if (d < best) {  // faces arrive in index order: strict '<' as the reference
-          best = d;
-          best_idx = base + k;
-          best_pt = pt;
+        if (tri_hit(reinterpret_cast<const float4*>(tile + k), o, dir, pt)) {
+          const float d = dist2(pt, o);
+          if (d < best) {
+            best = d;
+            best_idx = base + k;
+            best_pt = pt;
+          }
         }
       }
     }
@@ -263,7 +324,7 @@ __global__ void k_emit(const float* __restrict__ frames, const long long* __rest
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_rays; i += (long)gridDim.x * blockDim.x) {
     int lo = 0, hi = n_faces;  // largest f with ray_offsets[f] <= i
     while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
+      const int mid = (lo + hi) >> 1;
       if (ray_offsets[mid] <= i)
         lo = mid;
       else
@@ -271,12 +332,8 @@ __global__ void k_emit(const float* __restrict__ frames, const long long* __rest
     }
     const int f = lo;
     const uint32_t j = (uint32_t)(i - ray_offsets[f]);
-    float frame[18];
-#pragma unroll
-    for (int e = 0; e < 18; ++e)
-      frame[e] = __ldg(frames + 20 * (size_t)f + e);
     float3 o, e;
-    emit_ray(frame, (uint32_t)f, j, front[f], key0, key1, epoch, o, e);
+    emit_ray(frames + 20 * (size_t)f, (uint32_t)f, j, front[f], key0, key1, epoch, o, e);
     float* r = rays6 + 6 * i;
     r[0] = o.x; r[1] = o.y; r[2] = o.z;
     r[3] = e.x; r[4] = e.y; r[5] = e.z;

@@ -143,7 +143,11 @@ class Context:
         return self._h
 
     def set_stream(self, stream_ptr):
-        _check(self._lib.ffb_ctx_set_stream(self._h, stream_ptr))
+        """Use a cudaStream_t (an int address); 0/None restores the context's own stream."""
+        _check(self._lib.ffb_ctx_set_stream(self._h, stream_ptr or None))
+
+    def stream_ptr(self):
+        return int(self._lib.ffb_ctx_stream(self._h) or 0)
 
     def set_budget(self, nbytes):
         _check(self._lib.ffb_ctx_set_budget(self._h, int(nbytes)))

@@ -20,6 +20,8 @@
 #include "math/triangle.h"
 #include "math/mat.h"
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstdlib>
@@ -53,25 +55,33 @@ namespace
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   }
 
-  // Casts rays [0, n) of `task` on `n_threads` threads over disjoint slices
-  // (the reference casters keep no per-cast state, so slices are independent).
+  // Casts rays [0, n) of `task` on `n_threads` threads that take slices of
+  // 2048 rays from a shared cursor (the reference casters keep no per-cast
+  // state, so slices are independent; dynamic slices keep every core busy
+  // when ray cost varies across the batch).
   int cast_threads(ray_caster::system_t* sys, ray_caster::task_t* task, int n_threads)
   {
     if (n_threads <= 1)
       return ray_caster::system_cast(sys, task);
-    std::vector<std::thread> pool;
-    std::vector<int> rc(n_threads, 0);
     const long n = task->n_tasks;
+    const long slice = 2048;
+    std::atomic<long> cursor(0);
+    std::atomic<int> status(0);
+    std::vector<std::thread> pool;
     for (int t = 0; t < n_threads; ++t) {
-      long b = n * t / n_threads, e = n * (t + 1) / n_threads;
-      pool.emplace_back([=, &rc]() {
-        ray_caster::task_t sub = {(int)(e - b), task->ray + b, task->hit_face + b, task->hit_point + b};
-        rc[t] = ray_caster::system_cast(sys, &sub);
+      pool.emplace_back([&]() {
+        for (;;) {
+          long b = cursor.fetch_add(slice);
+          if (b >= n) break;
+          long e = std::min(n, b + slice);
+          ray_caster::task_t sub = {(int)(e - b), task->ray + b, task->hit_face + b, task->hit_point + b};
+          int r = ray_caster::system_cast(sys, &sub);
+          if (r < 0) status = r;
+        }
       });
     }
     for (auto& th : pool) th.join();
-    for (int r : rc) if (r < 0) return r;
-    return 0;
+    return status.load();
   }
 }
 
