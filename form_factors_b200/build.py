@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libffb200.so")
 PROBE_LIB = os.path.join(PKG, "libffb200_probe.so")
 
-CUDA_SOURCES = ["ffb_api.cu"]
+CUDA_SOURCES = ["ffb_api.cu", "ffb_static.cu"]
 CXX_SOURCES = ["ffb_systems.cpp"]
 
 NVCC_FLAGS = [

@@ -60,6 +60,14 @@ constexpr int kMaxRows = 65535;  // matrix index row * n + col stays below 0xFFF
 
 }  // namespace
 
+// Records an error for ffb_last_error (shared with the other translation
+// units of the library) and returns `code`.
+int ffb_set_error(int code, const char* msg)
+{
+  g_last_error = msg ? msg : "";
+  return code;
+}
+
 struct ffb_ctx {
   int device = 0;
   int n_sm = 0;

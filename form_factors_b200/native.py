@@ -82,6 +82,7 @@ def load(path=LIB_PATH):
         "ffb_form_factor_counts": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp]),
         "ffb_normalise": (i32, [vp, vp, vp, i32, vp]),
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
+        "ffb_cast_bruteforce_static": (i32, [vp, i32, vp, i64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -108,6 +109,16 @@ def _check(code):
     if code < 0:
         raise FFBError(code, load().ffb_last_error().decode(errors="replace"))
     return code
+
+
+def cast_bruteforce_static(faces, rays, hit, points=None, stream=None):
+    """ffb_cast_bruteforce_static on device tensors (no context, no allocation).
+    faces: (n, 9) float32, rays: (m, 6) float32, hit: (m,) int32, points: (m, 3)
+    float32 or None -- all CUDA tensors.  Enqueued on `stream` (an int
+    cudaStream_t or None for the default stream)."""
+    lib = load()
+    _check(lib.ffb_cast_bruteforce_static(_ptr(faces), int(faces.shape[0]), _ptr(rays), int(rays.shape[0]),
+                                          _ptr(hit), _ptr(points), stream or None))
 
 
 class Context:

@@ -128,6 +128,23 @@ int ffb_normalise(ffb_ctx* ctx, const uint32_t* counts, const int32_t* outgoing,
  * (synchronises the stream). */
 int ffb_stats_get(ffb_ctx* ctx, ffb_stats* out);
 
+/* Brute-force nearest hit for callers that cannot allocate device memory.
+ * No counterpart in the reference: it exists for callers that may not call
+ * cudaMalloc (code running under an allocator that owns all device memory,
+ * or in a plugin host that forbids device allocations after start-up).
+ * Same results as ffb_cast_bruteforce, without
+ * a context: faces9, rays6, hit_face and hit_point (may be NULL) must all be
+ * device memory; the work is enqueued on `stream` (a cudaStream_t, NULL for
+ * the default stream) and the call returns without waiting.  The only
+ * scratch, the per-face triangle records, lives in a static device array of
+ * 16384 faces (1 MiB, held by every GPU that loads the library until exit);
+ * larger scenes return FFB_ERR_TOO_LARGE.  All calls share that array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * The first call on a device resolves the array's address with that device
+ * current; make it before any stream capture. */
+int ffb_cast_bruteforce_static(const float* faces9, int n_faces, const float* rays6, long long n_rays,
+                               int32_t* hit_face, float* hit_point, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
