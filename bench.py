@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-sample-every", type=int, default=0, help="reference sample: every k-th source face")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="", help="grid dims nx,ny,nz (default: automatic)")
+    ap.add_argument("--cells-per-face", type=float, default=32.0, help="automatic grid sizing target")
+    ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
     return ap.parse_args()
 
 
@@ -239,7 +241,7 @@ def ours(args):
     ctx.scene_set(faces)
     dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
     t0 = time.perf_counter()
-    ctx.grid_build(dims=dims)
+    ctx.grid_build(dims=dims, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
     torch.cuda.synchronize()
     grid_s = time.perf_counter() - t0
     info = ctx.grid_info()
