@@ -87,7 +87,7 @@ struct ffb_ctx {
   DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist, scan_sums;
 
   // per-call scratch
-  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor;
+  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   std::vector<unsigned char> host_stage_dummy;
   void* pinned = nullptr;
   size_t pinned_cap = 0;
@@ -299,7 +299,7 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   DevBuf* bufs[] = {&c->faces,     &c->tri,       &c->box_lo,   &c->box_hi,     &c->frames,    &c->scene_ord,
                     &c->cell_start, &c->cell_fill, &c->ref_tri,  &c->ref_rec,    &c->empty_dist, &c->scan_sums,
                     &c->chunks,    &c->rows,      &c->cursor,   &c->stats,      &c->tmp_in,    &c->tmp_out,
-                    &c->tmp_out2,  &c->offsets,   &c->front_dev, &c->ray_cursor};
+                    &c->tmp_out2,  &c->offsets,   &c->front_dev, &c->ray_cursor, &c->ff_counts};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
@@ -764,6 +764,21 @@ extern "C" int ffb_normalise(ffb_ctx* c, const uint32_t* counts, const int32_t* 
     FFB_CUDA(cudaStreamSynchronize(c->stream));
   }
   return FFB_OK;
+}
+
+extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
+                                int flags, const int32_t* face_to_row, int n_rows, const int32_t* outgoing, float* ff)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_rows <= 0 || !outgoing || !ff)
+    return fail(FFB_ERR_ARG, "bad form-factor arguments");
+  if (n_rows > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
+  const size_t mat = (size_t)n_rows * n_rows;
+  FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * mat));
+  FFB_TRY(ffb_form_factor_counts(c, front, rear, seed, epoch, flags, face_to_row, n_rows,
+                                 dptr<uint32_t>(c->ff_counts)));
+  return ffb_normalise(c, dptr<uint32_t>(c->ff_counts), outgoing, n_rows, ff);
 }
 
 extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)

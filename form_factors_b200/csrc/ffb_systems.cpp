@@ -1,0 +1,581 @@
+// ffb_systems.cpp -- the B200 ray caster, emission and form-factor systems
+// behind the reference's C-style vtables (include/ffb_systems.h), on top of
+// the C ABI of include/ffb.h.
+//
+// Host arithmetic that decides how many rays a face emits and how a matrix
+// row is normalised is written with the reference's float operations in the
+// reference's order (compiled with -ffp-contract=off), so that the same
+// inputs spend the same rays and produce the same normalisation.
+#include "ffb_systems.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "ffb.h"
+
+namespace {
+
+// malley_emission::emitted_front / emitted_rear (emission/malley_emission.cpp:50-60).
+int emitted(int n_rays, float weight, float total_weight)
+{
+  return weight > 0 ? std::max<int>(1, (int)(n_rays * (weight / total_weight))) : 0;
+}
+
+// math::triangle_area (math/triangle.cpp:86-92).
+float triangle_area(const math::triangle_t& t)
+{
+  const math::vec3 a = t.points[0], b = t.points[1], c = t.points[2];
+  const float vx = b.x - a.x, vy = b.y - a.y, vz = b.z - a.z;
+  const float wx = c.x - a.x, wy = c.y - a.y, wz = c.z - a.z;
+  const float nx = vy * wz - vz * wy, ny = vz * wx - vx * wz, nz = vx * wy - vy * wx;
+  return sqrtf(nx * nx + ny * ny + nz * nz) / 2;
+}
+
+int device_from_env()
+{
+  const char* s = getenv("FFB_DEVICE");
+  return s ? atoi(s) : 0;
+}
+
+// ray_caster::task_create / task_free (ray_caster/system.cpp:44-62): every
+// array malloc'd so that the reference's task_free releases it.
+ray_caster::task_t* task_alloc(int n)
+{
+  ray_caster::task_t* t = (ray_caster::task_t*)malloc(sizeof(ray_caster::task_t));
+  t->n_tasks = n;
+  t->ray = (math::ray_t*)malloc((size_t)n * sizeof(math::ray_t));
+  t->hit_face = (ray_caster::face_t**)malloc((size_t)n * sizeof(ray_caster::face_t*));
+  t->hit_point = (math::vec3*)malloc((size_t)n * sizeof(math::vec3));
+  return t;
+}
+
+void task_release(ray_caster::task_t* t)
+{
+  if (!t)
+    return;
+  free(t->ray);
+  free(t->hit_face);
+  free(t->hit_point);
+  free(t);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Ray caster
+// ===========================================================================
+namespace b200_ray_caster {
+
+struct caster_t : ray_caster::system_t {
+  ffb_ctx* ctx;
+  ray_caster::scene_t* scene;
+  ffb_grid_params grid;
+  int prepared;
+  std::vector<int32_t>* idx;  // host staging
+  std::vector<float>* pts;
+};
+
+static int init(caster_t* s)
+{
+  s->ctx = nullptr;
+  s->scene = nullptr;
+  s->grid = ffb_grid_params{0, 0, 0, 32.f, 1};
+  s->prepared = 0;
+  s->idx = new std::vector<int32_t>();
+  s->pts = new std::vector<float>();
+  return ffb_ctx_create(device_from_env(), &s->ctx);
+}
+
+static int shutdown(caster_t* s)
+{
+  ffb_ctx_destroy(s->ctx);
+  s->ctx = nullptr;
+  delete s->idx;
+  delete s->pts;
+  s->idx = nullptr;
+  s->pts = nullptr;
+  return RAY_CASTER_OK;
+}
+
+static int set_scene(caster_t* s, ray_caster::scene_t* scene)
+{
+  s->scene = scene;
+  s->prepared = 0;
+  return RAY_CASTER_OK;
+}
+
+static int prepare(caster_t* s)
+{
+  if (s->scene == 0 || s->scene->n_faces == 0)
+    return -RAY_CASTER_ERROR;
+  if (!s->ctx)
+    return FFB_ERR_NO_DEVICE;
+  int r = ffb_scene_set(s->ctx, &s->scene->faces[0].points[0].x, s->scene->n_faces);
+  if (r < 0)
+    return r;
+  if ((r = ffb_grid_build(s->ctx, &s->grid)) < 0)
+    return r;
+  s->prepared = 1;
+  return RAY_CASTER_OK;
+}
+
+static int cast(caster_t* s, ray_caster::task_t* task)
+{
+  if (!s->prepared)
+    return -RAY_CASTER_ERROR;
+  const int n = task->n_tasks;
+  if (n <= 0)
+    return RAY_CASTER_OK;
+  s->idx->resize((size_t)n);
+  s->pts->resize(3 * (size_t)n);
+  int r = ffb_cast(s->ctx, &task->ray[0].origin.x, n, s->idx->data(), s->pts->data());
+  if (r < 0)
+    return r;
+  const int32_t* idx = s->idx->data();
+  const float* p = s->pts->data();
+  for (int i = 0; i < n; ++i) {
+    if (idx[i] >= 0) {
+      task->hit_face[i] = &s->scene->faces[idx[i]];
+      task->hit_point[i].x = p[3 * i];
+      task->hit_point[i].y = p[3 * i + 1];
+      task->hit_point[i].z = p[3 * i + 2];
+    } else {
+      task->hit_face[i] = 0;
+    }
+  }
+  return RAY_CASTER_OK;
+}
+
+static const ray_caster::system_methods_t methods = {
+    (int (*)(ray_caster::system_t*))&init,
+    (int (*)(ray_caster::system_t*))&shutdown,
+    (int (*)(ray_caster::system_t*, ray_caster::scene_t*))&set_scene,
+    (int (*)(ray_caster::system_t*))&prepare,
+    (int (*)(ray_caster::system_t*, ray_caster::task_t*))&cast,
+};
+
+ray_caster::system_t* system_create()
+{
+  caster_t* s = (caster_t*)malloc(sizeof(caster_t));
+  s->methods = &methods;
+  return s;
+}
+
+ray_caster::system_t* create()
+{
+  ray_caster::system_t* s = system_create();
+  s->methods->init(s);
+  return s;
+}
+
+void destroy(ray_caster::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+int set_grid(ray_caster::system_t* system, int nx, int ny, int nz, float cells_per_face)
+{
+  if (!system || system->methods != &methods)
+    return FFB_ERR_ARG;
+  caster_t* s = (caster_t*)system;
+  s->grid.nx = nx;
+  s->grid.ny = ny;
+  s->grid.nz = nz;
+  s->grid.cells_per_face = cells_per_face;
+  s->prepared = 0;
+  return FFB_OK;
+}
+
+}  // namespace b200_ray_caster
+
+// ===========================================================================
+// Emission
+// ===========================================================================
+namespace b200_emission {
+
+struct emitter_t : emission::system_t {
+  ray_caster::system_t* caster;
+  ray_caster::scene_t* scene;
+  ffb_ctx* ctx;
+  uint64_t seed;
+  uint32_t epoch;  // calls so far: every calculate draws fresh rays
+  int flags;
+};
+
+static int init(emitter_t* s, ray_caster::system_t* caster)
+{
+  s->caster = caster;
+  s->scene = nullptr;
+  s->ctx = nullptr;
+  s->seed = 1;
+  s->epoch = 0;
+  s->flags = 0;
+  return ffb_ctx_create(device_from_env(), &s->ctx);
+}
+
+static int shutdown(emitter_t* s)
+{
+  ffb_ctx_destroy(s->ctx);
+  s->ctx = nullptr;
+  s->scene = nullptr;
+  return EMISSION_OK;
+}
+
+// emission/malley_cpu.cpp:77-92: also sets and prepares the caster.
+static int set_scene(emitter_t* s, ray_caster::scene_t* scene)
+{
+  if (scene == 0 || scene->n_faces == 0)
+    return -EMISSION_ERROR;
+  s->scene = scene;
+  int r = 0;
+  if (s->caster) {
+    if ((r = s->caster->methods->set_scene(s->caster, scene)) < 0)
+      return r;
+    if ((r = s->caster->methods->prepare(s->caster)) < 0)
+      return r;
+  }
+  if (!s->ctx)
+    return FFB_ERR_NO_DEVICE;
+  return ffb_scene_set(s->ctx, &scene->faces[0].points[0].x, scene->n_faces);
+}
+
+// emission/malley_cpu.cpp:142-211: the task's weights decide the rays per
+// face side; the batch is packed face by face, front then rear.
+static int calculate(emitter_t* s, emission::task_t* task)
+{
+  if (!s->scene || !s->ctx)
+    return -EMISSION_ERROR;
+  malley_emission::task_t* t = (malley_emission::task_t*)task;
+  if (task->rays) {
+    task_release(task->rays);
+    task->rays = 0;
+  }
+  const int n = s->scene->n_faces;
+  std::vector<int32_t> front((size_t)n), rear((size_t)n);
+  long long total = 0;
+  for (int f = 0; f < n; ++f) {
+    front[f] = emitted(t->n_rays, t->weights[2 * f], t->total_weight);
+    rear[f] = emitted(t->n_rays, t->weights[2 * f + 1], t->total_weight);
+    total += (long long)front[f] + rear[f];
+  }
+  if (total == 0)
+    return EMISSION_OK;
+  if (total > 0x7FFFFFFF)
+    return FFB_ERR_TOO_LARGE;
+  ray_caster::task_t* rays = task_alloc((int)total);
+  int r = ffb_emit(s->ctx, front.data(), rear.data(), s->seed, s->epoch++, s->flags, &rays->ray[0].origin.x);
+  if (r < 0) {
+    task_release(rays);
+    return r;
+  }
+  task->rays = rays;
+  if (s->caster && (r = s->caster->methods->cast(s->caster, rays)) < 0)
+    return r;
+  return EMISSION_OK;
+}
+
+const emission::system_methods_t methods = {
+    (int (*)(emission::system_t*, ray_caster::system_t*))&init,
+    (int (*)(emission::system_t*))&shutdown,
+    (int (*)(emission::system_t*, ray_caster::scene_t*))&set_scene,
+    (int (*)(emission::system_t*, emission::task_t*))&calculate,
+};
+
+emission::system_t* system_create()
+{
+  emitter_t* s = (emitter_t*)malloc(sizeof(emitter_t));
+  s->methods = &methods;
+  return s;
+}
+
+emission::system_t* create(ray_caster::system_t* caster)
+{
+  emission::system_t* s = system_create();
+  s->methods->init(s, caster);
+  return s;
+}
+
+void destroy(emission::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+int set_seed(emission::system_t* system, uint64_t seed)
+{
+  if (!system || system->methods != &methods)
+    return FFB_ERR_ARG;
+  emitter_t* s = (emitter_t*)system;
+  s->seed = seed;
+  s->epoch = 0;
+  return FFB_OK;
+}
+
+int set_flags(emission::system_t* system, int flags)
+{
+  if (!system || system->methods != &methods)
+    return FFB_ERR_ARG;
+  ((emitter_t*)system)->flags = flags;
+  return FFB_OK;
+}
+
+// seed/epoch/flags of a B200 emitter for the fused form-factor path.
+bool draw_key(emission::system_t* system, uint64_t* seed, uint32_t* epoch, int* flags)
+{
+  if (!system || system->methods != &methods)
+    return false;
+  emitter_t* s = (emitter_t*)system;
+  *seed = s->seed;
+  *epoch = s->epoch++;
+  *flags = s->flags;
+  return true;
+}
+
+}  // namespace b200_emission
+
+// ===========================================================================
+// Form factors
+// ===========================================================================
+namespace b200_form_factors {
+
+struct ff_t : form_factors::system_t {
+  emission::system_t* emitter;
+  int fused;  // emission + trace + counts on the GPU
+  form_factors::scene_t* scene;
+  ray_caster::scene_t rc_scene;
+  float total_area;
+  float* face_weights;
+  int* face_to_mesh;
+  int mesh_layout_ok;  // meshes cover every face once, in face order
+  ffb_ctx* ctx;
+  ffb_grid_params grid;
+  uint64_t seed;
+  uint32_t epoch;
+  int flags;
+};
+
+static int init(ff_t* s, emission::system_t* emitter)
+{
+  s->emitter = emitter;
+  s->fused = emitter == 0 || emitter->methods == &b200_emission::methods;
+  s->scene = 0;
+  s->rc_scene = ray_caster::scene_t{0, 0};
+  s->total_area = 0;
+  s->face_weights = 0;
+  s->face_to_mesh = 0;
+  s->mesh_layout_ok = 0;
+  s->ctx = nullptr;
+  s->grid = ffb_grid_params{0, 0, 0, 32.f, 1};
+  s->seed = 1;
+  s->epoch = 0;
+  s->flags = 0;
+  return s->fused ? ffb_ctx_create(device_from_env(), &s->ctx) : FORM_FACTORS_OK;
+}
+
+static int shutdown(ff_t* s)
+{
+  s->scene = 0;
+  free(s->face_weights);
+  s->face_weights = 0;
+  free(s->face_to_mesh);
+  s->face_to_mesh = 0;
+  s->total_area = 0;
+  ffb_ctx_destroy(s->ctx);
+  s->ctx = nullptr;
+  return FORM_FACTORS_OK;
+}
+
+// cpuFactorsCalculator/cpu_system.cpp:82-92; the fused path uploads the scene
+// and builds the grid here, where the reference's emitter prepares its caster.
+static int set_scene(ff_t* s, form_factors::scene_t* scene)
+{
+  s->scene = scene;
+  s->rc_scene = ray_caster::scene_t{scene->n_faces, scene->faces};
+  if (!s->fused)
+    return s->emitter->methods->set_scene(s->emitter, &s->rc_scene);
+  if (scene->n_faces == 0)
+    return -EMISSION_ERROR;
+  if (!s->ctx)
+    return FFB_ERR_NO_DEVICE;
+  int r = ffb_scene_set(s->ctx, &scene->faces[0].points[0].x, scene->n_faces);
+  if (r < 0)
+    return r;
+  return ffb_grid_build(s->ctx, &s->grid);
+}
+
+// cpuFactorsCalculator/cpu_system.cpp:95-136, total_area accumulating as there.
+static int prepare(ff_t* s)
+{
+  if (s->scene == 0 || s->scene->n_faces == 0 || s->scene->n_meshes == 0)
+    return -FORM_FACTORS_EMPTY_SCENE;
+  const int n_faces = s->scene->n_faces;
+  free(s->face_weights);
+  s->face_weights = (float*)malloc(2 * (size_t)n_faces * sizeof(float));
+  free(s->face_to_mesh);
+  s->face_to_mesh = (int*)malloc((size_t)n_faces * sizeof(int));
+  int next = 0;
+  s->mesh_layout_ok = 1;
+  for (int m = 0; m != s->scene->n_meshes; ++m) {
+    const form_factors::mesh_t& mesh = s->scene->meshes[m];
+    if (mesh.first_idx != next || mesh.n_faces < 0)
+      s->mesh_layout_ok = 0;
+    for (int f = 0; f != mesh.n_faces; ++f) {
+      const int idx = mesh.first_idx + f;
+      if (idx >= 0 && idx < n_faces)
+        s->face_to_mesh[idx] = m;
+    }
+    next = mesh.first_idx + mesh.n_faces;
+  }
+  if (next != n_faces)
+    s->mesh_layout_ok = 0;
+  for (int i = 0; i != n_faces; ++i) {
+    const float face_area = triangle_area(s->scene->faces[i]);
+    s->total_area += 2.f * face_area;
+    s->face_weights[2 * i] = face_area;
+    s->face_weights[2 * i + 1] = face_area;
+  }
+  if (s->total_area < FLT_EPSILON)
+    return -FORM_FACTORS_SCENE_TOO_SMALL;
+  return FORM_FACTORS_OK;
+}
+
+static int calculate_fused(ff_t* s, form_factors::task_t* task)
+{
+  if (!s->mesh_layout_ok)
+    return -FORM_FACTORS_ERROR;
+  const int n_faces = s->scene->n_faces, n_meshes = s->scene->n_meshes;
+  std::vector<int32_t> front((size_t)n_faces), rear((size_t)n_faces), outgoing((size_t)n_meshes, 0);
+  for (int f = 0; f < n_faces; ++f) {
+    front[f] = emitted(task->n_rays, s->face_weights[2 * f], s->total_area);
+    rear[f] = emitted(task->n_rays, s->face_weights[2 * f + 1], s->total_area);
+    outgoing[s->face_to_mesh[f]] += front[f] + rear[f];
+  }
+  uint64_t seed = s->seed;
+  uint32_t epoch = 0;
+  int flags = s->flags;
+  if (!b200_emission::draw_key(s->emitter, &seed, &epoch, &flags))
+    epoch = s->epoch++;
+  return ffb_form_factors(s->ctx, front.data(), rear.data(), seed, epoch, flags, s->face_to_mesh, n_meshes,
+                          outgoing.data(), task->form_factors);
+}
+
+// cpuFactorsCalculator/cpu_system.cpp:149-201 with any emitter.
+static int calculate_generic(ff_t* s, form_factors::task_t* task)
+{
+  malley_emission::task_t emission_task(task->n_rays, s->total_area, s->face_weights);
+  int r = s->emitter->methods->calculate(s->emitter, &emission_task);
+  if (r < 0) {
+    task_release(emission_task.rays);
+    return r;
+  }
+  const int n_meshes = s->scene->n_meshes;
+  memset(task->form_factors, 0, (size_t)n_meshes * n_meshes * sizeof(float));
+  ray_caster::task_t* rays = emission_task.rays;
+  const int n_tasks = rays ? rays->n_tasks : 0;
+  int n_ray = 0;
+  for (int m = 0; m != n_meshes; ++m) {
+    int mesh_outgoing_rays = 0;
+    const form_factors::mesh_t& mesh = s->scene->meshes[m];
+    for (int f = 0; f != mesh.n_faces; ++f) {
+      const int face_idx = mesh.first_idx + f;
+      const int face_rays = emitted(task->n_rays, s->face_weights[2 * face_idx], s->total_area) +
+                            emitted(task->n_rays, s->face_weights[2 * face_idx + 1], s->total_area);
+      for (int j = 0; j != face_rays && n_ray < n_tasks; ++j, ++n_ray) {
+        ++mesh_outgoing_rays;
+        if (rays->hit_face[n_ray]) {
+          const int hit_face_idx = (int)(rays->hit_face[n_ray] - s->rc_scene.faces);
+          task->form_factors[m * n_meshes + s->face_to_mesh[hit_face_idx]] += 1.f;
+        }
+      }
+    }
+    const float mesh_ratio = 1.f / (float)mesh_outgoing_rays;
+    for (int j = 0; j != n_meshes; ++j)
+      task->form_factors[m * n_meshes + j] *= mesh_ratio;
+  }
+  task_release(rays);
+  return FORM_FACTORS_OK;
+}
+
+static int calculate(ff_t* s, form_factors::task_t* task)
+{
+  if (!s->scene || !s->face_weights)
+    return -FORM_FACTORS_EMPTY_SCENE;
+  return s->fused ? calculate_fused(s, task) : calculate_generic(s, task);
+}
+
+static const form_factors::system_methods_t methods = {
+    (int (*)(form_factors::system_t*, emission::system_t*))&init,
+    (int (*)(form_factors::system_t*))&shutdown,
+    (int (*)(form_factors::system_t*, form_factors::scene_t*))&set_scene,
+    (int (*)(form_factors::system_t*))&prepare,
+    (int (*)(form_factors::system_t*, form_factors::task_t*))&calculate,
+};
+
+form_factors::system_t* system_create()
+{
+  ff_t* s = (ff_t*)malloc(sizeof(ff_t));
+  s->methods = &methods;
+  return s;
+}
+
+form_factors::system_t* create(emission::system_t* emitter)
+{
+  form_factors::system_t* s = system_create();
+  s->methods->init(s, emitter);
+  return s;
+}
+
+void destroy(form_factors::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+static ff_t* as_ff(form_factors::system_t* system)
+{
+  return system && system->methods == &methods ? (ff_t*)system : nullptr;
+}
+
+int set_seed(form_factors::system_t* system, uint64_t seed)
+{
+  ff_t* s = as_ff(system);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->seed = seed;
+  s->epoch = 0;
+  return FFB_OK;
+}
+
+int set_flags(form_factors::system_t* system, int flags)
+{
+  ff_t* s = as_ff(system);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->flags = flags;
+  return FFB_OK;
+}
+
+int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells_per_face)
+{
+  ff_t* s = as_ff(system);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->grid.nx = nx;
+  s->grid.ny = ny;
+  s->grid.nz = nz;
+  s->grid.cells_per_face = cells_per_face;
+  return FFB_OK;
+}
+
+}  // namespace b200_form_factors

@@ -124,6 +124,14 @@ int ffb_form_factor_counts(ffb_ctx* ctx, const int32_t* front, const int32_t* re
  * counts and ff: host or device; outgoing: host int32[n_rows]. */
 int ffb_normalise(ffb_ctx* ctx, const uint32_t* counts, const int32_t* outgoing, int n_rows, float* ff);
 
+/* Form factors in one call: the counts of ffb_form_factor_counts in device
+ * scratch, then ff[m * n_rows + j] = (float)count * (1.f / (float)outgoing[m])
+ * as cpuFactorsCalculator/cpu_system.cpp:162-196 computes them.  outgoing:
+ * host int32[n_rows], the rays leaving each row (mesh); ff: host or device
+ * float[n_rows * n_rows].  form_factors::system_calculate, form_factors/system.h:115. */
+int ffb_form_factors(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
+                     int flags, const int32_t* face_to_row, int n_rows, const int32_t* outgoing, float* ff);
+
 /* Counters and kernel time of the last ffb_cast / ffb_form_factor_counts
  * (synchronises the stream). */
 int ffb_stats_get(ffb_ctx* ctx, ffb_stats* out);

@@ -1,0 +1,192 @@
+/*
+ * ffb_systems.h -- the B200 path as new selectable types behind the
+ * reference's own C++ interfaces:
+ *
+ *   ray_caster::system_t    ray_caster/system.h:85-116     RAY_CASTER_B200      (5)
+ *   emission::system_t      emission/system.h:77-93        EMISSION_MALLEY_B200 (3)
+ *   form_factors::system_t  form_factors/system.h:95-119   FORM_FACTORS_B200    (2)
+ *
+ * Each system_create() mallocs the system and sets its method table, exactly
+ * like the reference's implementation creators (e.g. ray_caster/naive_cpu.cpp
+ * system_create): the reference's factory then calls init, and system_free
+ * (shutdown + free) releases it.  create() does both steps for callers
+ * without the reference's factory, destroy() is shutdown + free.  Built
+ * inside the reference tree, define
+ * FFB_USE_REFERENCE_HEADERS and put the reference root on the include path:
+ * the reference's own headers then declare the interface types.  Otherwise
+ * the layout-identical declarations below are used (same members, same order,
+ * same method tables).
+ */
+#ifndef FFB_SYSTEMS_H
+#define FFB_SYSTEMS_H
+
+#include <stdint.h>
+
+#ifdef FFB_USE_REFERENCE_HEADERS
+#include "ray_caster/system.h"
+#include "emission/system.h"
+#include "emission/malley_emission.h"
+#include "form_factors/system.h"
+#else
+
+namespace math {
+typedef float point_t;
+struct vec3 {
+  point_t x, y, z;
+};
+struct triangle_t {
+  vec3 points[3];
+};
+typedef triangle_t face_t;
+struct ray_t {
+  vec3 origin;
+  vec3 direction;  // the END point of the ray, not a direction
+};
+}  // namespace math
+
+namespace ray_caster {
+typedef math::triangle_t face_t;
+typedef math::ray_t ray_t;
+struct task_t {
+  int n_tasks;
+  math::ray_t* ray;
+  face_t** hit_face;
+  math::vec3* hit_point;
+};
+struct scene_t {
+  int n_faces;
+  face_t* faces;
+};
+struct system_t {
+  const struct system_methods_t* methods;
+};
+#define RAY_CASTER_OK 0
+#define RAY_CASTER_ERROR 1
+#define RAY_CASTER_NOT_SUPPORTED 2
+struct system_methods_t {
+  int (*init)(system_t* system);
+  int (*shutdown)(system_t* system);
+  int (*set_scene)(system_t* system, scene_t* scene);
+  int (*prepare)(system_t* system);
+  int (*cast)(system_t* system, task_t* task);
+};
+}  // namespace ray_caster
+
+namespace emission {
+struct task_t {
+  task_t(int n) : n_rays(n), rays(0) {}
+  int n_rays;
+  ray_caster::task_t* rays;
+};
+struct system_t {
+  const struct system_methods_t* methods;
+};
+#define EMISSION_OK 0
+#define EMISSION_ERROR 200
+struct system_methods_t {
+  int (*init)(system_t* system, ray_caster::system_t* ray_caster);
+  int (*shutdown)(system_t* system);
+  int (*set_scene)(system_t* system, ray_caster::scene_t* scene);
+  int (*calculate)(system_t* system, task_t* task);
+};
+}  // namespace emission
+
+namespace malley_emission {
+struct task_t : emission::task_t {
+  task_t(int n, float total, float* ws) : emission::task_t(n), total_weight(total), weights(ws) {}
+  float total_weight;
+  float* weights;  // two per face: front, rear
+};
+}  // namespace malley_emission
+
+namespace form_factors {
+typedef math::triangle_t face_t;
+struct mesh_t {
+  int first_idx;
+  int n_faces;
+  int padding0;
+};
+struct scene_t {
+  int n_faces;
+  face_t* faces;
+  int n_meshes;
+  mesh_t* meshes;
+};
+struct task_t {
+  int n_rays;
+  float* form_factors;
+};
+struct system_t {
+  const struct system_methods_t* methods;
+};
+#define FORM_FACTORS_OK 0
+#define FORM_FACTORS_ERROR 100
+#define FORM_FACTORS_EMPTY_SCENE 101
+#define FORM_FACTORS_SCENE_TOO_SMALL 102
+struct system_methods_t {
+  int (*init)(system_t* system, emission::system_t* emitter);
+  int (*shutdown)(system_t* system);
+  int (*set_scene)(system_t* system, scene_t* scene);
+  int (*prepare)(system_t* system);
+  int (*calculate)(system_t* system, task_t* task);
+};
+}  // namespace form_factors
+
+#endif  // FFB_USE_REFERENCE_HEADERS
+
+/* Type IDs beside the reference's (ray_caster/system.h:106-109,
+ * emission/system.h:92-93, form_factors/system.h:119). */
+#define RAY_CASTER_B200 5
+#define EMISSION_MALLEY_B200 3
+#define FORM_FACTORS_B200 2
+
+namespace b200_ray_caster {
+/* Grid nearest-hit caster on the GPU.  set_scene keeps the pointer (the
+ * reference's casters do not own scenes); prepare uploads the faces and
+ * builds the grid (-RAY_CASTER_ERROR without a scene or with no faces, as
+ * ray_caster/zgrid_cpu.cpp:59-60); cast writes hit_face (a pointer into the
+ * caller's faces, or 0) and, for hits only, hit_point. */
+ray_caster::system_t* system_create();
+ray_caster::system_t* create();
+void destroy(ray_caster::system_t* system);
+/* Grid resolution (0,0,0 = automatic from cells_per_face). */
+int set_grid(ray_caster::system_t* system, int nx, int ny, int nz, float cells_per_face);
+}  // namespace b200_ray_caster
+
+namespace b200_emission {
+/* Malley emission on the GPU with Philox draws keyed by (seed, call, face,
+ * ray).  Works with any ray_caster::system_t: the rays are generated on the
+ * device, copied into task->rays (malloc'd, freed by the caller with
+ * ray_caster::task_free as in cpuFactorsCalculator/cpu_system.cpp:198) and
+ * cast with the given caster.  set_scene also sets and prepares the caster
+ * (emission/malley_cpu.cpp:77-92). */
+emission::system_t* system_create();
+emission::system_t* create(ray_caster::system_t* caster);
+void destroy(emission::system_t* system);
+/* Seed of the Philox stream (default 1); resets the per-call counter. */
+int set_seed(emission::system_t* system, uint64_t seed);
+/* FFB_EMIT_REF_NORMAL (1): rotate +z to the raw cross-product normal as the
+ * reference does; 0 (default): the normalised normal. */
+int set_flags(emission::system_t* system, int flags);
+}  // namespace b200_emission
+
+namespace b200_form_factors {
+/* Form factors between meshes.  With a B200 emitter (or a NULL emitter) the
+ * whole calculation -- emission, grid trace, per-(mesh, mesh) counts and the
+ * row normalisation -- runs fused on the GPU and no ray batch is ever
+ * materialised; with any other emitter it calls that emitter and counts on the
+ * host as cpuFactorsCalculator/cpu_system.cpp:149-201 does.  Weights, the
+ * total area (accumulating over prepare calls, cpu_system.cpp:126) and the
+ * per-face ray budget follow the reference.  The fused path needs meshes that
+ * cover every face exactly once in face order (the layout the reference's
+ * ray walk assumes, cpu_system.cpp:167-190); other layouts return
+ * -FORM_FACTORS_ERROR. */
+form_factors::system_t* system_create();
+form_factors::system_t* create(emission::system_t* emitter);
+void destroy(form_factors::system_t* system);
+int set_seed(form_factors::system_t* system, uint64_t seed);
+int set_flags(form_factors::system_t* system, int flags);
+int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells_per_face);
+}  // namespace b200_form_factors
+
+#endif /* FFB_SYSTEMS_H */

@@ -1,0 +1,404 @@
+// test_systems.cpp -- the B200 system types driven through the reference's
+// C-style interfaces, in the manner of the reference's typed gtest suites
+// (test/ray_casting.cpp, test/form_factors.cpp): the same checks run for
+// every engine type.
+//
+// Built two ways:
+//  * standalone (include/ffb_systems.h declarations): B200 types only;
+//  * with -DFFB_WITH_REFERENCE and the reference's headers/objects: the
+//    reference's naive_cpu / zgrid_cpu casters, malley_cpu emitter and
+//    cpu_form_factors calculator run beside the B200 types and mixed with
+//    them (reference calculator over the B200 emitter and caster, B200
+//    calculator over the reference emitter).
+// Exit status 0 when every check passes.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "ffb_systems.h"
+
+static int g_failures = 0;
+static int g_checks = 0;
+#define CHECK(cond)                                                              \
+  do {                                                                           \
+    ++g_checks;                                                                  \
+    if (!(cond)) {                                                               \
+      ++g_failures;                                                              \
+      std::fprintf(stderr, "FAIL %s:%d: %s [%s]\n", __FILE__, __LINE__, #cond, g_case.c_str()); \
+    }                                                                            \
+  } while (0)
+
+static std::string g_case;
+
+using math::vec3;
+
+static vec3 V(float x, float y, float z) { return vec3{x, y, z}; }
+static vec3 add(vec3 a, vec3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static vec3 sub(vec3 a, vec3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static math::triangle_t T(vec3 a, vec3 b, vec3 c) { return math::triangle_t{{a, b, c}}; }
+static vec3 center(const math::triangle_t& t)
+{
+  return V((t.points[0].x + t.points[1].x + t.points[2].x) / 3.f, (t.points[0].y + t.points[1].y + t.points[2].y) / 3.f,
+           (t.points[0].z + t.points[1].z + t.points[2].z) / 3.f);
+}
+// math::ray_to_triangle: towards the centre, ending half way.
+static math::ray_t ray_to(vec3 o, const math::triangle_t& t)
+{
+  vec3 c = center(t);
+  vec3 h = sub(c, o);
+  return math::ray_t{o, add(o, V(h.x / 2.f, h.y / 2.f, h.z / 2.f))};
+}
+static bool near_enough(vec3 a, vec3 b)
+{
+  vec3 d = sub(a, b);
+  return d.x * d.x + d.y * d.y + d.z * d.z < 1e-8;
+}
+
+// ---------------------------------------------------------------------------
+// engines
+// ---------------------------------------------------------------------------
+struct Caster {
+  const char* name;
+  std::function<ray_caster::system_t*()> make;
+  std::function<void(ray_caster::system_t*)> free_;
+};
+
+static std::vector<Caster> casters()
+{
+  std::vector<Caster> v;
+  v.push_back({"B200", [] { return b200_ray_caster::create(); }, [](ray_caster::system_t* s) { b200_ray_caster::destroy(s); }});
+#ifdef FFB_WITH_REFERENCE
+  v.push_back({"NAIVE_CPU", [] { return ray_caster::system_create(RAY_CASTER_NAIVE_CPU); },
+               [](ray_caster::system_t* s) { ray_caster::system_free(s); }});
+  v.push_back({"ZGRID_CPU", [] { return ray_caster::system_create(RAY_CASTER_ZGRID_CPU); },
+               [](ray_caster::system_t* s) { ray_caster::system_free(s); }});
+#endif
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// ray caster checks (test/ray_casting.cpp:113-322)
+// ---------------------------------------------------------------------------
+static void ray_caster_suite(const Caster& E)
+{
+  auto floor1 = T(V(0, 0, 0), V(1, 0, 0), V(0, 1, 0));
+  auto floor2 = T(V(1, 0, 0), V(0, 1, 0), V(1, 1, 0));
+  auto stack = T(V(0, 0, -1), V(1, 0, -1), V(0, 1, -1));
+  {
+    g_case = std::string(E.name) + " empty scene";
+    ray_caster::system_t* s = E.make();
+    ray_caster::scene_t empty = {0, 0};
+    CHECK(s->methods->set_scene(s, &empty) == RAY_CASTER_OK);
+    CHECK(s->methods->prepare(s) == -RAY_CASTER_ERROR);
+    E.free_(s);
+  }
+  {
+    g_case = std::string(E.name) + " prepare without scene";
+    ray_caster::system_t* s = E.make();
+    CHECK(s->methods->prepare(s) == -RAY_CASTER_ERROR);
+    E.free_(s);
+  }
+  {
+    g_case = std::string(E.name) + " floor";
+    ray_caster::system_t* s = E.make();
+    math::triangle_t faces[2] = {floor1, floor2};
+    ray_caster::scene_t scene = {2, faces};
+    CHECK(s->methods->set_scene(s, &scene) == RAY_CASTER_OK);
+    CHECK(s->methods->prepare(s) == RAY_CASTER_OK);
+    math::ray_t rays[2] = {ray_to(add(center(faces[0]), V(0, 0, 1)), faces[0]),
+                           ray_to(add(center(faces[1]), V(0, 0, -1)), faces[1])};
+    ray_caster::face_t* hit[2] = {0, 0};
+    vec3 pts[2];
+    ray_caster::task_t task = {2, rays, hit, pts};
+    CHECK(s->methods->cast(s, &task) == RAY_CASTER_OK);
+    CHECK(hit[0] == &faces[0] && hit[1] == &faces[1]);
+    CHECK(near_enough(pts[0], center(faces[0])) && near_enough(pts[1], center(faces[1])));
+    E.free_(s);
+  }
+  {
+    g_case = std::string(E.name) + " stack";
+    ray_caster::system_t* s = E.make();
+    math::triangle_t faces[2] = {floor1, stack};
+    ray_caster::scene_t scene = {2, faces};
+    s->methods->set_scene(s, &scene);
+    CHECK(s->methods->prepare(s) == RAY_CASTER_OK);
+    vec3 c0 = center(faces[0]), c1 = center(faces[1]);
+    math::ray_t rays[4] = {
+        math::ray_t{add(c0, V(0, 0, .5f)), sub(c0, V(0, 0, .5f))},  // HandleRayIntersectingTriangle
+        ray_to(add(c0, V(0, 0, 1)), faces[0]),                     // FindNearestTriangle
+        ray_to(add(c1, V(0, 0, .9f)), faces[1]),                   // SkipTriangleNearButInOppositeDirection
+        ray_to(add(c1, V(2, 2, 2)), faces[1])};                    // IntersectTriganglesNotPlanes
+    ray_caster::face_t* hit[4] = {0, 0, 0, 0};
+    vec3 pts[4];
+    ray_caster::task_t task = {4, rays, hit, pts};
+    CHECK(s->methods->cast(s, &task) == RAY_CASTER_OK);
+    CHECK(hit[0] == &faces[0] && hit[1] == &faces[0] && hit[2] == &faces[1] && hit[3] == &faces[1]);
+    CHECK(near_enough(pts[0], c0) && near_enough(pts[1], c0) && near_enough(pts[2], c1) && near_enough(pts[3], c1));
+    E.free_(s);
+  }
+  {
+    g_case = std::string(E.name) + " large scene";
+    ray_caster::system_t* s = E.make();
+    std::vector<math::triangle_t> faces;
+    for (int i = -500; i != 500; ++i) {
+      vec3 sh = V(0, 0, .1f * (float)i);
+      faces.push_back(T(add(floor1.points[0], sh), add(floor1.points[1], sh), add(floor1.points[2], sh)));
+    }
+    ray_caster::scene_t scene = {(int)faces.size(), faces.data()};
+    s->methods->set_scene(s, &scene);
+    CHECK(s->methods->prepare(s) == RAY_CASTER_OK);
+    vec3 c = center(faces[0]);
+    math::ray_t ray = ray_to(add(c, V(2, 2, -2)), faces[0]);
+    ray_caster::face_t* hit = 0;
+    vec3 pt;
+    ray_caster::task_t task = {1, &ray, &hit, &pt};
+    CHECK(s->methods->cast(s, &task) == RAY_CASTER_OK);
+    CHECK(hit == &faces[0] && near_enough(pt, c));
+    E.free_(s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// form factors (test/form_factors.cpp:192-298, two-sided semantics: F is half
+// the one-sided analytic value)
+// ---------------------------------------------------------------------------
+static double vf_parallel(double a, double b, double c)
+{
+  double x = a / c, y = b / c, xq = x * x, yq = y * y;
+  return 2.0 / M_PI / x / y *
+         (std::log(std::sqrt((1 + xq) * (1 + yq) / (1 + xq + yq))) + x * std::sqrt(1 + yq) * std::atan(x / std::sqrt(1 + yq)) +
+          y * std::sqrt(1 + xq) * std::atan(y / std::sqrt(1 + xq)) - x * std::atan(x) - y * std::atan(y));
+}
+
+static double vf_perpendicular(double H, double W, double L)
+{
+  double h = H / L, w = W / L;
+  double a = (1 + h * h) * (1 + w * w) / (1 + h * h + w * w);
+  double b = w * w * (1 + h * h + w * w) / (1 + w * w) / (h * h + w * w);
+  double c = h * h * (1 + h * h + w * w) / (1 + h * h) / (h * h + w * w);
+  return 1.0 / M_PI / w *
+         (h * std::atan(1 / h) + w * std::atan(1 / w) - std::sqrt(h * h + w * w) * std::atan(1 / std::sqrt(h * h + w * w)) +
+          0.25 * std::log(a * std::pow(b, w * w) * std::pow(c, h * h)));
+}
+
+static std::vector<math::triangle_t> square(vec3 o)
+{
+  return {T(add(V(0, 0, 0), o), add(V(1, 0, 0), o), add(V(0, 1, 0), o)),
+          T(add(V(1, 0, 0), o), add(V(1, 1, 0), o), add(V(0, 1, 0), o))};
+}
+
+struct Calculator {
+  const char* name;
+  std::function<void(form_factors::system_t**, emission::system_t**, ray_caster::system_t**)> make;
+  std::function<void(form_factors::system_t*, emission::system_t*, ray_caster::system_t*)> free_;
+};
+
+static std::vector<Calculator> calculators()
+{
+  std::vector<Calculator> v;
+  // fused B200 path (B200 emitter, whose caster is the B200 caster)
+  v.push_back({"B200 fused",
+               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
+                 *r = b200_ray_caster::create();
+                 *e = b200_emission::create(*r);
+                 *f = b200_form_factors::create(*e);
+               },
+               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
+                 b200_form_factors::destroy(f);
+                 b200_emission::destroy(e);
+                 b200_ray_caster::destroy(r);
+               }});
+#ifdef FFB_WITH_REFERENCE
+  // reference calculator over the B200 emitter and caster
+  v.push_back({"CPU calculator + B200 emission/caster",
+               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
+                 *r = b200_ray_caster::create();
+                 *e = b200_emission::create(*r);
+                 *f = form_factors::system_create(FORM_FACTORS_CPU, *e);
+               },
+               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
+                 form_factors::system_free(f);
+                 b200_emission::destroy(e);
+                 b200_ray_caster::destroy(r);
+               }});
+  // reference calculator and emitter over the B200 caster
+  v.push_back({"CPU calculator + malley_cpu + B200 caster",
+               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
+                 *r = b200_ray_caster::create();
+                 *e = emission::system_create(EMISSION_MALLEY_CPU, *r);
+                 *f = form_factors::system_create(FORM_FACTORS_CPU, *e);
+               },
+               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
+                 form_factors::system_free(f);
+                 emission::system_free(e);
+                 b200_ray_caster::destroy(r);
+               }});
+  // B200 calculator over the reference emitter and caster (host counting path)
+  v.push_back({"B200 calculator + malley_cpu + naive_cpu",
+               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
+                 *r = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
+                 *e = emission::system_create(EMISSION_MALLEY_CPU, *r);
+                 *f = b200_form_factors::create(*e);
+               },
+               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
+                 b200_form_factors::destroy(f);
+                 emission::system_free(e);
+                 ray_caster::system_free(r);
+               }});
+  // the reference alone, as the control
+  v.push_back({"CPU reference",
+               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
+                 *r = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
+                 *e = emission::system_create(EMISSION_MALLEY_CPU, *r);
+                 *f = form_factors::system_create(FORM_FACTORS_CPU, *e);
+               },
+               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
+                 form_factors::system_free(f);
+                 emission::system_free(e);
+                 ray_caster::system_free(r);
+               }});
+#endif
+  return v;
+}
+
+static void form_factor_suite(const Calculator& C)
+{
+  const float distances[] = {.5f, 1, 2, 3, 10};
+  for (float d : distances) {
+    g_case = std::string(C.name) + " parallel d=" + std::to_string(d);
+    form_factors::system_t* f;
+    emission::system_t* e;
+    ray_caster::system_t* r;
+    C.make(&f, &e, &r);
+    std::vector<math::triangle_t> faces = square(V(0, 0, 0));
+    std::vector<math::triangle_t> top = square(V(0, 0, d));
+    faces.insert(faces.end(), top.begin(), top.end());
+    form_factors::mesh_t meshes[2] = {{0, 2, 0}, {2, 2, 0}};
+    form_factors::scene_t scene = {4, faces.data(), 2, meshes};
+    CHECK(f->methods->set_scene(f, &scene) >= 0);
+    CHECK(f->methods->prepare(f) == FORM_FACTORS_OK);
+    float ff[4];
+    form_factors::task_t task = {40000, ff};
+    CHECK(f->methods->calculate(f, &task) == FORM_FACTORS_OK);
+    const double want = vf_parallel(1, 1, d) / 2;
+    CHECK(std::fabs(ff[1] - want) < 0.01 && std::fabs(ff[2] - want) < 0.01);
+    // a plate sees itself only through FP32 rounding of grazing rays
+    CHECK(ff[0] < 1e-3f && ff[3] < 1e-3f);
+    C.free_(f, e, r);
+  }
+  {
+    g_case = std::string(C.name) + " perpendicular";
+    form_factors::system_t* f;
+    emission::system_t* e;
+    ray_caster::system_t* r;
+    C.make(&f, &e, &r);
+    std::vector<math::triangle_t> faces = square(V(0, 0, 0));
+    faces.push_back(T(V(0, 0, 0), V(0, 1, 0), V(0, 0, 1)));
+    faces.push_back(T(V(0, 1, 0), V(0, 0, 1), V(0, 1, 1)));
+    form_factors::mesh_t meshes[2] = {{0, 2, 0}, {2, 2, 0}};
+    form_factors::scene_t scene = {4, faces.data(), 2, meshes};
+    f->methods->set_scene(f, &scene);
+    CHECK(f->methods->prepare(f) == FORM_FACTORS_OK);
+    float ff[4];
+    form_factors::task_t task = {40000, ff};
+    CHECK(f->methods->calculate(f, &task) == FORM_FACTORS_OK);
+    CHECK(std::fabs(ff[2] - vf_perpendicular(1, 1, 1) / 2) < 0.01);
+    C.free_(f, e, r);
+  }
+  {
+    g_case = std::string(C.name) + " box";
+    form_factors::system_t* f;
+    emission::system_t* e;
+    ray_caster::system_t* r;
+    C.make(&f, &e, &r);
+    vec3 v[] = {V(0, 0, 0), V(1, 0, 0), V(1, 1, 0), V(0, 1, 0), V(0, 0, 1), V(1, 0, 1), V(1, 1, 1), V(0, 1, 1)};
+    math::triangle_t faces[12];
+    faces[0] = T(v[0], v[1], v[2]);
+    faces[1] = T(v[0], v[3], v[2]);
+    faces[8] = T(v[0], v[1], v[5]);
+    faces[9] = T(v[0], v[4], v[5]);
+    faces[4] = T(v[0], v[3], v[7]);
+    faces[5] = T(v[0], v[4], v[7]);
+    faces[6] = T(v[1], v[2], v[6]);
+    faces[7] = T(v[1], v[5], v[6]);
+    faces[2] = T(v[3], v[2], v[6]);
+    faces[3] = T(v[3], v[7], v[6]);
+    faces[10] = T(v[4], v[5], v[6]);
+    faces[11] = T(v[4], v[7], v[6]);
+    form_factors::mesh_t mesh = {0, 12, 0};
+    form_factors::scene_t scene = {12, faces, 1, &mesh};
+    f->methods->set_scene(f, &scene);
+    CHECK(f->methods->prepare(f) == FORM_FACTORS_OK);
+    float ff[1];
+    form_factors::task_t task = {40000, ff};
+    CHECK(f->methods->calculate(f, &task) == FORM_FACTORS_OK);
+    CHECK(std::fabs(ff[0] - 0.5f) < 0.01);
+    C.free_(f, e, r);
+  }
+  {
+    g_case = std::string(C.name) + " empty scene";
+    form_factors::system_t* f;
+    emission::system_t* e;
+    ray_caster::system_t* r;
+    C.make(&f, &e, &r);
+    form_factors::scene_t scene = {0, 0, 0, 0};
+    f->methods->set_scene(f, &scene);
+    CHECK(f->methods->prepare(f) == -FORM_FACTORS_EMPTY_SCENE);
+    C.free_(f, e, r);
+  }
+}
+
+// Emission: the batch layout of emission/malley_cpu.cpp:142-189 and the ray
+// budget of emission/malley_emission.cpp:50-60.
+static void emission_suite()
+{
+  g_case = "B200 emission";
+  ray_caster::system_t* r = b200_ray_caster::create();
+  emission::system_t* e = b200_emission::create(r);
+  std::vector<math::triangle_t> faces = square(V(0, 0, 0));
+  std::vector<math::triangle_t> top = square(V(0, 0, 1));
+  faces.insert(faces.end(), top.begin(), top.end());
+  ray_caster::scene_t scene = {4, faces.data()};
+  CHECK(e->methods->set_scene(e, &scene) == EMISSION_OK);
+  float w[8] = {1, 1, 2, 0, 0.5f, 0.5f, 0, 0};
+  malley_emission::task_t task(1000, 5.f, w);
+  CHECK(e->methods->calculate(e, &task) == EMISSION_OK);
+  // 200+200, 400+0, 100+100, 0+0 rays
+  CHECK(task.rays && task.rays->n_tasks == 1000);
+  if (task.rays) {
+    int hits = 0;
+    for (int i = 0; i < task.rays->n_tasks; ++i) {
+      math::ray_t ray = task.rays->ray[i];
+      // origins lie on the emitting face (z = 0 for faces 0-1, z = 1 for face 2)
+      const int face = i < 400 ? 0 : (i < 800 ? 1 : 2);
+      const float z = face < 2 ? 0.f : 1.f;
+      CHECK(std::fabs(ray.origin.z - z) < 2e-4f);
+      // front rays of face 0 point up (+z), rear rays down
+      if (face == 0)
+        CHECK((i < 200) == (ray.direction.z > ray.origin.z));
+      hits += task.rays->hit_face[i] != 0;
+    }
+    CHECK(hits > 50);
+    free(task.rays->ray);
+    free(task.rays->hit_face);
+    free(task.rays->hit_point);
+    free(task.rays);
+  }
+  b200_emission::destroy(e);
+  b200_ray_caster::destroy(r);
+}
+
+int main()
+{
+  for (const Caster& c : casters())
+    ray_caster_suite(c);
+  emission_suite();
+  for (const Calculator& c : calculators())
+    form_factor_suite(c);
+  std::printf("%d checks, %d failures\n", g_checks, g_failures);
+  return g_failures == 0 ? 0 : 1;
+}
