@@ -1,9 +1,10 @@
 // ffb_api.cu -- the C ABI of libffb200.so (declared in include/ffb.h).
 //
-// Host orchestration of the B200 form-factor path: resident scene and grid
-// per context, one CUDA stream per context, grow-only device scratch, pinned
-// staging for host arguments.  No CPU fallback: every result is computed by
-// the kernels of ffb_grid.cuh / ffb_trace.cuh.
+// Host orchestration of the B200 form-factor path: resident scenes and grids
+// per context (one main scene, or a batch of scenes for one fused launch),
+// one CUDA stream per context, grow-only device scratch, pinned staging for
+// host arguments.  No CPU fallback: every result is computed by the kernels of
+// ffb_grid.cuh / ffb_trace.cuh.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -58,6 +59,15 @@ struct DevBuf {
 constexpr int kChunkRays = 256;  // rays per work chunk of the fused kernel
 constexpr int kMaxRows = 65535;  // matrix index row * n + col stays below 0xFFFFFFFF
 
+// One resident scene: faces, triangle records and its grid.
+struct SceneData {
+  int n_faces = -1;  // -1: no scene
+  DevBuf faces, tri, box_lo, box_hi, scene_ord;
+  bool grid_ok = false;
+  ffb_grid_info info{};
+  DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist;
+};
+
 }  // namespace
 
 // Records an error for ffb_last_error (shared with the other translation
@@ -76,19 +86,18 @@ struct ffb_ctx {
   unsigned long long budget = 0;  // 0 = unlimited
   unsigned long long bytes = 0;   // device bytes held in DevBufs
 
-  // scene
-  int n_faces = -1;  // -1: no scene
-  DevBuf faces, tri, box_lo, box_hi, frames, scene_ord;
-  int frames_mode = -1;  // emission flags the frames were built for
+  SceneData main;                 // the scene of the single-scene calls
+  DevBuf frames;                  // emission frames of the main scene
+  int frames_mode = -1;           // emission flags the frames were built for
 
-  // grid
-  bool grid_ok = false;
-  ffb_grid_info info{};
-  DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist, scan_sums;
+  std::vector<SceneData> batch;   // the scenes of the batched calls
+  std::vector<long long> batch_offsets;
+  DevBuf batch_frames, batch_chunks, batch_keys, batch_epoch;
+  int batch_frames_mode = -1;
+  int batch_n_chunks = 0;
 
   // per-call scratch
-  DevBuf chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
-  std::vector<unsigned char> host_stage_dummy;
+  DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   void* pinned = nullptr;
   size_t pinned_cap = 0;
   cudaEvent_t pinned_free = nullptr;  // recorded after the last copy out of `pinned`
@@ -132,6 +141,16 @@ void release(ffb_ctx* c, DevBuf& b)
   }
   b.ptr = nullptr;
   b.cap = 0;
+}
+
+void release_scene(ffb_ctx* c, SceneData& s)
+{
+  DevBuf* bufs[] = {&s.faces,      &s.tri,     &s.box_lo,  &s.box_hi,  &s.scene_ord,
+                    &s.cell_start, &s.cell_fill, &s.ref_tri, &s.ref_rec, &s.empty_dist};
+  for (DevBuf* b : bufs)
+    release(c, *b);
+  s.n_faces = -1;
+  s.grid_ok = false;
 }
 
 template <class T>
@@ -186,10 +205,10 @@ int grid_blocks(long long n, int threads, int max_blocks = 1 << 20)
   return (int)std::max<long long>(1, std::min<long long>(b, max_blocks));
 }
 
-GridView make_view(ffb_ctx* c)
+GridView make_view(SceneData& s)
 {
   GridView g;
-  const ffb_grid_info& I = c->info;
+  const ffb_grid_info& I = s.info;
   g.lo = make_float3(I.lo[0], I.lo[1], I.lo[2]);
   g.hi = make_float3(I.hi[0], I.hi[1], I.hi[2]);
   g.cs = make_float3(I.cell[0], I.cell[1], I.cell[2]);
@@ -198,10 +217,10 @@ GridView make_view(ffb_ctx* c)
   g.ny = I.ny;
   g.nz = I.nz;
   g.slack = 2.f * I.margin;
-  g.cell_start = dptr<uint32_t>(c->cell_start);
-  g.ref_tri = dptr<int32_t>(c->ref_tri);
-  g.ref_rec = dptr<TriRec>(c->ref_rec);
-  g.empty_dist = I.skip_empty ? dptr<uint8_t>(c->empty_dist) : nullptr;
+  g.cell_start = dptr<uint32_t>(s.cell_start);
+  g.ref_tri = dptr<int32_t>(s.ref_tri);
+  g.ref_rec = dptr<TriRec>(s.ref_rec);
+  g.empty_dist = I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr;
   return g;
 }
 
@@ -213,16 +232,22 @@ int check_ctx(ffb_ctx* c)
   return FFB_OK;
 }
 
+// Emission frames for n_faces faces starting at `faces9` into `frames`.
+int build_frames(ffb_ctx* c, const float* faces9, int n_faces, int mode, float* frames)
+{
+  if (n_faces > 0)
+    k_face_frames<<<grid_blocks(n_faces, 256), 256, 0, c->stream>>>(faces9, n_faces, mode, frames);
+  FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
+}
+
 int ensure_frames(ffb_ctx* c, int flags)
 {
-  int mode = flags & FFB_EMIT_REF_NORMAL;
+  const int mode = flags & FFB_EMIT_REF_NORMAL;
   if (c->frames_mode == mode)
     return FFB_OK;
-  FFB_TRY(ensure(c, c->frames, sizeof(float) * 20 * (size_t)std::max(c->n_faces, 1)));
-  if (c->n_faces > 0)
-    k_face_frames<<<grid_blocks(c->n_faces, 256), 256, 0, c->stream>>>(dptr<float>(c->faces), c->n_faces, mode,
-                                                                       dptr<float>(c->frames));
-  FFB_CUDA(cudaGetLastError());
+  FFB_TRY(ensure(c, c->frames, sizeof(float) * 20 * (size_t)std::max(c->main.n_faces, 1)));
+  FFB_TRY(build_frames(c, dptr<float>(c->main.faces), c->main.n_faces, mode, dptr<float>(c->frames)));
   c->frames_mode = mode;
   return FFB_OK;
 }
@@ -249,6 +274,211 @@ void timing_end(ffb_ctx* c)
 {
   cudaEventRecord(c->ev1, c->stream);
   c->timed = true;
+}
+
+// ---------------------------------------------------------------------------
+// Scene upload and grid build on a SceneData
+// ---------------------------------------------------------------------------
+int scene_upload(ffb_ctx* c, SceneData& s, const float* faces9, int n_faces)
+{
+  s.grid_ok = false;
+  s.n_faces = n_faces;
+  if (n_faces == 0)
+    return FFB_OK;
+  const size_t bytes = sizeof(float) * 9 * (size_t)n_faces;
+  if (is_device_ptr(faces9)) {
+    FFB_TRY(ensure(c, s.faces, bytes));
+    FFB_CUDA(cudaMemcpyAsync(s.faces.ptr, faces9, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    FFB_TRY(upload(c, s.faces, faces9, bytes));
+  }
+  FFB_TRY(ensure(c, s.tri, sizeof(TriRec) * (size_t)n_faces));
+  FFB_TRY(ensure(c, s.box_lo, sizeof(float4) * (size_t)n_faces));
+  FFB_TRY(ensure(c, s.box_hi, sizeof(float4) * (size_t)n_faces));
+  FFB_TRY(ensure(c, s.scene_ord, sizeof(uint32_t) * 6));
+  uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+  FFB_TRY(upload(c, s.scene_ord, init, sizeof init));
+  k_face_prepare<<<grid_blocks(n_faces, 256), 256, 0, c->stream>>>(
+      dptr<float>(s.faces), n_faces, dptr<TriRec>(s.tri), dptr<float4>(s.box_lo), dptr<float4>(s.box_hi),
+      dptr<uint32_t>(s.scene_ord));
+  FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
+}
+
+int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
+{
+  s.grid_ok = false;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "grid build without a scene (or with an empty scene)");
+  ffb_grid_params P = {0, 0, 0, 2.f, 1};
+  if (params)
+    P = *params;
+  if (P.cells_per_face <= 0.f)
+    P.cells_per_face = 2.f;
+  if (P.nx < 0 || P.ny < 0 || P.nz < 0 || P.nx > kMaxDim || P.ny > kMaxDim || P.nz > kMaxDim)
+    return fail(FFB_ERR_TOO_LARGE, "grid dims %dx%dx%d outside [0, %d]", P.nx, P.ny, P.nz, kMaxDim);
+
+  uint32_t ord[6];
+  FFB_CUDA(cudaMemcpyAsync(ord, s.scene_ord.ptr, sizeof ord, cudaMemcpyDeviceToHost, c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  float smin[3], smax[3];
+  for (int a = 0; a < 3; ++a) {
+    smin[a] = ord2f(ord[a]);
+    smax[a] = ord2f(ord[3 + a]);
+  }
+  ffb_grid_info I{};
+  bool any = ord[0] != 0xFFFFFFFFu && smin[0] <= smax[0];
+  if (!any) {  // nothing can be hit: a single empty cell
+    for (int a = 0; a < 3; ++a) {
+      smin[a] = 0.f;
+      smax[a] = 1.f;
+    }
+  }
+  float max_ext = 0.f, max_abs = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    max_ext = std::max(max_ext, smax[a] - smin[a]);
+    max_abs = std::max(max_abs, std::max(std::fabs(smin[a]), std::fabs(smax[a])));
+  }
+  // margin: far above the rounding of a computed hit point (a few ulps of the
+  // coordinates) and far below a cell
+  const float margin = max_ext * 0x1p-12f + max_abs * 0x1p-17f + 1e-30f;
+  double ext[3];
+  for (int a = 0; a < 3; ++a) {
+    I.lo[a] = smin[a] - 2.f * margin;
+    I.hi[a] = smax[a] + 2.f * margin;
+    ext[a] = (double)I.hi[a] - (double)I.lo[a];
+  }
+  int dims[3] = {P.nx, P.ny, P.nz};
+  if (!any) {
+    dims[0] = dims[1] = dims[2] = 1;
+  } else if (!P.nx || !P.ny || !P.nz) {
+    double mx = std::max(ext[0], std::max(ext[1], ext[2]));
+    double vol = 1.0;
+    for (int a = 0; a < 3; ++a)
+      vol *= std::max(ext[a], mx / 32.0);
+    double target = (double)P.cells_per_face * s.n_faces;
+    double sc = std::cbrt(target / vol);
+    for (int a = 0; a < 3; ++a) {
+      if (!dims[a])
+        dims[a] = (int)std::min<double>(kMaxDim, std::max(1.0, std::round(ext[a] * sc)));
+    }
+  }
+  I.nx = dims[0];
+  I.ny = dims[1];
+  I.nz = dims[2];
+  for (int a = 0; a < 3; ++a)
+    I.cell[a] = (float)(ext[a] / dims[a]);
+  // the last boundary lo + n*cs must reach hi: nudge the cell size up if the
+  // float product falls short
+  for (int a = 0; a < 3; ++a) {
+    while (I.lo[a] + (float)dims[a] * I.cell[a] < I.hi[a])
+      I.cell[a] = std::nextafter(I.cell[a], INFINITY);
+    I.hi[a] = I.lo[a] + (float)dims[a] * I.cell[a];
+  }
+  I.margin = margin;
+  I.skip_empty = P.skip_empty ? 1 : 0;
+  const long long n_cells = (long long)I.nx * I.ny * I.nz;
+
+  FFB_TRY(ensure(c, s.cell_start, sizeof(uint32_t) * (size_t)(n_cells + 1)));
+  FFB_TRY(ensure(c, s.cell_fill, sizeof(uint32_t) * (size_t)n_cells));
+  FFB_CUDA(cudaMemsetAsync(s.cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
+  BinGeom bg;
+  bg.lo = make_float3(I.lo[0], I.lo[1], I.lo[2]);
+  bg.cs = make_float3(I.cell[0], I.cell[1], I.cell[2]);
+  bg.inv_cs = make_float3(1.f / I.cell[0], 1.f / I.cell[1], 1.f / I.cell[2]);
+  bg.nx = I.nx;
+  bg.ny = I.ny;
+  bg.nz = I.nz;
+  bg.margin = margin;
+  const int nb = grid_blocks(s.n_faces, 128);
+  k_grid_count<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(s.faces), dptr<float4>(s.box_lo), dptr<float4>(s.box_hi),
+                                          s.n_faces, dptr<uint32_t>(s.cell_fill));
+  FFB_CUDA(cudaGetLastError());
+  FFB_TRY(scan(c, dptr<uint32_t>(s.cell_fill), (int)n_cells, dptr<uint32_t>(s.cell_start)));
+  uint32_t total = 0;
+  FFB_CUDA(cudaMemcpyAsync(&total, dptr<uint32_t>(s.cell_start) + n_cells, sizeof total, cudaMemcpyDeviceToHost,
+                           c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  FFB_TRY(ensure(c, s.ref_tri, sizeof(int32_t) * (size_t)std::max<uint32_t>(total, 1)));
+  FFB_CUDA(cudaMemsetAsync(s.cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
+  k_grid_fill<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(s.faces), dptr<float4>(s.box_lo), dptr<float4>(s.box_hi),
+                                         s.n_faces, dptr<uint32_t>(s.cell_start), dptr<uint32_t>(s.cell_fill),
+                                         dptr<int32_t>(s.ref_tri));
+  k_cell_sort<<<grid_blocks(n_cells, 128), 128, 0, c->stream>>>(dptr<uint32_t>(s.cell_start), (int)n_cells,
+                                                                dptr<int32_t>(s.ref_tri));
+  FFB_TRY(ensure(c, s.ref_rec, sizeof(TriRec) * (size_t)std::max<uint32_t>(total, 1)));
+  k_ref_gather<<<grid_blocks(total, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+      dptr<int32_t>(s.ref_tri), total, dptr<TriRec>(s.tri), dptr<TriRec>(s.ref_rec));
+  FFB_CUDA(cudaGetLastError());
+  if (I.skip_empty) {
+    FFB_TRY(ensure(c, s.empty_dist, (size_t)n_cells));
+    uint8_t* d = dptr<uint8_t>(s.empty_dist);
+    k_empty_init<<<grid_blocks(n_cells, 256), 256, 0, c->stream>>>(dptr<uint32_t>(s.cell_start), (int)n_cells, d);
+    k_empty_pass<<<grid_blocks((long long)I.ny * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 0);
+    k_empty_pass<<<grid_blocks((long long)I.nx * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 1);
+    k_empty_pass<<<grid_blocks((long long)I.nx * I.ny, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 2);
+    FFB_CUDA(cudaGetLastError());
+  }
+  // live faces: those with a non-empty binning box
+  I.n_refs = total;
+  I.n_live_faces = 0;
+  {
+    std::vector<float4> lo((size_t)s.n_faces), hi((size_t)s.n_faces);
+    FFB_CUDA(cudaMemcpyAsync(lo.data(), s.box_lo.ptr, sizeof(float4) * lo.size(), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FFB_CUDA(cudaMemcpyAsync(hi.data(), s.box_hi.ptr, sizeof(float4) * hi.size(), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+    for (int f = 0; f < s.n_faces; ++f)
+      I.n_live_faces += lo[f].x <= hi[f].x;
+  }
+  s.info = I;
+  s.grid_ok = true;
+  return FFB_OK;
+}
+
+// Appends the chunks of face rays [0, front + rear) of every face.
+void add_chunks(std::vector<Chunk>& out, const int32_t* front, const int32_t* rear, int n_faces, int scene)
+{
+  for (int f = 0; f < n_faces; ++f) {
+    const int nf = front[f] + rear[f];
+    for (int j0 = 0; j0 < nf; j0 += kChunkRays)
+      out.push_back(Chunk{f, j0, (int16_t)std::min(kChunkRays, nf - j0), (int16_t)scene, front[f]});
+  }
+}
+
+int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long long* total)
+{
+  if (!front || !rear)
+    return fail(FFB_ERR_ARG, "null ray counts");
+  long long t = 0;
+  for (int f = 0; f < n_faces; ++f) {
+    if (front[f] < 0 || rear[f] < 0)
+      return fail(FFB_ERR_ARG, "negative ray count at face %d", f);
+    t += (long long)front[f] + rear[f];
+  }
+  *total = t;
+  return FFB_OK;
+}
+
+// Occupancy-sized persistent launch of the fused kernel for `n_chunks` chunks.
+template <bool kSkip, int kScenes>
+int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, bool timed)
+{
+  auto kern = k_form_factors<kSkip, kScenes>;
+  int per_sm = 0;
+  FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
+  // persistent blocks: a full wave, fewer when there are fewer chunks than warps
+  const long long wave = (long long)std::max(per_sm, 1) * c->n_sm;
+  const long long by_work = ((long long)p.n_chunks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
+  if (timed)
+    timing_begin(c);
+  kern<<<blocks, kTraceThreads, 0, c->stream>>>(p);
+  if (timed)
+    timing_end(c);
+  FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
 }
 
 }  // namespace
@@ -296,10 +526,13 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
     return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->faces,     &c->tri,       &c->box_lo,   &c->box_hi,     &c->frames,    &c->scene_ord,
-                    &c->cell_start, &c->cell_fill, &c->ref_tri,  &c->ref_rec,    &c->empty_dist, &c->scan_sums,
-                    &c->chunks,    &c->rows,      &c->cursor,   &c->stats,      &c->tmp_in,    &c->tmp_out,
-                    &c->tmp_out2,  &c->offsets,   &c->front_dev, &c->ray_cursor, &c->ff_counts};
+  release_scene(c, c->main);
+  for (SceneData& s : c->batch)
+    release_scene(c, s);
+  DevBuf* bufs[] = {&c->frames,   &c->batch_frames, &c->batch_chunks, &c->batch_keys, &c->batch_epoch,
+                    &c->scan_sums, &c->chunks,      &c->rows,         &c->cursor,     &c->stats,
+                    &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
+                    &c->ray_cursor, &c->ff_counts};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
@@ -343,173 +576,23 @@ extern "C" int ffb_scene_set(ffb_ctx* c, const float* faces9, int n_faces)
   FFB_TRY(check_ctx(c));
   if (n_faces < 0 || (n_faces > 0 && !faces9))
     return fail(FFB_ERR_ARG, "bad scene (n_faces=%d)", n_faces);
-  c->grid_ok = false;
   c->frames_mode = -1;
-  c->n_faces = n_faces;
-  if (n_faces == 0)
-    return FFB_OK;
-  const size_t bytes = sizeof(float) * 9 * (size_t)n_faces;
-  if (is_device_ptr(faces9)) {
-    FFB_TRY(ensure(c, c->faces, bytes));
-    FFB_CUDA(cudaMemcpyAsync(c->faces.ptr, faces9, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  } else {
-    FFB_TRY(upload(c, c->faces, faces9, bytes));
-  }
-  FFB_TRY(ensure(c, c->tri, sizeof(TriRec) * (size_t)n_faces));
-  FFB_TRY(ensure(c, c->box_lo, sizeof(float4) * (size_t)n_faces));
-  FFB_TRY(ensure(c, c->box_hi, sizeof(float4) * (size_t)n_faces));
-  FFB_TRY(ensure(c, c->scene_ord, sizeof(uint32_t) * 6));
-  uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
-  FFB_TRY(upload(c, c->scene_ord, init, sizeof init));
-  k_face_prepare<<<grid_blocks(n_faces, 256), 256, 0, c->stream>>>(
-      dptr<float>(c->faces), n_faces, dptr<TriRec>(c->tri), dptr<float4>(c->box_lo), dptr<float4>(c->box_hi),
-      dptr<uint32_t>(c->scene_ord));
-  FFB_CUDA(cudaGetLastError());
-  return FFB_OK;
+  return scene_upload(c, c->main, faces9, n_faces);
 }
 
 extern "C" int ffb_grid_build(ffb_ctx* c, const ffb_grid_params* params)
 {
   FFB_TRY(check_ctx(c));
-  c->grid_ok = false;
-  if (c->n_faces <= 0)
-    return fail(FFB_ERR_NO_SCENE, "grid build without a scene (or with an empty scene)");
-  ffb_grid_params P = {0, 0, 0, 2.f, 1};
-  if (params)
-    P = *params;
-  if (P.cells_per_face <= 0.f)
-    P.cells_per_face = 2.f;
-  if (P.nx < 0 || P.ny < 0 || P.nz < 0 || P.nx > kMaxDim || P.ny > kMaxDim || P.nz > kMaxDim)
-    return fail(FFB_ERR_TOO_LARGE, "grid dims %dx%dx%d outside [0, %d]", P.nx, P.ny, P.nz, kMaxDim);
-
-  uint32_t ord[6];
-  FFB_CUDA(cudaMemcpyAsync(ord, c->scene_ord.ptr, sizeof ord, cudaMemcpyDeviceToHost, c->stream));
-  FFB_CUDA(cudaStreamSynchronize(c->stream));
-  float smin[3], smax[3];
-  for (int a = 0; a < 3; ++a) {
-    smin[a] = ord2f(ord[a]);
-    smax[a] = ord2f(ord[3 + a]);
-  }
-  ffb_grid_info I{};
-  bool any = ord[0] != 0xFFFFFFFFu && smin[0] <= smax[0];
-  if (!any) {  // nothing can be hit: a single empty cell
-    for (int a = 0; a < 3; ++a) {
-      smin[a] = 0.f;
-      smax[a] = 1.f;
-    }
-  }
-  float max_ext = 0.f, max_abs = 0.f;
-  for (int a = 0; a < 3; ++a) {
-    max_ext = std::max(max_ext, smax[a] - smin[a]);
-    max_abs = std::max(max_abs, std::max(std::fabs(smin[a]), std::fabs(smax[a])));
-  }
-  // margin: far above the rounding of a computed hit point (a few ulps of the
-  // coordinates) and far below a cell
-  const float margin = max_ext * 0x1p-12f + max_abs * 0x1p-17f + 1e-30f;
-  double ext[3];
-  for (int a = 0; a < 3; ++a) {
-    I.lo[a] = smin[a] - 2.f * margin;
-    I.hi[a] = smax[a] + 2.f * margin;
-    ext[a] = (double)I.hi[a] - (double)I.lo[a];
-  }
-  int dims[3] = {P.nx, P.ny, P.nz};
-  if (!any) {
-    dims[0] = dims[1] = dims[2] = 1;
-  } else if (!P.nx || !P.ny || !P.nz) {
-    double mx = std::max(ext[0], std::max(ext[1], ext[2]));
-    double e2[3], vol = 1.0;
-    for (int a = 0; a < 3; ++a) {
-      e2[a] = std::max(ext[a], mx / 32.0);
-      vol *= e2[a];
-    }
-    double target = (double)P.cells_per_face * c->n_faces;
-    double s = std::cbrt(target / vol);
-    for (int a = 0; a < 3; ++a) {
-      if (!dims[a])
-        dims[a] = (int)std::min<double>(kMaxDim, std::max(1.0, std::round(ext[a] * s)));
-    }
-  }
-  I.nx = dims[0];
-  I.ny = dims[1];
-  I.nz = dims[2];
-  for (int a = 0; a < 3; ++a)
-    I.cell[a] = (float)(ext[a] / dims[a]);
-  // the last boundary lo + n*cs must reach hi: nudge the cell size up if the
-  // float product falls short
-  for (int a = 0; a < 3; ++a) {
-    while (I.lo[a] + (float)dims[a] * I.cell[a] < I.hi[a])
-      I.cell[a] = std::nextafter(I.cell[a], INFINITY);
-    I.hi[a] = I.lo[a] + (float)dims[a] * I.cell[a];
-  }
-  I.margin = margin;
-  I.skip_empty = P.skip_empty ? 1 : 0;
-  const long long n_cells = (long long)I.nx * I.ny * I.nz;
-
-  FFB_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (size_t)(n_cells + 1)));
-  FFB_TRY(ensure(c, c->cell_fill, sizeof(uint32_t) * (size_t)n_cells));
-  FFB_CUDA(cudaMemsetAsync(c->cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
-  BinGeom bg;
-  bg.lo = make_float3(I.lo[0], I.lo[1], I.lo[2]);
-  bg.cs = make_float3(I.cell[0], I.cell[1], I.cell[2]);
-  bg.inv_cs = make_float3(1.f / I.cell[0], 1.f / I.cell[1], 1.f / I.cell[2]);
-  bg.nx = I.nx;
-  bg.ny = I.ny;
-  bg.nz = I.nz;
-  bg.margin = margin;
-  const int nb = grid_blocks(c->n_faces, 128);
-  k_grid_count<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(c->faces), dptr<float4>(c->box_lo),
-                                          dptr<float4>(c->box_hi), c->n_faces, dptr<uint32_t>(c->cell_fill));
-  FFB_CUDA(cudaGetLastError());
-  FFB_TRY(scan(c, dptr<uint32_t>(c->cell_fill), (int)n_cells, dptr<uint32_t>(c->cell_start)));
-  uint32_t total = 0;
-  FFB_CUDA(cudaMemcpyAsync(&total, dptr<uint32_t>(c->cell_start) + n_cells, sizeof total, cudaMemcpyDeviceToHost,
-                           c->stream));
-  FFB_CUDA(cudaStreamSynchronize(c->stream));
-  FFB_TRY(ensure(c, c->ref_tri, sizeof(int32_t) * (size_t)std::max<uint32_t>(total, 1)));
-  FFB_CUDA(cudaMemsetAsync(c->cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
-  k_grid_fill<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(c->faces), dptr<float4>(c->box_lo),
-                                         dptr<float4>(c->box_hi), c->n_faces, dptr<uint32_t>(c->cell_start),
-                                         dptr<uint32_t>(c->cell_fill), dptr<int32_t>(c->ref_tri));
-  k_cell_sort<<<grid_blocks(n_cells, 128), 128, 0, c->stream>>>(dptr<uint32_t>(c->cell_start), (int)n_cells,
-                                                                dptr<int32_t>(c->ref_tri));
-  FFB_TRY(ensure(c, c->ref_rec, sizeof(TriRec) * (size_t)std::max<uint32_t>(total, 1)));
-  k_ref_gather<<<grid_blocks(total, 256, c->n_sm * 8), 256, 0, c->stream>>>(
-      dptr<int32_t>(c->ref_tri), total, dptr<TriRec>(c->tri), dptr<TriRec>(c->ref_rec));
-  FFB_CUDA(cudaGetLastError());
-  if (I.skip_empty) {
-    FFB_TRY(ensure(c, c->empty_dist, (size_t)n_cells));
-    uint8_t* d = dptr<uint8_t>(c->empty_dist);
-    k_empty_init<<<grid_blocks(n_cells, 256), 256, 0, c->stream>>>(dptr<uint32_t>(c->cell_start), (int)n_cells, d);
-    k_empty_pass<<<grid_blocks((long long)I.ny * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 0);
-    k_empty_pass<<<grid_blocks((long long)I.nx * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 1);
-    k_empty_pass<<<grid_blocks((long long)I.nx * I.ny, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 2);
-    FFB_CUDA(cudaGetLastError());
-  }
-  // live faces: those with a non-empty binning box
-  I.n_refs = total;
-  I.n_live_faces = 0;
-  {
-    std::vector<float4> lo((size_t)c->n_faces), hi((size_t)c->n_faces);
-    FFB_CUDA(cudaMemcpyAsync(lo.data(), c->box_lo.ptr, sizeof(float4) * lo.size(), cudaMemcpyDeviceToHost,
-                             c->stream));
-    FFB_CUDA(cudaMemcpyAsync(hi.data(), c->box_hi.ptr, sizeof(float4) * hi.size(), cudaMemcpyDeviceToHost,
-                             c->stream));
-    FFB_CUDA(cudaStreamSynchronize(c->stream));
-    for (int f = 0; f < c->n_faces; ++f)
-      I.n_live_faces += lo[f].x <= hi[f].x;
-  }
-  c->info = I;
-  c->grid_ok = true;
-  return FFB_OK;
+  return grid_build(c, c->main, params);
 }
 
 extern "C" int ffb_grid_info_get(ffb_ctx* c, ffb_grid_info* out)
 {
   if (!c || !out)
     return fail(FFB_ERR_ARG, "null argument");
-  if (!c->grid_ok)
+  if (!c->main.grid_ok)
     return fail(FFB_ERR_NO_GRID, "no grid built");
-  *out = c->info;
+  *out = c->main.info;
   return FFB_OK;
 }
 
@@ -559,9 +642,10 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
   FFB_TRY(check_ctx(c));
   if (n_rays < 0 || (n_rays > 0 && (!rays6 || !hit_face)))
     return fail(FFB_ERR_ARG, "bad cast arguments");
-  if (c->n_faces < 0)
+  SceneData& s = c->main;
+  if (s.n_faces < 0)
     return fail(FFB_ERR_NO_SCENE, "cast without a scene");
-  if (!brute && !c->grid_ok)
+  if (!brute && !s.grid_ok)
     return fail(FFB_ERR_NO_GRID, "cast before ffb_grid_build");
   if (n_rays == 0)
     return FFB_OK;
@@ -574,11 +658,11 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
   timing_begin(c);
-  if (brute || c->n_faces == 0) {
+  if (brute || s.n_faces == 0) {
     k_cast_brute<<<grid_blocks(n_rays, kTraceThreads), kTraceThreads, 0, c->stream>>>(
-        dptr<TriRec>(c->tri), c->n_faces, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit, (float*)d_pt);
+        dptr<TriRec>(s.tri), s.n_faces, (const float*)d_rays, (long)n_rays, (int32_t*)d_hit, (float*)d_pt);
   } else {
-    GridView g = make_view(c);
+    GridView g = make_view(s);
     FFB_TRY(ensure(c, c->ray_cursor, sizeof(unsigned long long)));
     FFB_CUDA(cudaMemsetAsync(c->ray_cursor.ptr, 0, sizeof(unsigned long long), c->stream));
     auto kern = g.empty_dist ? k_cast<true> : k_cast<false>;
@@ -616,50 +700,31 @@ extern "C" int ffb_cast_bruteforce(ffb_ctx* c, const float* rays6, long long n_r
 // ===========================================================================
 // Emission and form factors
 // ===========================================================================
-namespace {
-
-int check_counts(ffb_ctx* c, const int32_t* front, const int32_t* rear, long long* total)
-{
-  if (c->n_faces <= 0)
-    return fail(FFB_ERR_NO_SCENE, "no scene");
-  if (!front || !rear)
-    return fail(FFB_ERR_ARG, "null ray counts");
-  long long t = 0;
-  for (int f = 0; f < c->n_faces; ++f) {
-    if (front[f] < 0 || rear[f] < 0)
-      return fail(FFB_ERR_ARG, "negative ray count at face %d", f);
-    t += (long long)front[f] + rear[f];
-  }
-  *total = t;
-  return FFB_OK;
-}
-
-}  // namespace
-
 extern "C" int ffb_emit(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
                         int flags, float* rays6)
 {
   FFB_TRY(check_ctx(c));
+  if (c->main.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  const int n_faces = c->main.n_faces;
   long long total = 0;
-  FFB_TRY(check_counts(c, front, rear, &total));
+  FFB_TRY(check_counts(n_faces, front, rear, &total));
   if (total == 0)
     return FFB_OK;
   if (!rays6)
     return fail(FFB_ERR_ARG, "null ray output");
   FFB_TRY(ensure_frames(c, flags));
-  std::vector<long long> offs((size_t)c->n_faces + 1);
+  std::vector<long long> offs((size_t)n_faces + 1);
   offs[0] = 0;
-  for (int f = 0; f < c->n_faces; ++f)
+  for (int f = 0; f < n_faces; ++f)
     offs[f + 1] = offs[f] + front[f] + rear[f];
   FFB_TRY(upload(c, c->offsets, offs.data(), sizeof(long long) * offs.size()));
-  // front counts after the offsets in the same stage would race the stage;
-  // upload() waits for the previous copy, so sequential uploads are safe
-  FFB_TRY(upload(c, c->front_dev, front, sizeof(int32_t) * (size_t)c->n_faces));
+  FFB_TRY(upload(c, c->front_dev, front, sizeof(int32_t) * (size_t)n_faces));
   void* d_rays;
   bool host_out;
   FFB_TRY(output_ptr(c, rays6, sizeof(float) * 6 * (size_t)total, c->tmp_out, &d_rays, &host_out));
   k_emit<<<grid_blocks(total, 256, c->n_sm * 32), 256, 0, c->stream>>>(
-      dptr<float>(c->frames), dptr<long long>(c->offsets), dptr<int32_t>(c->front_dev), c->n_faces, (long)total,
+      dptr<float>(c->frames), dptr<long long>(c->offsets), dptr<int32_t>(c->front_dev), n_faces, (long)total,
       (uint32_t)seed, (uint32_t)(seed >> 32), epoch, (float*)d_rays);
   FFB_CUDA(cudaGetLastError());
   if (host_out) {
@@ -674,18 +739,21 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
                                       uint32_t* counts)
 {
   FFB_TRY(check_ctx(c));
-  if (!c->grid_ok)
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!s.grid_ok)
     return fail(FFB_ERR_NO_GRID, "form factors before ffb_grid_build");
   long long total = 0;
-  FFB_TRY(check_counts(c, front, rear, &total));
+  FFB_TRY(check_counts(s.n_faces, front, rear, &total));
   if (!counts)
     return fail(FFB_ERR_ARG, "null counts");
-  if (!face_to_row && n_rows != c->n_faces)
-    return fail(FFB_ERR_ARG, "identity rows need n_rows == n_faces (%d != %d)", n_rows, c->n_faces);
+  if (!face_to_row && n_rows != s.n_faces)
+    return fail(FFB_ERR_ARG, "identity rows need n_rows == n_faces (%d != %d)", n_rows, s.n_faces);
   if (n_rows <= 0)
     return fail(FFB_ERR_ARG, "n_rows must be positive");
   if (face_to_row) {
-    for (int f = 0; f < c->n_faces; ++f)
+    for (int f = 0; f < s.n_faces; ++f)
       if (face_to_row[f] < 0 || face_to_row[f] >= n_rows)
         return fail(FFB_ERR_ARG, "face_to_row[%d] = %d outside [0, %d)", f, face_to_row[f], n_rows);
   }
@@ -693,12 +761,8 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
     return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
   FFB_TRY(ensure_frames(c, flags));
   std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / kChunkRays + c->n_faces));
-  for (int f = 0; f < c->n_faces; ++f) {
-    const int nf = front[f] + rear[f];
-    for (int j0 = 0; j0 < nf; j0 += kChunkRays)
-      chunks.push_back(Chunk{f, j0, std::min(kChunkRays, nf - j0), front[f]});
-  }
+  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
+  add_chunks(chunks, front, rear, s.n_faces, 0);
   const size_t mat = (size_t)n_rows * n_rows;
   void* d_counts;
   bool host_out;
@@ -709,33 +773,29 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
   if (!chunks.empty()) {
     FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
     if (face_to_row)
-      FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)c->n_faces));
+      FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)s.n_faces));
     FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
     FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
-    TraceParams p;
-    p.g = make_view(c);
+    TraceParams<1> p;
     p.frames = dptr<float>(c->frames);
     p.chunks = dptr<Chunk>(c->chunks);
     p.n_chunks = (int)chunks.size();
-    p.face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
-    p.n_cols = n_rows;
-    p.counts = (uint32_t*)d_counts;
     p.key0 = (uint32_t)seed;
     p.key1 = (uint32_t)(seed >> 32);
     p.epoch = epoch;
+    p.epoch_ptr = nullptr;
+    p.scene_keys = nullptr;
     p.chunk_cursor = dptr<uint32_t>(c->cursor);
     p.stats = dptr<unsigned long long>(c->stats);
-    void (*kern)(TraceParams) = p.g.empty_dist ? k_form_factors<true> : k_form_factors<false>;
-    int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
-    // persistent blocks: a full wave, fewer when there are fewer chunks than warps
-    const long long wave = (long long)std::max(per_sm, 1) * c->n_sm;
-    const long long by_work = ((long long)chunks.size() + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
-    timing_begin(c);
-    kern<<<blocks, kTraceThreads, 0, c->stream>>>(p);
-    timing_end(c);
-    FFB_CUDA(cudaGetLastError());
+    p.scenes[0].g = make_view(s);
+    p.scenes[0].counts = (uint32_t*)d_counts;
+    p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
+    p.scenes[0].face_base = 0;
+    p.scenes[0].n_cols = n_rows;
+    if (p.scenes[0].g.empty_dist)
+      FFB_TRY((launch_fused<true, 1>(c, p, true)));
+    else
+      FFB_TRY((launch_fused<false, 1>(c, p, true)));
   }
   if (host_out) {
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * mat));
@@ -779,6 +839,143 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   FFB_TRY(ffb_form_factor_counts(c, front, rear, seed, epoch, flags, face_to_row, n_rows,
                                  dptr<uint32_t>(c->ff_counts)));
   return ffb_normalise(c, dptr<uint32_t>(c->ff_counts), outgoing, n_rows, ff);
+}
+
+// ===========================================================================
+// Batched scenes: one fused launch over many independent scenes
+// ===========================================================================
+extern "C" int ffb_batch_set(ffb_ctx* c, int n_scenes, const long long* face_offsets, const float* faces9,
+                             const ffb_grid_params* params)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_scenes <= 0 || n_scenes > kMaxBatchScenes || !face_offsets || !faces9)
+    return fail(FFB_ERR_ARG, "batch of %d scenes (1..%d) without offsets or faces", n_scenes, kMaxBatchScenes);
+  for (int s = 0; s < n_scenes; ++s) {
+    const long long n = face_offsets[s + 1] - face_offsets[s];
+    if (face_offsets[s] < 0 || n <= 0 || n > 0x7FFFFFFF)
+      return fail(FFB_ERR_ARG, "scene %d has %lld faces", s, n);
+  }
+  for (SceneData& s : c->batch)
+    release_scene(c, s);
+  c->batch.clear();
+  c->batch.resize((size_t)n_scenes);
+  c->batch_offsets.assign(face_offsets, face_offsets + n_scenes + 1);
+  c->batch_frames_mode = -1;
+  c->batch_n_chunks = 0;
+  for (int s = 0; s < n_scenes; ++s) {
+    const long long f0 = face_offsets[s];
+    const int n = (int)(face_offsets[s + 1] - f0);
+    FFB_TRY(scene_upload(c, c->batch[s], faces9 + 9 * f0, n));
+    FFB_TRY(grid_build(c, c->batch[s], params ? params + s : nullptr));
+  }
+  return FFB_OK;
+}
+
+extern "C" int ffb_batch_grid_info(ffb_ctx* c, int scene, ffb_grid_info* out)
+{
+  if (!c || !out || scene < 0 || scene >= (int)c->batch.size())
+    return fail(FFB_ERR_ARG, "bad batch scene %d", scene);
+  *out = c->batch[scene].info;
+  return FFB_OK;
+}
+
+extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, const uint64_t* seeds,
+                                 int flags)
+{
+  FFB_TRY(check_ctx(c));
+  const int n_scenes = (int)c->batch.size();
+  if (!n_scenes)
+    return fail(FFB_ERR_NO_SCENE, "no batch set");
+  const long long n_all = c->batch_offsets[n_scenes];
+  long long total = 0;
+  FFB_TRY(check_counts((int)n_all, front, rear, &total));
+  std::vector<Chunk> chunks;
+  chunks.reserve((size_t)(total / kChunkRays + n_all));
+  for (int s = 0; s < n_scenes; ++s) {
+    const long long f0 = c->batch_offsets[s];
+    add_chunks(chunks, front + f0, rear + f0, c->batch[s].n_faces, s);
+  }
+  c->batch_n_chunks = (int)chunks.size();
+  if (!chunks.empty())
+    FFB_TRY(upload(c, c->batch_chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
+  std::vector<uint2> keys((size_t)n_scenes);
+  for (int s = 0; s < n_scenes; ++s) {
+    const uint64_t k = seeds ? seeds[s] : 1;
+    keys[s] = make_uint2((uint32_t)k, (uint32_t)(k >> 32));
+  }
+  FFB_TRY(upload(c, c->batch_keys, keys.data(), sizeof(uint2) * keys.size()));
+  const int mode = flags & FFB_EMIT_REF_NORMAL;
+  if (c->batch_frames_mode != mode) {
+    FFB_TRY(ensure(c, c->batch_frames, sizeof(float) * 20 * (size_t)n_all));
+    for (int s = 0; s < n_scenes; ++s)
+      FFB_TRY(build_frames(c, dptr<float>(c->batch[s].faces), c->batch[s].n_faces, mode,
+                           dptr<float>(c->batch_frames) + 20 * c->batch_offsets[s]));
+    c->batch_frames_mode = mode;
+  }
+  FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
+  FFB_TRY(ensure(c, c->batch_epoch, sizeof(uint32_t)));
+  FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
+  FFB_CUDA(cudaMemsetAsync(c->batch_epoch.ptr, 0, sizeof(uint32_t), c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  return FFB_OK;
+}
+
+extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned long long* counts_offsets,
+                                unsigned long long counts_words, int advance_epoch)
+{
+  FFB_TRY(check_ctx(c));
+  const int n_scenes = (int)c->batch.size();
+  if (!n_scenes || !c->batch_keys.ptr)
+    return fail(FFB_ERR_NO_SCENE, "batch not set and prepared");
+  if (!counts || !counts_offsets)
+    return fail(FFB_ERR_ARG, "null counts");
+  for (int s = 0; s < n_scenes; ++s) {
+    const unsigned long long n = (unsigned long long)c->batch[s].n_faces;
+    if (counts_offsets[s] + n * n > counts_words)
+      return fail(FFB_ERR_ARG, "scene %d matrix beyond the counts buffer", s);
+    if (c->batch[s].n_faces > kMaxRows)
+      return fail(FFB_ERR_TOO_LARGE, "scene %d has more than %d faces", s, kMaxRows);
+  }
+  if (!is_device_ptr(counts))
+    return fail(FFB_ERR_ARG, "batched counts must be device memory");
+  FFB_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * counts_words, c->stream));
+  FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
+  FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
+  if (advance_epoch) {
+    k_epoch_bump<<<1, 32, 0, c->stream>>>(dptr<uint32_t>(c->batch_epoch));
+    FFB_CUDA(cudaGetLastError());
+  }
+  if (c->batch_n_chunks == 0)
+    return FFB_OK;
+  TraceParams<kMaxBatchScenes> p;
+  p.frames = dptr<float>(c->batch_frames);
+  p.chunks = dptr<Chunk>(c->batch_chunks);
+  p.n_chunks = c->batch_n_chunks;
+  p.key0 = p.key1 = p.epoch = 0;
+  p.epoch_ptr = dptr<uint32_t>(c->batch_epoch);
+  p.scene_keys = dptr<uint2>(c->batch_keys);
+  p.chunk_cursor = dptr<uint32_t>(c->cursor);
+  p.stats = dptr<unsigned long long>(c->stats);
+  // all scenes share one kernel variant: empty-space jumps need every
+  // scene's distance map
+  bool skip = true;
+  for (int s = 0; s < kMaxBatchScenes; ++s) {
+    SceneSlot& slot = p.scenes[s];
+    memset(&slot, 0, sizeof slot);
+    if (s >= n_scenes)
+      continue;
+    slot.g = make_view(c->batch[s]);
+    slot.counts = counts + counts_offsets[s];
+    slot.face_to_row = nullptr;
+    slot.face_base = (int)c->batch_offsets[s];
+    slot.n_cols = c->batch[s].n_faces;
+    skip = skip && slot.g.empty_dist != nullptr;
+  }
+  if (skip)
+    FFB_TRY((launch_fused<true, kMaxBatchScenes>(c, p, false)));
+  else
+    FFB_TRY((launch_fused<false, kMaxBatchScenes>(c, p, false)));
+  return FFB_OK;
 }
 
 extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)

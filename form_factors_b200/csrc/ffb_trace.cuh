@@ -8,28 +8,43 @@
 namespace ffb {
 
 // A unit of work of the fused kernel: `count` consecutive rays [j0, j0+count)
-// of one face.  Rays j < front leave the front side, the others the rear.
+// of face `face` (index within its scene) of scene `scene`.  Rays j < front
+// leave the front side, the others the rear.
 struct Chunk {
   int32_t face;
   int32_t j0;
-  int32_t count;
+  int16_t count;
+  int16_t scene;
   int32_t front;
 };
 
 // Statistics slots (uint64 each), accumulated once per warp.
 enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatSlots = 4 };
 
-struct TraceParams {
+// One scene of a fused launch: its grid, its count matrix and where its faces
+// start in the launch's frame table.
+struct SceneSlot {
   GridView g;
-  const float* __restrict__ frames;          // 20 floats per face
+  uint32_t* __restrict__ counts;              // n_cols * n_cols
+  const int32_t* __restrict__ face_to_row;   // face -> matrix row/column (mesh), or null for identity
+  int face_base;                              // first frame of the scene
+  int n_cols;                                 // matrix side
+};
+
+// Up to 256 scenes ride in the kernel parameter space (32 KB on sm_100).
+constexpr int kMaxBatchScenes = 256;
+
+template <int kScenes>
+struct TraceParams {
+  const float* __restrict__ frames;          // 20 floats per face, scenes concatenated
   const Chunk* __restrict__ chunks;
   int n_chunks;
-  const int32_t* __restrict__ face_to_row;   // face -> matrix row/column (mesh), or null for identity
-  int n_cols;                                 // matrix side
-  uint32_t* __restrict__ counts;              // n_cols * n_cols
   uint32_t key0, key1, epoch;
+  const uint32_t* __restrict__ epoch_ptr;    // when set, the epoch is read from device memory
+  const uint2* __restrict__ scene_keys;      // per-scene Philox key, or null for (key0, key1)
   uint32_t* __restrict__ chunk_cursor;        // work counter, zero before the launch
   unsigned long long* __restrict__ stats;     // kStatSlots, or null
+  SceneSlot scenes[kScenes];
 };
 
 constexpr int kTraceThreads = 128;
@@ -108,10 +123,15 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // the grid traversal state machine one unit of work per iteration.  A finished
 // hit adds one to the warp's shared-memory hash histogram keyed by the matrix
 // index row(f) * n_cols + row(h); the warp flushes the table to the global
-// uint32 matrix with atomic adds when it is half full and at the end.
+// uint32 matrix with atomic adds when it is half full, when it changes scene
+// and at the end.
+//
+// With several scenes in one launch a warp works on one scene at a time: a
+// chunk of another scene is taken only once every lane is idle (drain before
+// switch), so that the scene's grid is warp-uniform.
 // ---------------------------------------------------------------------------
-template <bool kSkip>
-__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(TraceParams p)
+template <bool kSkip, int kScenes>
+__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams<kScenes> p)
 {
   __shared__ uint32_t s_keys[kWarpsPerBlock][kWarpHash];
   __shared__ uint32_t s_vals[kWarpsPerBlock][kWarpHash];
@@ -123,10 +143,19 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     vals[i] = 0;
   }
   __syncwarp();
+  const uint32_t epoch = p.epoch_ptr ? *p.epoch_ptr : p.epoch;
   const unsigned lane_below = (1u << lane) - 1u;
   int fill = 0;  // occupied slots (warp-uniform)
-  // current chunk (warp-uniform)
+  // current chunk and scene (warp-uniform)
   int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0;
+  int scene = 0;
+  uint32_t key0 = p.key0, key1 = p.key1;
+  if (p.scene_keys) {
+    const uint2 k = p.scene_keys[0];
+    key0 = k.x;
+    key1 = k.y;
+  }
+  int pending = -1;  // a fetched chunk of another scene, waiting for the warp to drain
   bool exhausted = false;
   // lane state
   Tracer T;
@@ -137,31 +166,50 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     unsigned need = __ballot_sync(kFull, !active);
     while (need && !exhausted) {
       if (c_left == 0) {
-        int k = 0;
-        if (lane == 0)
-          k = (int)atomicAdd(p.chunk_cursor, 1u);
-        k = __shfl_sync(kFull, k, 0);
-        if (k >= p.n_chunks) {
-          exhausted = true;
-          break;
+        int k = pending;
+        if (k < 0) {
+          if (lane == 0)
+            k = (int)atomicAdd(p.chunk_cursor, 1u);
+          k = __shfl_sync(kFull, k, 0);
+          if (k >= p.n_chunks) {
+            exhausted = true;
+            break;
+          }
         }
         const Chunk ch = p.chunks[k];
+        if (kScenes > 1 && ch.scene != scene) {
+          if (__any_sync(kFull, active)) {  // drain before switching scene
+            pending = k;
+            break;
+          }
+          warp_hash_flush(keys, vals, p.scenes[scene].counts, lane);
+          fill = 0;
+          scene = ch.scene;
+          if (p.scene_keys) {
+            const uint2 sk = p.scene_keys[scene];
+            key0 = sk.x;
+            key1 = sk.y;
+          }
+        }
+        pending = -1;
+        const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
         c_face = ch.face;
         c_j = ch.j0;
         c_left = ch.count;
         c_front = ch.front;
-        c_row = p.face_to_row ? __ldg(p.face_to_row + ch.face) : ch.face;
+        c_row = S.face_to_row ? __ldg(S.face_to_row + ch.face) : ch.face;
       }
+      const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
       const int take = min(__popc(need), c_left);
       const int rank = __popc(need & lane_below);
       const bool mine = ((need >> lane) & 1u) && rank < take;
       if (mine) {
         float3 o, e;
-        emit_ray(p.frames + 20 * (size_t)c_face, (uint32_t)c_face, (uint32_t)(c_j + rank), c_front, p.key0, p.key1,
-                 p.epoch, o, e);
+        emit_ray(p.frames + 20 * ((size_t)S.face_base + c_face), (uint32_t)c_face, (uint32_t)(c_j + rank), c_front,
+                 key0, key1, epoch, o, e);
         ++n_rays;
         my_row = c_row;
-        active = tracer_begin<kSkip>(T, p.g, o, e, n_cells);
+        active = tracer_begin<kSkip>(T, S.g, o, e, n_cells);
       }
       need &= ~__ballot_sync(kFull, mine);
       c_j += take;
@@ -169,29 +217,38 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     }
     if (exhausted && !__any_sync(kFull, active))
       break;
+    const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
     int hit = -1;
     if (active) {
       if (T.i < T.en) {
-        tracer_test(T, p.g, n_tests);
-      } else if (!tracer_advance<kSkip>(T, p.g, n_cells)) {
+        tracer_test(T, S.g, n_tests);
+      } else if (!tracer_advance<kSkip>(T, S.g, n_cells)) {
         active = false;
-        hit = tracer_result(T, p.g);
+        hit = tracer_result(T, S.g);
       }
     }
     bool fresh = false;
     if (hit >= 0) {
       ++n_hits;
-      const int col = p.face_to_row ? __ldg(p.face_to_row + hit) : hit;
-      fresh = warp_hash_add(keys, vals, (uint32_t)my_row * (uint32_t)p.n_cols + (uint32_t)col, p.counts);
+      const int col = S.face_to_row ? __ldg(S.face_to_row + hit) : hit;
+      fresh = warp_hash_add(keys, vals, (uint32_t)my_row * (uint32_t)S.n_cols + (uint32_t)col, S.counts);
     }
     fill += __popc(__ballot_sync(kFull, fresh));
     if (fill > kWarpHash / 2) {
-      warp_hash_flush(keys, vals, p.counts, lane);
+      warp_hash_flush(keys, vals, S.counts, lane);
       fill = 0;
     }
   }
-  warp_hash_flush(keys, vals, p.counts, lane);
+  warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
   warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
+}
+
+// Advances the device-resident Philox epoch of a captured launch, so that every
+// replay of a CUDA graph draws fresh rays.
+__global__ void k_epoch_bump(uint32_t* epoch)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    *epoch += 1;
 }
 
 // ---------------------------------------------------------------------------

@@ -83,6 +83,11 @@ def load(path=LIB_PATH):
         "ffb_normalise": (i32, [vp, vp, vp, i32, vp]),
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
         "ffb_cast_bruteforce_static": (i32, [vp, i32, vp, i64, vp, vp, vp]),
+        "ffb_form_factors": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp, vp]),
+        "ffb_batch_set": (i32, [vp, i32, vp, vp, vp]),
+        "ffb_batch_grid_info": (i32, [vp, i32, C.POINTER(GridInfo)]),
+        "ffb_batch_prepare": (i32, [vp, vp, vp, vp, i32]),
+        "ffb_batch_launch": (i32, [vp, vp, vp, C.c_ulonglong, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -229,6 +234,67 @@ class Context:
             out = np.empty((n, n), np.float32)
         _check(self._lib.ffb_normalise(self._h, _ptr(counts), _ptr(outgoing), n, _ptr(out)))
         return out
+
+    def form_factors(self, front, rear, seed, epoch=0, flags=0, face_to_row=None, n_rows=None, outgoing=None,
+                     out=None):
+        """Counts and row normalisation in one call (ffb_form_factors)."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        if face_to_row is not None:
+            face_to_row = np.ascontiguousarray(face_to_row, np.int32)
+        if n_rows is None:
+            n_rows = self.n_faces if face_to_row is None else int(face_to_row.max()) + 1
+        if outgoing is None:
+            rows = np.arange(self.n_faces) if face_to_row is None else face_to_row
+            outgoing = np.zeros(n_rows, np.int64)
+            np.add.at(outgoing, rows, front.astype(np.int64) + rear)
+        outgoing = np.ascontiguousarray(outgoing, np.int32)
+        if out is None:
+            out = np.empty((n_rows, n_rows), np.float32)
+        _check(self._lib.ffb_form_factors(self._h, _ptr(front), _ptr(rear), int(seed), int(epoch), int(flags),
+                                          _ptr(face_to_row), int(n_rows), _ptr(outgoing), _ptr(out)))
+        return out
+
+    # ---- batched scenes -------------------------------------------------
+    def batch_set(self, scenes_faces, cells_per_face=32.0, skip_empty=True, dims=None):
+        """Uploads a list of (n_i, 9) float32 scenes and builds their grids."""
+        sizes = [len(f) for f in scenes_faces]
+        offsets = np.zeros(len(sizes) + 1, np.int64)
+        offsets[1:] = np.cumsum(sizes)
+        faces = np.ascontiguousarray(np.concatenate(scenes_faces), np.float32)
+        params = (GridParams * len(sizes))()
+        for i in range(len(sizes)):
+            params[i] = GridParams(0, 0, 0, float(cells_per_face), int(bool(skip_empty)))
+            if dims is not None:
+                params[i].nx, params[i].ny, params[i].nz = dims[i]
+        _check(self._lib.ffb_batch_set(self._h, len(sizes), _ptr(offsets), _ptr(faces), C.cast(params, C.c_void_p)))
+        self.batch_sizes = sizes
+        self.batch_offsets = offsets
+        return offsets
+
+    def batch_grid_info(self, scene):
+        info = GridInfo()
+        _check(self._lib.ffb_batch_grid_info(self._h, int(scene), C.byref(info)))
+        return info
+
+    def batch_prepare(self, front, rear, seeds=None, flags=0):
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        if seeds is not None:
+            seeds = np.ascontiguousarray(seeds, np.uint64)
+        _check(self._lib.ffb_batch_prepare(self._h, _ptr(front), _ptr(rear), _ptr(seeds), int(flags)))
+
+    def batch_counts_layout(self):
+        """(offsets, words): where each scene's N x N matrix starts in one buffer."""
+        sq = np.array([n * n for n in self.batch_sizes], np.uint64)
+        offs = np.zeros(len(sq), np.uint64)
+        offs[1:] = np.cumsum(sq)[:-1]
+        return np.ascontiguousarray(offs), int(sq.sum())
+
+    def batch_launch(self, counts, counts_offsets, advance_epoch=True):
+        counts_offsets = np.ascontiguousarray(counts_offsets, np.uint64)
+        words = int(counts.numel()) if hasattr(counts, "numel") else int(counts.size)
+        _check(self._lib.ffb_batch_launch(self._h, _ptr(counts), _ptr(counts_offsets), words, int(bool(advance_epoch))))
 
     def stats(self):
         s = Stats()
