@@ -20,7 +20,7 @@ FFB_OK = 0
 FFB_EMIT_REF_NORMAL = 1
 ERRORS = {
     -301: "FFB_ERR_ARG", -302: "FFB_ERR_CUDA", -303: "FFB_ERR_NO_SCENE", -304: "FFB_ERR_NO_GRID",
-    -305: "FFB_ERR_NO_MEMORY", -306: "FFB_ERR_TOO_LARGE", -307: "FFB_ERR_NO_DEVICE",
+    -305: "FFB_ERR_NO_MEMORY", -306: "FFB_ERR_TOO_LARGE", -307: "FFB_ERR_NO_DEVICE", -308: "FFB_ERR_TIMEOUT",
 }
 
 
@@ -44,6 +44,16 @@ class GridInfo(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("tests", C.c_ulonglong), ("cells", C.c_ulonglong), ("rays", C.c_ulonglong),
                 ("hits", C.c_ulonglong), ("kernel_ms", C.c_float)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("error", C.c_int), ("n_faces", C.c_int), ("queue_s", C.c_double),
+                ("latency_s", C.c_double), ("gpu_ms", C.c_double)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("queued", C.c_int), ("running", C.c_int), ("peak_running", C.c_int),
+                ("reserved_bytes", C.c_ulonglong), ("budget_bytes", C.c_ulonglong)]
 
 
 _lib = None
@@ -88,6 +98,13 @@ def load(path=LIB_PATH):
         "ffb_batch_grid_info": (i32, [vp, i32, C.POINTER(GridInfo)]),
         "ffb_batch_prepare": (i32, [vp, vp, vp, vp, i32]),
         "ffb_batch_launch": (i32, [vp, vp, vp, C.c_ulonglong, i32]),
+        "ffb_server_create": (i32, [i32, C.c_ulonglong, i32, C.POINTER(vp)]),
+        "ffb_server_destroy": (None, [vp]),
+        "ffb_server_submit": (i32, [vp, vp, i32, i32, u64, i32, C.c_float, C.POINTER(C.c_longlong)]),
+        "ffb_server_wait": (i32, [vp, C.c_longlong, C.c_double, C.POINTER(RequestInfo)]),
+        "ffb_server_result": (i32, [vp, C.c_longlong, vp]),
+        "ffb_server_release": (i32, [vp, C.c_longlong]),
+        "ffb_server_stats": (i32, [vp, C.POINTER(ServerInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -300,3 +317,51 @@ class Context:
         s = Stats()
         _check(self._lib.ffb_stats_get(self._h, C.byref(s)))
         return s
+
+
+class Server:
+    """Request loop over the C ABI's ffb_server_* (admission by memory budget,
+    concurrent slots, resident results)."""
+
+    def __init__(self, device=0, budget_bytes=0, slots=4):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.ffb_server_create(int(device), int(budget_bytes), int(slots), C.byref(h)))
+        self._h, self._lib = h, lib
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ffb_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, faces, rays_per_face, seed, flags=0, cells_per_face=32.0):
+        faces = np.ascontiguousarray(faces, np.float32).reshape(-1, 9)
+        rid = C.c_longlong()
+        _check(self._lib.ffb_server_submit(self._h, _ptr(faces), len(faces), int(rays_per_face), int(seed),
+                                           int(flags), float(cells_per_face), C.byref(rid)))
+        return rid.value
+
+    def wait(self, rid, timeout_s=-1.0):
+        info = RequestInfo()
+        _check(self._lib.ffb_server_wait(self._h, int(rid), float(timeout_s), C.byref(info)))
+        return info
+
+    def result(self, rid, n_faces, out=None):
+        if out is None:
+            out = np.empty((n_faces, n_faces), np.uint32)
+        _check(self._lib.ffb_server_result(self._h, int(rid), _ptr(out)))
+        return out
+
+    def release(self, rid):
+        _check(self._lib.ffb_server_release(self._h, int(rid)))
+
+    def stats(self):
+        info = ServerInfo()
+        _check(self._lib.ffb_server_stats(self._h, C.byref(info)))
+        return info

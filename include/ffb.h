@@ -37,6 +37,7 @@ extern "C" {
 #define FFB_ERR_NO_MEMORY (-305) /* device allocation failed or over the context budget */
 #define FFB_ERR_TOO_LARGE (-306) /* a size beyond a documented limit */
 #define FFB_ERR_NO_DEVICE (-307) /* no CUDA device / not an sm_100 device */
+#define FFB_ERR_TIMEOUT (-308)   /* a wait ended before the work finished */
 
 /* Emission flag: rotate +z towards the raw cross-product normal, as the
  * reference's emission/malley_cpu.cpp:125-129 does.  Without it the normal is
@@ -154,6 +155,50 @@ int ffb_batch_prepare(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, c
  * enqueues work on the context stream (capturable). */
 int ffb_batch_launch(ffb_ctx* ctx, uint32_t* counts, const unsigned long long* counts_offsets,
                      unsigned long long counts_words, int advance_epoch);
+
+/* Serving: form-factor solves submitted as requests of different sizes
+ * (BASELINE config "served"), admitted in arrival order into `n_slots`
+ * concurrent slots while the device-memory budget allows (0 = no budget); a
+ * finished result keeps its reservation until released.  Each slot is a context with
+ * its own stream and worker thread so that admitted requests overlap on the
+ * device.  A request is a scene (host faces9, copied at submit),
+ * rays_per_face front-side rays per face, a Philox seed and emission flags;
+ * its per-face N x N uint32 counts stay resident on the device until
+ * ffb_server_release.  The result of a request does not depend on the other
+ * requests in flight. */
+#define FFB_REQ_QUEUED 0
+#define FFB_REQ_RUNNING 1
+#define FFB_REQ_DONE 2
+#define FFB_REQ_FAILED 3
+
+typedef struct ffb_server ffb_server;
+
+typedef struct {
+  int state;         /* FFB_REQ_* */
+  int error;         /* FFB_ERR_* of a failed request */
+  int n_faces;
+  double queue_s;    /* submit -> admission */
+  double latency_s;  /* submit -> result resident */
+  double gpu_ms;     /* device time of the request's work on its slot stream */
+} ffb_request_info;
+
+typedef struct {
+  int queued, running, peak_running;
+  unsigned long long reserved_bytes, budget_bytes;
+} ffb_server_info;
+
+int ffb_server_create(int device, unsigned long long budget_bytes, int n_slots, ffb_server** out);
+void ffb_server_destroy(ffb_server* server);
+int ffb_server_submit(ffb_server* server, const float* faces9, int n_faces, int rays_per_face, uint64_t seed,
+                      int flags, float cells_per_face, long long* request_id);
+/* Waits for a request (timeout_s < 0: no limit); FFB_ERR_TIMEOUT if it is
+ * still queued or running when the time is up. */
+int ffb_server_wait(ffb_server* server, long long request_id, double timeout_s, ffb_request_info* info);
+/* Copies a finished request's counts (host or device, N*N uint32). */
+int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts);
+/* Frees a finished request's resident matrix and its budget reservation. */
+int ffb_server_release(ffb_server* server, long long request_id);
+int ffb_server_stats(ffb_server* server, ffb_server_info* out);
 
 /* Counters and kernel time of the last ffb_cast / ffb_form_factor_counts
  * (synchronises the stream). */

@@ -1,0 +1,57 @@
+"""Serving loop (ffb_server_*): requests admitted by memory budget into
+concurrent slots; each result equals the same solve run alone."""
+import numpy as np
+import pytest
+
+from form_factors_b200 import native, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    return [(scenes.parallel_plates(6, 1.0), 800, 21), (scenes.icosphere(3, 1.0, inward=True), 300, 22),
+            (scenes.clutter(150, 0.08, seed=2, enclosure_cells=4), 500, 23), (scenes.unit_box(), 5000, 24),
+            (scenes.perpendicular_plates(8), 600, 25), (scenes.icosphere(2, 0.7, inward=True), 900, 26)]
+
+
+def test_results_in_the_mix_equal_results_alone(ctx):
+    reqs = _requests()
+    server = native.Server(0, budget_bytes=0, slots=3)
+    ids = [server.submit(f, rpf, seed) for f, rpf, seed in reqs]
+    infos = [server.wait(i, timeout_s=300) for i in ids]
+    assert all(inf.state == 2 for inf in infos)
+    for (f, rpf, seed), rid in zip(reqs, ids):
+        got = server.result(rid, len(f))
+        ctx.scene_set(f)
+        ctx.grid_build(cells_per_face=32)
+        want = ctx.form_factor_counts(np.full(len(f), rpf, np.int32), np.zeros(len(f), np.int32), seed=seed, epoch=0)
+        assert np.array_equal(got, want)
+        server.release(rid)
+    st = server.stats()
+    assert st.peak_running >= 2  # requests overlapped
+    assert st.reserved_bytes == 0 and st.queued == 0 and st.running == 0
+    server.close()
+
+
+def test_admission_by_memory_budget():
+    reqs = _requests()
+    n_max = max(len(f) for f, _, _ in reqs)
+    # room for the largest request alone (4 N^2 + 1536 N + 8 MiB), not for two
+    budget = 4 * n_max * n_max + 1536 * n_max + (8 << 20) + (1 << 20)
+    server = native.Server(0, budget_bytes=budget, slots=4)
+    ids = [server.submit(f, rpf, seed) for f, rpf, seed in reqs]
+    # a finished result keeps its reservation until released: a client that
+    # consumes results in order lets the next request in
+    for i in ids:
+        assert server.wait(i, timeout_s=120).state == 2
+        assert server.stats().reserved_bytes <= budget
+        server.release(i)
+    # the largest request fills the budget: at most two of the small ones fit together
+    assert 1 <= server.stats().peak_running <= 2
+    # a request larger than the whole budget is refused at submit
+    big = scenes.icosphere(5, 1.0)  # 20480 faces: 1.7 GB of counts
+    with pytest.raises(native.FFBError) as e:
+        server.submit(big, 10, 1)
+    assert e.value.code == -305
+    assert server.stats().reserved_bytes == 0
+    server.close()
