@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--grid", default="", help="grid dims nx,ny,nz (default: automatic)")
     ap.add_argument("--cells-per-face", type=float, default=32.0, help="automatic grid sizing target")
     ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
+    ap.add_argument("--served-requests", type=int, default=16)
+    ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     return ap.parse_args()
 
 
@@ -191,6 +195,114 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# batched scenes (one persistent launch, CUDA graph) vs the plain path
+# ---------------------------------------------------------------------------
+def batched_section(ctx, stream, args):
+    """256 scenes, triangle counts log-uniform 200-20k (plate pairs, inward UV
+    spheres, clutter in a box), 1k-10k front rays per face.  Batched: the grids
+    and the 256 count matrices resident, one fused launch replayed from a CUDA
+    graph.  Plain: the same scenes one at a time through the single-scene path
+    (upload, grid build, counts)."""
+    import torch
+    from form_factors_b200 import scenes
+    sl, rpf = scenes.batch_workload(256, 200, 20000, 1000, 10000, seed=4)
+    sizes = np.array([len(f) for f in sl])
+    fronts = [np.full(len(f), int(r), np.int32) for f, r in zip(sl, rpf)]
+    rears = [np.zeros(len(f), np.int32) for f in sl]
+    seeds = np.arange(1, len(sl) + 1, dtype=np.uint64) * np.uint64(7919)
+    rays = int(sum(int(f.sum()) for f in fronts))
+    t0 = time.perf_counter()
+    ctx.batch_set(sl, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
+    ctx.batch_prepare(np.concatenate(fronts), np.concatenate(rears), seeds)
+    build_s = time.perf_counter() - t0
+    offs, words = ctx.batch_counts_layout()
+    counts = torch.empty(words, dtype=torch.int32, device="cuda")
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        ctx.batch_launch(counts, offs, advance_epoch=True)
+    graph.replay()  # warm-up
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    graph.replay()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    batched_s = ev0.elapsed_time(ev1) / 1e3
+    del graph
+    # plain: one scene at a time, grid built per scene
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for i, f in enumerate(sl):
+        n = len(f)
+        ctx.scene_set(f)
+        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
+        ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2, out=counts[int(offs[i]):int(offs[i]) + n * n],
+                               n_rows=n)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    plain_s = ev0.elapsed_time(ev1) / 1e3
+    plain_wall = time.perf_counter() - t0
+    del counts
+    torch.cuda.empty_cache()
+    return {"workload": "256 scenes, faces log-uniform 200-20000 (plates/UV spheres/clutter), "
+                        "1k-10k front rays/face, per-scene N^2 uint32 counts resident",
+            "faces_total": int(sizes.sum()), "rays": rays, "counts_gb": round(4 * float((sizes.astype(float) ** 2).sum()) / 1e9, 2),
+            "batched_s": batched_s, "plain_s": plain_s, "plain_wall_s": plain_wall, "grid_build_s": build_s,
+            "batched_scenes_per_s": len(sl) / batched_s, "plain_scenes_per_s": len(sl) / plain_s,
+            "batched_rays_per_s": rays / batched_s, "plain_rays_per_s": rays / plain_s,
+            "speedup_scenes_per_s": plain_s / batched_s, "launches": "1 fused kernel per batch (CUDA graph replay)"}
+
+
+# ---------------------------------------------------------------------------
+# served requests (Poisson arrivals, admission by memory budget)
+# ---------------------------------------------------------------------------
+def served_section(args):
+    """Requests of scenes with faces log-uniform 500-50k (the three families),
+    1k-100k front rays per face, Poisson arrivals at args.served_rate/s,
+    admitted by an 80 GB device budget into 4 slots; each result stays
+    resident until released.  Plain: the same requests one at a time."""
+    from form_factors_b200 import native, scenes
+    rng = np.random.default_rng(9)
+    n = args.served_requests
+    fams = ("plates", "sphere", "clutter")
+    sizes = np.exp(rng.uniform(np.log(500), np.log(50000), n))
+    reqs = [(scenes.family_scene(fams[i % 3], sizes[i], rng), int(rng.integers(1000, 100001)), 100 + i)
+            for i in range(n)]
+    gaps = rng.exponential(1.0 / args.served_rate, n)
+    rays = sum(len(f) * r for f, r, _ in reqs)
+
+    def run(slots, arrivals):
+        server = native.Server(0, budget_bytes=int(80e9), slots=slots)
+        t0 = time.perf_counter()
+        ids = []
+        for (f, r, sd), at in zip(reqs, arrivals):
+            delay = t0 + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(server.submit(f, r, sd))
+        infos = []
+        for i in ids:
+            infos.append(server.wait(i, timeout_s=600))
+            server.release(i)
+        wall = time.perf_counter() - t0
+        peak = server.stats().peak_running
+        server.close()
+        lat = np.array([inf.latency_s for inf in infos])
+        return wall, lat, peak
+
+    served_wall, lat, peak = run(4, np.cumsum(gaps))
+    plain_wall, plain_lat, _ = run(1, np.zeros(n))
+    return {"workload": "%d requests, faces log-uniform 500-50000 (plates/UV spheres/clutter), 1k-100k front "
+                        "rays/face, Poisson %.0f req/s, 80 GB budget, 4 slots" % (n, args.served_rate),
+            "rays": int(rays), "served_scenes_per_s": n / served_wall, "plain_scenes_per_s": n / plain_wall,
+            "speedup_scenes_per_s": plain_wall / served_wall, "served_rays_per_s": rays / served_wall,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "plain_p50_latency_s": float(np.percentile(plain_lat, 50)),
+            "offered_rays_per_s": rays / max(float(np.sum(gaps)), 1e-9), "peak_concurrent": int(peak),
+            "note": "offered load far above capacity: latency is queueing under saturation"}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def fp32_peak(device):
@@ -312,6 +424,12 @@ def ours(args):
     h2d = 16 * n_chunks
     d2h = 4 * n * n
 
+    batched = served = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_section(ctx, stream, args)
+    if rank == 0 and world == 1 and not args.no_served:
+        served = served_section(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out = reference_sampler(faces, args.rays_per_face, args.cpu_sample_every)
@@ -347,6 +465,10 @@ def ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if batched is not None:
+            line["batched"] = batched
+        if served is not None:
+            line["served"] = served
         print(json.dumps(line))
     ctx.close()
     if world > 1:

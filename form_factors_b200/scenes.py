@@ -21,19 +21,20 @@ import numpy as np
 
 
 def plate_grid(width=1.0, height=1.0, cells_x=10, cells_y=10):
-    """Two triangles per cell, normals +z: (A, B, D) and (C, D, B)."""
+    """Two triangles per cell, normals +z: (A, B, D) and (C, D, B), cells in
+    the order of subject/objects.cpp:52-77 (i outer, j inner), float32 steps."""
     sx, sy = np.float32(width / cells_x), np.float32(height / cells_y)
-    out = np.zeros((cells_x * cells_y * 2, 9), np.float32)
-    for i in range(cells_x):
-        for j in range(cells_y):
-            x, y = np.float32(sx * i), np.float32(sy * j)
-            A = (x, y, 0)
-            B = (x + sx, y, 0)
-            C = (x + sx, y + sy, 0)
-            D = (x, y + sy, 0)
-            k = (i * cells_y + j) * 2
-            out[k] = A + B + D
-            out[k + 1] = C + D + B
+    i, j = np.meshgrid(np.arange(cells_x), np.arange(cells_y), indexing="ij")
+    x = (sx * i.astype(np.float32)).ravel()
+    y = (sy * j.astype(np.float32)).ravel()
+    z = np.zeros_like(x)
+    A = np.stack([x, y, z], 1)
+    B = np.stack([x + sx, y, z], 1)
+    C = np.stack([x + sx, y + sy, z], 1)
+    D = np.stack([x, y + sy, z], 1)
+    out = np.empty((cells_x * cells_y * 2, 9), np.float32)
+    out[0::2] = np.concatenate([A, B, D], 1)
+    out[1::2] = np.concatenate([C, D, B], 1)
     return out
 
 
@@ -173,6 +174,54 @@ def unit_box():
     for k, (a, b, c) in idx.items():
         out[k] = np.concatenate([v[a], v[b], v[c]])
     return out
+
+
+def uv_sphere(n_lat, n_lon, radius=1.0, inward=True, center=(0, 0, 0)):
+    """Latitude/longitude sphere of 2 * n_lon * (n_lat - 1) triangles (one
+    triangle per polar quad, two elsewhere), no degenerate faces."""
+    th = np.linspace(0, np.pi, n_lat + 1)
+    ph = np.linspace(0, 2 * np.pi, n_lon + 1)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    V = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1) * radius + np.asarray(center)
+    tris = []
+    j = np.arange(n_lon)
+    tris.append(np.stack([V[0, j], V[1, j + 1], V[1, j]], 1))               # north cap
+    for i in range(1, n_lat - 1):
+        tris.append(np.stack([V[i, j], V[i, j + 1], V[i + 1, j + 1]], 1))
+        tris.append(np.stack([V[i, j], V[i + 1, j + 1], V[i + 1, j]], 1))
+    tris.append(np.stack([V[n_lat - 1, j], V[n_lat - 1, j + 1], V[n_lat, j]], 1))  # south cap
+    out = np.concatenate(tris).reshape(-1, 9).astype(np.float32)
+    out = _orient_inward(out, center)
+    return out if inward else flip(out)
+
+
+def family_scene(family, n_target, rng):
+    """A scene of about n_target triangles of one family: 'plates' (two
+    parallel plate grids at distance 1), 'sphere' (inward UV sphere) or
+    'clutter' (random equilateral triangles in a unit-cube enclosure)."""
+    n_target = max(int(n_target), 24)
+    if family == "plates":
+        k = max(1, int(round(np.sqrt(n_target / 4.0))))
+        return parallel_plates(k, 1.0)
+    if family == "sphere":
+        n_lon = max(4, int(round(np.sqrt(n_target))))
+        n_lat = max(3, int(round(n_target / (2.0 * n_lon))) + 1)
+        return uv_sphere(n_lat, n_lon, 1.0, inward=True)
+    k = max(1, int(round(np.sqrt(n_target / 48.0))))  # enclosure: a quarter of the faces
+    n_c = max(1, n_target - 12 * k * k)
+    return clutter(n_c, 0.05, seed=int(rng.integers(1 << 31)), enclosure_cells=k)
+
+
+def batch_workload(n_scenes=256, n_min=200, n_max=20000, rays_min=1000, rays_max=10000, seed=4):
+    """Batched workload: triangle counts log-uniform in [n_min, n_max], the
+    three families in turn, rays per face uniform in [rays_min, rays_max].
+    Returns (list of faces arrays, rays per face per scene)."""
+    rng = np.random.default_rng(seed)
+    fams = ("plates", "sphere", "clutter")
+    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_scenes))
+    rays = rng.integers(rays_min, rays_max + 1, n_scenes)
+    out = [family_scene(fams[i % 3], sizes[i], rng) for i in range(n_scenes)]
+    return out, rays.astype(np.int64)
 
 
 def areas(faces):
