@@ -734,9 +734,9 @@ extern "C" int ffb_emit(ffb_ctx* c, const int32_t* front, const int32_t* rear, u
   return FFB_OK;
 }
 
-extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
-                                      uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
-                                      uint32_t* counts)
+extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                           uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
+                                           int row_begin, int row_end, uint32_t* counts)
 {
   FFB_TRY(check_ctx(c));
   SceneData& s = c->main;
@@ -752,22 +752,33 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
     return fail(FFB_ERR_ARG, "identity rows need n_rows == n_faces (%d != %d)", n_rows, s.n_faces);
   if (n_rows <= 0)
     return fail(FFB_ERR_ARG, "n_rows must be positive");
+  if (n_rows > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
+  if (row_begin < 0 || row_end > n_rows || row_begin >= row_end)
+    return fail(FFB_ERR_ARG, "row range [%d, %d) outside [0, %d)", row_begin, row_end, n_rows);
   if (face_to_row) {
     for (int f = 0; f < s.n_faces; ++f)
       if (face_to_row[f] < 0 || face_to_row[f] >= n_rows)
         return fail(FFB_ERR_ARG, "face_to_row[%d] = %d outside [0, %d)", f, face_to_row[f], n_rows);
   }
-  if (n_rows > kMaxRows)
-    return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
   FFB_TRY(ensure_frames(c, flags));
+  // only the faces of rows [row_begin, row_end) emit
+  std::vector<int32_t> fr(front, front + s.n_faces), re(rear, rear + s.n_faces);
+  if (row_begin > 0 || row_end < n_rows) {
+    for (int f = 0; f < s.n_faces; ++f) {
+      const int row = face_to_row ? face_to_row[f] : f;
+      if (row < row_begin || row >= row_end)
+        fr[f] = re[f] = 0;
+    }
+  }
   std::vector<Chunk> chunks;
   chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
-  add_chunks(chunks, front, rear, s.n_faces, 0);
-  const size_t mat = (size_t)n_rows * n_rows;
+  add_chunks(chunks, fr.data(), re.data(), s.n_faces, 0);
+  const size_t words = (size_t)(row_end - row_begin) * n_rows;
   void* d_counts;
   bool host_out;
-  FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * mat, c->tmp_out, &d_counts, &host_out));
-  FFB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * mat, c->stream));
+  FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * words, c->tmp_out, &d_counts, &host_out));
+  FFB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * words, c->stream));
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
   if (!chunks.empty()) {
@@ -788,7 +799,10 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
     p.chunk_cursor = dptr<uint32_t>(c->cursor);
     p.stats = dptr<unsigned long long>(c->stats);
     p.scenes[0].g = make_view(s);
-    p.scenes[0].counts = (uint32_t*)d_counts;
+    // the kernel adds at row * n_rows + col; the block holds rows from
+    // row_begin, so its base is moved back by row_begin rows (only rows of
+    // the block are ever written)
+    p.scenes[0].counts = (uint32_t*)((uintptr_t)d_counts - sizeof(uint32_t) * (size_t)row_begin * n_rows);
     p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
     p.scenes[0].face_base = 0;
     p.scenes[0].n_cols = n_rows;
@@ -798,10 +812,17 @@ extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const in
       FFB_TRY((launch_fused<false, 1>(c, p, true)));
   }
   if (host_out) {
-    FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * mat));
+    FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
     FFB_CUDA(cudaStreamSynchronize(c->stream));
   }
   return FFB_OK;
+}
+
+extern "C" int ffb_form_factor_counts(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                      uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
+                                      uint32_t* counts)
+{
+  return ffb_form_factor_counts_rows(c, front, rear, seed, epoch, flags, face_to_row, n_rows, 0, n_rows, counts);
 }
 
 extern "C" int ffb_normalise(ffb_ctx* c, const uint32_t* counts, const int32_t* outgoing, int n_rows, float* ff)
@@ -976,6 +997,57 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
   else
     FFB_TRY((launch_fused<false, kMaxBatchScenes>(c, p, false)));
   return FFB_OK;
+}
+
+// ===========================================================================
+// Autotuning of the grid
+// ===========================================================================
+extern "C" int ffb_autotune_grid(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                 const ffb_grid_params* candidates, int n_candidates, int sample_every,
+                                 ffb_grid_params* best, float* best_ms)
+{
+  FFB_TRY(check_ctx(c));
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!candidates || n_candidates <= 0 || !best)
+    return fail(FFB_ERR_ARG, "no candidates");
+  long long total = 0;
+  FFB_TRY(check_counts(s.n_faces, front, rear, &total));
+  if (sample_every < 1)
+    sample_every = 1;
+  // sample: every k-th face emits (same rays as in the full solve)
+  std::vector<int32_t> fr((size_t)s.n_faces, 0), re((size_t)s.n_faces, 0);
+  for (int f = 0; f < s.n_faces; f += sample_every) {
+    fr[f] = front[f];
+    re[f] = rear[f];
+  }
+  const size_t mat = (size_t)s.n_faces * s.n_faces;
+  if (s.n_faces > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "scene too large");
+  FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * mat));
+  float best_t = INFINITY;
+  int best_i = -1;
+  for (int i = 0; i < n_candidates; ++i) {
+    FFB_TRY(grid_build(c, s, candidates + i));
+    float t = INFINITY;
+    for (int rep = 0; rep < 2; ++rep) {  // first run warms the grid into L2
+      FFB_TRY(ffb_form_factor_counts(c, fr.data(), re.data(), seed, 0, 0, nullptr, s.n_faces,
+                                     dptr<uint32_t>(c->ff_counts)));
+      FFB_CUDA(cudaStreamSynchronize(c->stream));
+      float ms = 0;
+      FFB_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      t = std::min(t, ms);
+    }
+    if (t < best_t) {
+      best_t = t;
+      best_i = i;
+    }
+  }
+  *best = candidates[best_i];
+  if (best_ms)
+    *best_ms = best_t;
+  return grid_build(c, s, best);
 }
 
 extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)

@@ -94,6 +94,8 @@ def load(path=LIB_PATH):
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
         "ffb_cast_bruteforce_static": (i32, [vp, i32, vp, i64, vp, vp, vp]),
         "ffb_form_factors": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp, vp]),
+        "ffb_form_factor_counts_rows": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, i32, i32, vp]),
+        "ffb_autotune_grid": (i32, [vp, vp, vp, u64, vp, i32, i32, C.POINTER(GridParams), C.POINTER(C.c_float)]),
         "ffb_batch_set": (i32, [vp, i32, vp, vp, vp]),
         "ffb_batch_grid_info": (i32, [vp, i32, C.POINTER(GridInfo)]),
         "ffb_batch_prepare": (i32, [vp, vp, vp, vp, i32]),
@@ -202,6 +204,27 @@ class Context:
             p.nx, p.ny, p.nz = [int(d) for d in dims]
         _check(self._lib.ffb_grid_build(self._h, C.byref(p)))
 
+    def autotune_grid(self, front, rear, seed=1, candidates=None, sample_every=8):
+        """Times grid candidates on a sample of the ray budget and keeps the
+        fastest built.  candidates: list of dicts with dims / cells_per_face /
+        skip_empty; default: cubic 32..128 and 8..64 cells per face."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        if candidates is None:
+            candidates = [dict(dims=(d, d, d)) for d in (32, 48, 64, 96, 128)] + \
+                         [dict(cells_per_face=c) for c in (8, 16, 32, 64)]
+        arr = (GridParams * len(candidates))()
+        for i, cand in enumerate(candidates):
+            arr[i] = GridParams(0, 0, 0, float(cand.get("cells_per_face", 32.0)), int(cand.get("skip_empty", True)))
+            if cand.get("dims"):
+                arr[i].nx, arr[i].ny, arr[i].nz = cand["dims"]
+        best = GridParams()
+        ms = C.c_float()
+        _check(self._lib.ffb_autotune_grid(self._h, _ptr(front), _ptr(rear), int(seed), C.cast(arr, C.c_void_p),
+                                           len(candidates), int(sample_every), C.byref(best), C.byref(ms)))
+        return dict(dims=(best.nx, best.ny, best.nz), cells_per_face=best.cells_per_face,
+                    skip_empty=bool(best.skip_empty), sample_ms=ms.value)
+
     def grid_info(self):
         info = GridInfo()
         _check(self._lib.ffb_grid_info_get(self._h, C.byref(info)))
@@ -240,6 +263,22 @@ class Context:
             out = np.empty((n_rows, n_rows), np.uint32)
         _check(self._lib.ffb_form_factor_counts(self._h, _ptr(front), _ptr(rear), int(seed), int(epoch), int(flags),
                                                 _ptr(face_to_row), int(n_rows), _ptr(out)))
+        return out
+
+    def form_factor_counts_rows(self, front, rear, seed, row_begin, row_end, epoch=0, flags=0, face_to_row=None,
+                                n_rows=None, out=None):
+        """Rows [row_begin, row_end) of the count matrix (one shard)."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        if face_to_row is not None:
+            face_to_row = np.ascontiguousarray(face_to_row, np.int32)
+        if n_rows is None:
+            n_rows = self.n_faces if face_to_row is None else int(face_to_row.max()) + 1
+        if out is None:
+            out = np.empty((row_end - row_begin, n_rows), np.uint32)
+        _check(self._lib.ffb_form_factor_counts_rows(self._h, _ptr(front), _ptr(rear), int(seed), int(epoch),
+                                                     int(flags), _ptr(face_to_row), int(n_rows), int(row_begin),
+                                                     int(row_end), _ptr(out)))
         return out
 
     def normalise(self, counts, outgoing, out=None):

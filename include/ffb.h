@@ -120,6 +120,15 @@ int ffb_emit(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t s
 int ffb_form_factor_counts(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
                            int flags, const int32_t* face_to_row, int n_rows, uint32_t* counts);
 
+/* The rows [row_begin, row_end) of the same matrix: only the faces of those
+ * rows emit, and counts ((row_end - row_begin) x n_rows, host or device)
+ * receives row r at (r - row_begin) * n_rows.  Row blocks are independent,
+ * which is how the matrix is sharded across GPUs (no collective while
+ * tracing; the blocks are gathered afterwards if a rank needs them all). */
+int ffb_form_factor_counts_rows(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows, int row_begin,
+                                int row_end, uint32_t* counts);
+
 /* ff[m * n_rows + j] = (float)counts[m * n_rows + j] * (1.f / (float)outgoing[m]),
  * the row normalisation of cpuFactorsCalculator/cpu_system.cpp:193-195.
  * counts and ff: host or device; outgoing: host int32[n_rows]. */
@@ -199,6 +208,15 @@ int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts
 /* Frees a finished request's resident matrix and its budget reservation. */
 int ffb_server_release(ffb_server* server, long long request_id);
 int ffb_server_stats(ffb_server* server, ffb_server_info* out);
+
+/* Grid autotuner: builds the grid with each candidate (resolution,
+ * cells_per_face, empty-space jumps), times the fused kernel on a sample of
+ * the given ray budget (every sample_every-th face emits its rays), keeps the
+ * fastest built and returns it in *best (and its sample time in *best_ms).
+ * The scene must be set; nothing about the results depends on the choice. */
+int ffb_autotune_grid(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed,
+                      const ffb_grid_params* candidates, int n_candidates, int sample_every, ffb_grid_params* best,
+                      float* best_ms);
 
 /* Counters and kernel time of the last ffb_cast / ffb_form_factor_counts
  * (synchronises the stream). */

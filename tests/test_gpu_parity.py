@@ -104,8 +104,9 @@ def test_form_factor_counts_mesh_rows(ctx, oracle):
     assert np.array_equal(got.astype(np.uint64), want)
 
 
-def test_hash_histogram_path(ctx, oracle):
-    """More than 8192 faces selects the shared-memory hash histogram."""
+def test_wide_matrix_sparse_sources(ctx, oracle):
+    """A 10 240-face matrix with few emitting faces: the warp histograms see
+    keys spread over a 105 M-entry matrix."""
     faces = scenes.icosphere(4, 1.0, inward=True)  # 5120 faces
     faces = np.concatenate([faces, scenes.transform(faces, shift=(3, 0, 0))])  # 10240 faces
     n = len(faces)
@@ -119,3 +120,20 @@ def test_hash_histogram_path(ctx, oracle):
     got = ctx.form_factor_counts(front, rear, seed=99)
     want = oracle.form_factor_counts(faces, front, rear, seed=99)
     assert np.array_equal(got, want)
+
+
+def test_row_blocks_concatenate_to_full_matrix(ctx):
+    """Shards of source rows (one per GPU in a multi-GPU run) are independent:
+    their blocks concatenate to the full matrix, bit for bit."""
+    from form_factors_b200 import shard
+    faces = scenes.clutter(200, 0.08, seed=6, enclosure_cells=4)
+    n = len(faces)
+    w, total = emission.two_sided_weights(faces)
+    front, rear = emission.ray_counts(400 * n, w, total)
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=16)
+    full = ctx.form_factor_counts(front, rear, seed=12, epoch=3)
+    for world in (2, 3):
+        blocks = [ctx.form_factor_counts_rows(front, rear, 12, b, e, epoch=3)
+                  for b, e in shard.row_ranges(shard.rays_per_row(front, rear), world)]
+        assert np.array_equal(np.concatenate(blocks), full)
