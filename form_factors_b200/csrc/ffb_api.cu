@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -462,10 +463,18 @@ int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long lo
 }
 
 // Occupancy-sized persistent launch of the fused kernel for `n_chunks` chunks.
+#ifndef FFB_COOP_DEFAULT
+#define FFB_COOP_DEFAULT 1
+#endif
+
 template <bool kSkip, int kScenes>
 int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, bool timed)
 {
-  auto kern = k_form_factors<kSkip, kScenes>;
+  static const int coop = [] {
+    const char* e = getenv("FFB_COOP");
+    return e ? atoi(e) : FFB_COOP_DEFAULT;
+  }();
+  auto kern = coop ? k_form_factors_coop<kSkip, kScenes> : k_form_factors<kSkip, kScenes>;
   int per_sm = 0;
   FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
   // persistent blocks: a full wave, fewer when there are fewer chunks than warps

@@ -430,6 +430,16 @@ __device__ __forceinline__ float next_t(int s, int c, float lo, float cs, float 
   return s == 0 ? INFINITY : boundary_t(lo, c + (s > 0), cs, o, inv);
 }
 
+// boundary_t with the edge index already in float: the DDA keeps an exact
+// float copy of each cell index (integers below 2^24 are exact), which gives
+// the same boundary as the int version without an int-to-float conversion on
+// the conversion unit per step.
+__device__ __forceinline__ float boundary_tf(float lo, float edge, float cs, float o, float inv)
+{
+  float t = (lo + edge * cs - o) * inv;
+  return t == t ? t : INFINITY;
+}
+
 // Landing cell on one axis after a jump to parameter tj: never against the
 // ray, never beyond the empty cube of half-width `jump`.
 __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, float tj, float lo, float ics)
@@ -461,6 +471,7 @@ struct Tracer {
   float3 o, dir, inv;
   float t1, dlen, best;
   float tnx, tny, tnz;
+  float ex, ey, ez;  // float index of the next boundary on each axis (cell + (step > 0))
   float3 best_pt;
   int cx, cy, cz;
   int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
@@ -502,6 +513,9 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.tnx = next_t(sgn(T.dir.x), T.cx, g.lo.x, g.cs.x, o.x, T.inv.x);
   T.tny = next_t(sgn(T.dir.y), T.cy, g.lo.y, g.cs.y, o.y, T.inv.y);
   T.tnz = next_t(sgn(T.dir.z), T.cz, g.lo.z, g.cs.z, o.z, T.inv.z);
+  T.ex = (float)(T.cx + (T.dir.x > 0.f));
+  T.ey = (float)(T.cy + (T.dir.y > 0.f));
+  T.ez = (float)(T.cz + (T.dir.z > 0.f));
   T.dlen = sqrtf(dot3(T.dir, T.dir));
   T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
   T.best_ref = -1;
@@ -597,27 +611,34 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
       T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
       T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
       T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
+      T.ex = (float)(nx + (sx > 0));
+      T.ey = (float)(ny + (sy > 0));
+      T.ez = (float)(nz + (sz > 0));
       ++n_cells;
       tracer_enter<kSkip>(T, g);
       return true;
     }
   }
   // one DDA step along the axis whose boundary comes first
+  // (the chosen axis has a finite boundary, hence a nonzero step)
   if (T.tnx <= T.tny && T.tnx <= T.tnz) {
     T.cx += sx;
     if ((unsigned)T.cx >= (unsigned)g.nx)
       return false;
-    T.tnx = next_t(sx, T.cx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
+    T.ex += T.dir.x > 0.f ? 1.f : -1.f;
+    T.tnx = boundary_tf(g.lo.x, T.ex, g.cs.x, T.o.x, T.inv.x);
   } else if (T.tny <= T.tnz) {
     T.cy += sy;
     if ((unsigned)T.cy >= (unsigned)g.ny)
       return false;
-    T.tny = next_t(sy, T.cy, g.lo.y, g.cs.y, T.o.y, T.inv.y);
+    T.ey += T.dir.y > 0.f ? 1.f : -1.f;
+    T.tny = boundary_tf(g.lo.y, T.ey, g.cs.y, T.o.y, T.inv.y);
   } else {
     T.cz += sz;
     if ((unsigned)T.cz >= (unsigned)g.nz)
       return false;
-    T.tnz = next_t(sz, T.cz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
+    T.ez += T.dir.z > 0.f ? 1.f : -1.f;
+    T.tnz = boundary_tf(g.lo.z, T.ez, g.cs.z, T.o.z, T.inv.z);
   }
   ++n_cells;
   tracer_enter<kSkip>(T, g);
