@@ -86,6 +86,7 @@ struct ffb_ctx {
   cudaStream_t stream = nullptr;
   unsigned long long budget = 0;  // 0 = unlimited
   unsigned long long bytes = 0;   // device bytes held in DevBufs
+  bool stats_on = true;           // fused kernel with counters
 
   SceneData main;                 // the scene of the single-scene calls
   DevBuf frames;                  // emission frames of the main scene
@@ -464,26 +465,42 @@ int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long lo
 
 // Occupancy-sized persistent launch of the fused kernel for `n_chunks` chunks.
 #ifndef FFB_COOP_DEFAULT
-#define FFB_COOP_DEFAULT 1
+#define FFB_COOP_DEFAULT 0
+#endif
+
+// Matrices of at least this many entries take one global reduction per hit
+// instead of the warp histogram (keys rarely repeat within a warp there).
+#ifndef FFB_DIRECT_MIN_WORDS
+#define FFB_DIRECT_MIN_WORDS (1ull << 22)
 #endif
 
 template <bool kSkip, int kScenes>
-int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, bool timed)
+int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, int n_scenes, bool timed)
 {
   static const int coop = [] {
     const char* e = getenv("FFB_COOP");
     return e ? atoi(e) : FFB_COOP_DEFAULT;
   }();
-  auto kern = coop ? k_form_factors_coop<kSkip, kScenes> : k_form_factors<kSkip, kScenes>;
+  bool hash = false;
+  for (int s = 0; s < n_scenes; ++s)
+    hash |= (unsigned long long)p.scenes[s].n_cols * (unsigned long long)p.scenes[s].n_cols < FFB_DIRECT_MIN_WORDS;
+  void (*kern)(TraceParams<kScenes>);
+  if (coop)
+    kern = k_form_factors_coop<kSkip, kScenes>;
+  else if (p.stats)
+    kern = hash ? k_form_factors<kSkip, kScenes, true, true> : k_form_factors<kSkip, kScenes, true, false>;
+  else
+    kern = hash ? k_form_factors<kSkip, kScenes, false, true> : k_form_factors<kSkip, kScenes, false, false>;
+  const size_t smem = (!coop && hash) ? kHashSmem : 0;
   int per_sm = 0;
-  FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
+  FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, smem));
   // persistent blocks: a full wave, fewer when there are fewer chunks than warps
   const long long wave = (long long)std::max(per_sm, 1) * c->n_sm;
   const long long by_work = ((long long)p.n_chunks + kWarpsPerBlock - 1) / kWarpsPerBlock;
   const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
   if (timed)
     timing_begin(c);
-  kern<<<blocks, kTraceThreads, 0, c->stream>>>(p);
+  kern<<<blocks, kTraceThreads, smem, c->stream>>>(p);
   if (timed)
     timing_end(c);
   FFB_CUDA(cudaGetLastError());
@@ -574,6 +591,14 @@ extern "C" int ffb_ctx_set_budget(ffb_ctx* c, unsigned long long bytes)
 }
 
 extern "C" unsigned long long ffb_ctx_bytes(ffb_ctx* c) { return c ? c->bytes : 0; }
+
+extern "C" int ffb_ctx_set_stats(ffb_ctx* c, int on)
+{
+  if (!c)
+    return fail(FFB_ERR_ARG, "null context");
+  c->stats_on = on != 0;
+  return FFB_OK;
+}
 
 extern "C" const char* ffb_last_error(void) { return g_last_error.c_str(); }
 
@@ -806,7 +831,7 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     p.epoch_ptr = nullptr;
     p.scene_keys = nullptr;
     p.chunk_cursor = dptr<uint32_t>(c->cursor);
-    p.stats = dptr<unsigned long long>(c->stats);
+    p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
     p.scenes[0].g = make_view(s);
     // the kernel adds at row * n_rows + col; the block holds rows from
     // row_begin, so its base is moved back by row_begin rows (only rows of
@@ -816,9 +841,9 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     p.scenes[0].face_base = 0;
     p.scenes[0].n_cols = n_rows;
     if (p.scenes[0].g.empty_dist)
-      FFB_TRY((launch_fused<true, 1>(c, p, true)));
+      FFB_TRY((launch_fused<true, 1>(c, p, 1, true)));
     else
-      FFB_TRY((launch_fused<false, 1>(c, p, true)));
+      FFB_TRY((launch_fused<false, 1>(c, p, 1, true)));
   }
   if (host_out) {
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
@@ -985,7 +1010,7 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
   p.epoch_ptr = dptr<uint32_t>(c->batch_epoch);
   p.scene_keys = dptr<uint2>(c->batch_keys);
   p.chunk_cursor = dptr<uint32_t>(c->cursor);
-  p.stats = dptr<unsigned long long>(c->stats);
+  p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
   // all scenes share one kernel variant: empty-space jumps need every
   // scene's distance map
   bool skip = true;
@@ -1002,9 +1027,9 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     skip = skip && slot.g.empty_dist != nullptr;
   }
   if (skip)
-    FFB_TRY((launch_fused<true, kMaxBatchScenes>(c, p, false)));
+    FFB_TRY((launch_fused<true, kMaxBatchScenes>(c, p, n_scenes, false)));
   else
-    FFB_TRY((launch_fused<false, kMaxBatchScenes>(c, p, false)));
+    FFB_TRY((launch_fused<false, kMaxBatchScenes>(c, p, n_scenes, false)));
   return FFB_OK;
 }
 

@@ -430,16 +430,6 @@ __device__ __forceinline__ float next_t(int s, int c, float lo, float cs, float 
   return s == 0 ? INFINITY : boundary_t(lo, c + (s > 0), cs, o, inv);
 }
 
-// boundary_t with the edge index already in float: the DDA keeps an exact
-// float copy of each cell index (integers below 2^24 are exact), which gives
-// the same boundary as the int version without an int-to-float conversion on
-// the conversion unit per step.
-__device__ __forceinline__ float boundary_tf(float lo, float edge, float cs, float o, float inv)
-{
-  float t = (lo + edge * cs - o) * inv;
-  return t == t ? t : INFINITY;
-}
-
 // Landing cell on one axis after a jump to parameter tj: never against the
 // ray, never beyond the empty cube of half-width `jump`.
 __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, float tj, float lo, float ics)
@@ -466,12 +456,17 @@ __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, fl
 #ifndef FFB_MAILBOX
 #define FFB_MAILBOX 0
 #endif
+#ifndef FFB_SELECT_STEP
+#define FFB_SELECT_STEP 1
+#endif
+#ifndef FFB_PREFETCH
+#define FFB_PREFETCH 0
+#endif
 
 struct Tracer {
   float3 o, dir, inv;
   float t1, dlen, best;
   float tnx, tny, tnz;
-  float ex, ey, ez;  // float index of the next boundary on each axis (cell + (step > 0))
   float3 best_pt;
   int cx, cy, cz;
   int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
@@ -513,9 +508,6 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.tnx = next_t(sgn(T.dir.x), T.cx, g.lo.x, g.cs.x, o.x, T.inv.x);
   T.tny = next_t(sgn(T.dir.y), T.cy, g.lo.y, g.cs.y, o.y, T.inv.y);
   T.tnz = next_t(sgn(T.dir.z), T.cz, g.lo.z, g.cs.z, o.z, T.inv.z);
-  T.ex = (float)(T.cx + (T.dir.x > 0.f));
-  T.ey = (float)(T.cy + (T.dir.y > 0.f));
-  T.ez = (float)(T.cz + (T.dir.z > 0.f));
   T.dlen = sqrtf(dot3(T.dir, T.dir));
   T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
   T.best_ref = -1;
@@ -552,6 +544,10 @@ __device__ __forceinline__ void tracer_test(Tracer& T, const GridView& g, uint32
 #endif
   ++n_tests;
   const float4* rec = reinterpret_cast<const float4*>(g.ref_rec + i);
+#if FFB_PREFETCH
+  if (T.i < T.en)  // the next record of the cell, while this one is tested
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.ref_rec + T.i));
+#endif
   float3 pt;
   if (tri_hit_regs(__ldg(rec), __ldg(rec + 1), __ldg(rec + 2), __ldg(rec + 3), T.o, T.dir, pt)) {
     const float d = dist2(pt, T.o);
@@ -611,35 +607,47 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
       T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
       T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
       T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
-      T.ex = (float)(nx + (sx > 0));
-      T.ey = (float)(ny + (sy > 0));
-      T.ez = (float)(nz + (sz > 0));
       ++n_cells;
       tracer_enter<kSkip>(T, g);
       return true;
     }
   }
   // one DDA step along the axis whose boundary comes first
-  // (the chosen axis has a finite boundary, hence a nonzero step)
+#if FFB_SELECT_STEP
+  // the axis is chosen with selects, so that lanes stepping along different
+  // axes run the same instructions
+  const bool ax = T.tnx <= T.tny && T.tnx <= T.tnz;
+  const bool ay = !ax && T.tny <= T.tnz;
+  const int s = ax ? sx : (ay ? sy : sz);
+  const int c = (ax ? T.cx : (ay ? T.cy : T.cz)) + s;
+  if ((unsigned)c >= (unsigned)(ax ? g.nx : (ay ? g.ny : g.nz)))
+    return false;
+  const float tn = next_t(s, c, ax ? g.lo.x : (ay ? g.lo.y : g.lo.z), ax ? g.cs.x : (ay ? g.cs.y : g.cs.z),
+                          ax ? T.o.x : (ay ? T.o.y : T.o.z), ax ? T.inv.x : (ay ? T.inv.y : T.inv.z));
+  T.cx = ax ? c : T.cx;
+  T.cy = ay ? c : T.cy;
+  T.cz = (ax || ay) ? T.cz : c;
+  T.tnx = ax ? tn : T.tnx;
+  T.tny = ay ? tn : T.tny;
+  T.tnz = (ax || ay) ? T.tnz : tn;
+#else
   if (T.tnx <= T.tny && T.tnx <= T.tnz) {
     T.cx += sx;
     if ((unsigned)T.cx >= (unsigned)g.nx)
       return false;
-    T.ex += T.dir.x > 0.f ? 1.f : -1.f;
-    T.tnx = boundary_tf(g.lo.x, T.ex, g.cs.x, T.o.x, T.inv.x);
+    T.tnx = next_t(sx, T.cx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
   } else if (T.tny <= T.tnz) {
     T.cy += sy;
     if ((unsigned)T.cy >= (unsigned)g.ny)
       return false;
-    T.ey += T.dir.y > 0.f ? 1.f : -1.f;
-    T.tny = boundary_tf(g.lo.y, T.ey, g.cs.y, T.o.y, T.inv.y);
+    T.tny = next_t(sy, T.cy, g.lo.y, g.cs.y, T.o.y, T.inv.y);
   } else {
     T.cz += sz;
     if ((unsigned)T.cz >= (unsigned)g.nz)
       return false;
-    T.ez += T.dir.z > 0.f ? 1.f : -1.f;
-    T.tnz = boundary_tf(g.lo.z, T.ez, g.cs.z, T.o.z, T.inv.z);
+    T.tnz = next_t(sz, T.cz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
   }
+#endif
   ++n_cells;
   tracer_enter<kSkip>(T, g);
   return true;

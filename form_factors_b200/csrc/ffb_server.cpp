@@ -109,6 +109,8 @@ void worker_main(ffb_server* s, int slot)
   cudaSetDevice(s->device);
   ffb_ctx* ctx = nullptr;
   int rc = ffb_ctx_create(s->device, &ctx);
+  if (ctx)
+    ffb_ctx_set_stats(ctx, 0);  // requests return counts only
   cudaStream_t stream = ctx ? (cudaStream_t)ffb_ctx_stream(ctx) : nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);

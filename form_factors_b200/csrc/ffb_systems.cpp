@@ -378,7 +378,12 @@ static int init(ff_t* s, emission::system_t* emitter)
   s->seed = 1;
   s->epoch = 0;
   s->flags = 0;
-  return s->fused ? ffb_ctx_create(device_from_env(), &s->ctx) : FORM_FACTORS_OK;
+  if (!s->fused)
+    return FORM_FACTORS_OK;
+  const int rc = ffb_ctx_create(device_from_env(), &s->ctx);
+  if (rc == FFB_OK)
+    ffb_ctx_set_stats(s->ctx, 0);  // the calculator reports no counters
+  return rc;
 }
 
 static int shutdown(ff_t* s)

@@ -57,6 +57,7 @@ constexpr int kWarpsPerBlock = kTraceThreads / 32;
 constexpr int kWarpHashLog2 = 9;
 constexpr int kWarpHash = 1 << kWarpHashLog2;  // histogram slots per warp
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr size_t kHashSmem = sizeof(uint32_t) * 2 * kWarpHash * kWarpsPerBlock;  // dynamic shared bytes with kHash
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 __device__ __forceinline__ void warp_stats(unsigned long long* stats, uint32_t tests, uint32_t cells, uint32_t rays,
@@ -119,30 +120,49 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // Fused form-factor kernel.  Persistent warps, no block barriers.  Each warp
 // keeps a current chunk (consecutive rays of one face) and hands its rays to
 // lanes as they fall idle (one ballot per refill, one global atomic per
-// chunk), so a warp may hold rays of several faces at once.  Each lane runs
-// the grid traversal state machine one unit of work per iteration.  A finished
-// hit adds one to the warp's shared-memory hash histogram keyed by the matrix
-// index row(f) * n_cols + row(h); the warp flushes the table to the global
-// uint32 matrix with atomic adds when it is half full, when it changes scene
-// and at the end.
+// chunk), so a warp may hold rays of several faces at once.  Idle lanes are
+// refilled together once at least kRefillMin of them wait (or the whole warp
+// is idle): emission and ray setup then run with several lanes at once
+// instead of one lane at a time.  Each iteration a lane whose cell is
+// exhausted moves on (stop, DDA step or empty-space jump) and, if its cell
+// has references left, tests one of them.  A finished hit adds one to the
+// warp's shared-memory hash histogram keyed by the matrix index
+// row(f) * n_cols + row(h); the warp flushes the table to the global uint32
+// matrix with atomic adds when it is half full, when it changes scene and at
+// the end.
 //
 // With several scenes in one launch a warp works on one scene at a time: a
 // chunk of another scene is taken only once every lane is idle (drain before
 // switch), so that the scene's grid is warp-uniform.
+//
+// kStats adds the test / cell / ray / hit counters (four live registers per
+// lane); without it p.stats is ignored.  kHash selects the warp histogram;
+// without it each hit is one global reduction (red.global.add) into the
+// matrix, which suits large, sparse matrices (distinct keys per warp, so the
+// histogram merges little) and leaves the shared memory to the L1 cache.
 // ---------------------------------------------------------------------------
-template <bool kSkip, int kScenes>
+#ifndef FFB_REFILL_MIN
+#define FFB_REFILL_MIN 4
+#endif
+constexpr int kRefillMin = FFB_REFILL_MIN;
+#ifndef FFB_IFIF
+#define FFB_IFIF 0
+#endif
+
+template <bool kSkip, int kScenes, bool kStats, bool kHash>
 __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams<kScenes> p)
 {
-  __shared__ uint32_t s_keys[kWarpsPerBlock][kWarpHash];
-  __shared__ uint32_t s_vals[kWarpsPerBlock][kWarpHash];
+  extern __shared__ uint32_t s_hash[];  // kWarpsPerBlock x (keys, values) when kHash
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* keys = s_keys[warp];
-  uint32_t* vals = s_vals[warp];
-  for (int i = lane; i < kWarpHash; i += 32) {
-    keys[i] = kEmptyKey;
-    vals[i] = 0;
+  uint32_t* keys = s_hash + warp * 2 * kWarpHash;
+  uint32_t* vals = keys + kWarpHash;
+  if (kHash) {
+    for (int i = lane; i < kWarpHash; i += 32) {
+      keys[i] = kEmptyKey;
+      vals[i] = 0;
+    }
+    __syncwarp();
   }
-  __syncwarp();
   const uint32_t epoch = p.epoch_ptr ? *p.epoch_ptr : p.epoch;
   const unsigned lane_below = (1u << lane) - 1u;
   int fill = 0;  // occupied slots (warp-uniform)
@@ -164,6 +184,8 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
   uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0;
   for (;;) {
     unsigned need = __ballot_sync(kFull, !active);
+    if (__popc(need) < kRefillMin && need != kFull)
+      need = 0;
     while (need && !exhausted) {
       if (c_left == 0) {
         int k = pending;
@@ -182,7 +204,8 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
             pending = k;
             break;
           }
-          warp_hash_flush(keys, vals, p.scenes[scene].counts, lane);
+          if (kHash)
+            warp_hash_flush(keys, vals, p.scenes[scene].counts, lane);
           fill = 0;
           scene = ch.scene;
           if (p.scene_keys) {
@@ -220,27 +243,44 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
     int hit = -1;
     if (active) {
+#if FFB_IFIF
+      if (T.i >= T.en && !tracer_advance<kSkip>(T, S.g, n_cells)) {
+        active = false;
+        hit = tracer_result(T, S.g);
+      } else if (T.i < T.en) {
+        tracer_test(T, S.g, n_tests);
+      }
+#else
       if (T.i < T.en) {
         tracer_test(T, S.g, n_tests);
       } else if (!tracer_advance<kSkip>(T, S.g, n_cells)) {
         active = false;
         hit = tracer_result(T, S.g);
       }
+#endif
     }
     bool fresh = false;
     if (hit >= 0) {
       ++n_hits;
       const int col = S.face_to_row ? __ldg(S.face_to_row + hit) : hit;
-      fresh = warp_hash_add(keys, vals, (uint32_t)my_row * (uint32_t)S.n_cols + (uint32_t)col, S.counts);
+      const uint32_t key = (uint32_t)my_row * (uint32_t)S.n_cols + (uint32_t)col;
+      if (kHash)
+        fresh = warp_hash_add(keys, vals, key, S.counts);
+      else
+        atomicAdd(S.counts + key, 1u);
     }
-    fill += __popc(__ballot_sync(kFull, fresh));
-    if (fill > kWarpHash / 2) {
-      warp_hash_flush(keys, vals, S.counts, lane);
-      fill = 0;
+    if (kHash) {
+      fill += __popc(__ballot_sync(kFull, fresh));
+      if (fill > kWarpHash / 2) {
+        warp_hash_flush(keys, vals, S.counts, lane);
+        fill = 0;
+      }
     }
   }
-  warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
-  warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
+  if (kHash)
+    warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
+  if (kStats)
+    warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
 }
 
 // ---------------------------------------------------------------------------

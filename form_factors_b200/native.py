@@ -81,6 +81,7 @@ def load(path=LIB_PATH):
         "ffb_ctx_set_stream": (i32, [vp, vp]),
         "ffb_ctx_stream": (vp, [vp]),
         "ffb_ctx_set_budget": (i32, [vp, C.c_ulonglong]),
+        "ffb_ctx_set_stats": (i32, [vp, i32]),
         "ffb_ctx_bytes": (C.c_ulonglong, [vp]),
         "ffb_last_error": (C.c_char_p, []),
         "ffb_scene_set": (i32, [vp, vp, i32]),
@@ -186,6 +187,10 @@ class Context:
 
     def set_budget(self, nbytes):
         _check(self._lib.ffb_ctx_set_budget(self._h, int(nbytes)))
+
+    def set_stats(self, on):
+        """Counters in the fused kernel on or off (on by default)."""
+        _check(self._lib.ffb_ctx_set_stats(self._h, 1 if on else 0))
 
     def device_bytes(self):
         return int(self._lib.ffb_ctx_bytes(self._h))

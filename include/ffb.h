@@ -80,6 +80,11 @@ void* ffb_ctx_stream(ffb_ctx* ctx);
 /* Device-memory budget of the context in bytes (0 = unlimited). */
 int ffb_ctx_set_budget(ffb_ctx* ctx, unsigned long long bytes);
 unsigned long long ffb_ctx_bytes(ffb_ctx* ctx);
+/* Test / cell / ray / hit counters of the fused kernel (on by default).  Off,
+ * the kernel variant without counters runs and ffb_stats_get reports zero
+ * counts (kernel_ms stays).  No reference counterpart: the reference keeps no
+ * such counters. */
+int ffb_ctx_set_stats(ffb_ctx* ctx, int on);
 const char* ffb_last_error(void);
 
 /* Scene upload and per-face precompute (host or device faces9).
