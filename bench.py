@@ -403,7 +403,7 @@ def ours(args):
     step(10_003)
     s = ctx.stats()
     ctx.set_stats(False)
-    tests, cells, hits = s.tests, s.cells, s.hits
+    tests, cells, hits, jumps = s.tests, s.cells, s.hits, s.jumps
     tests_per_launch = tests
     achieved = tests_per_launch * FLOPS_PER_TEST / (k_ms * 1e-3)
     peak = fp32_peak(local)
@@ -463,6 +463,7 @@ def ours(args):
                              FLOPS_PER_TEST, tests_per_launch),
                          "peak_source": "measured live: FMUL+FADD issue probe (libffb200_probe.so)"},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
+            "jumps_per_ray": jumps / rays_per_step,
             "hit_fraction": hits / rays_per_step,
             "clocks": clk,
         }

@@ -66,7 +66,7 @@ struct SceneData {
   DevBuf faces, tri, box_lo, box_hi, scene_ord;
   bool grid_ok = false;
   ffb_grid_info info{};
-  DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist;
+  DevBuf cell_start, cell_fill, ref_tri, ref_rec, empty_dist, cell_rec;
 };
 
 }  // namespace
@@ -148,7 +148,7 @@ void release(ffb_ctx* c, DevBuf& b)
 void release_scene(ffb_ctx* c, SceneData& s)
 {
   DevBuf* bufs[] = {&s.faces,      &s.tri,     &s.box_lo,  &s.box_hi,  &s.scene_ord,
-                    &s.cell_start, &s.cell_fill, &s.ref_tri, &s.ref_rec, &s.empty_dist};
+                    &s.cell_start, &s.cell_fill, &s.ref_tri, &s.ref_rec, &s.empty_dist, &s.cell_rec};
   for (DevBuf* b : bufs)
     release(c, *b);
   s.n_faces = -1;
@@ -219,10 +219,14 @@ GridView make_view(SceneData& s)
   g.ny = I.ny;
   g.nz = I.nz;
   g.slack = 2.f * I.margin;
-  g.cell_start = dptr<uint32_t>(s.cell_start);
   g.ref_tri = dptr<int32_t>(s.ref_tri);
   g.ref_rec = dptr<TriRec>(s.ref_rec);
+#if FFB_CELL_REC
+  g.cell_rec = dptr<uint2>(s.cell_rec);
+#else
+  g.cell_start = dptr<uint32_t>(s.cell_start);
   g.empty_dist = I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr;
+#endif
   return g;
 }
 
@@ -401,6 +405,8 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
   FFB_CUDA(cudaMemcpyAsync(&total, dptr<uint32_t>(s.cell_start) + n_cells, sizeof total, cudaMemcpyDeviceToHost,
                            c->stream));
   FFB_CUDA(cudaStreamSynchronize(c->stream));
+  if (total >= kCellEmpty)  // reference offsets must stay below the empty-cell flag
+    return fail(FFB_ERR_TOO_LARGE, "%u grid references; at most %u", total, kCellEmpty - 1);
   FFB_TRY(ensure(c, s.ref_tri, sizeof(int32_t) * (size_t)std::max<uint32_t>(total, 1)));
   FFB_CUDA(cudaMemsetAsync(s.cell_fill.ptr, 0, sizeof(uint32_t) * (size_t)n_cells, c->stream));
   k_grid_fill<<<nb, 128, 0, c->stream>>>(bg, dptr<float>(s.faces), dptr<float4>(s.box_lo), dptr<float4>(s.box_hi),
@@ -421,6 +427,11 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
     k_empty_pass<<<grid_blocks((long long)I.nx * I.ny, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 2);
     FFB_CUDA(cudaGetLastError());
   }
+  FFB_TRY(ensure(c, s.cell_rec, sizeof(uint2) * (size_t)n_cells));
+  k_cell_rec<<<grid_blocks(n_cells, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+      dptr<uint32_t>(s.cell_start), I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr, (int)n_cells,
+      dptr<uint2>(s.cell_rec));
+  FFB_CUDA(cudaGetLastError());
   // live faces: those with a non-empty binning box
   I.n_refs = total;
   I.n_live_faces = 0;
@@ -463,35 +474,25 @@ int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long lo
   return FFB_OK;
 }
 
-// Occupancy-sized persistent launch of the fused kernel for `n_chunks` chunks.
-#ifndef FFB_COOP_DEFAULT
-#define FFB_COOP_DEFAULT 0
-#endif
-
 // Matrices of at least this many entries take one global reduction per hit
 // instead of the warp histogram (keys rarely repeat within a warp there).
 #ifndef FFB_DIRECT_MIN_WORDS
 #define FFB_DIRECT_MIN_WORDS (1ull << 22)
 #endif
 
+// Occupancy-sized persistent launch of the fused kernel for p.n_chunks chunks.
 template <bool kSkip, int kScenes>
 int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, int n_scenes, bool timed)
 {
-  static const int coop = [] {
-    const char* e = getenv("FFB_COOP");
-    return e ? atoi(e) : FFB_COOP_DEFAULT;
-  }();
   bool hash = false;
   for (int s = 0; s < n_scenes; ++s)
     hash |= (unsigned long long)p.scenes[s].n_cols * (unsigned long long)p.scenes[s].n_cols < FFB_DIRECT_MIN_WORDS;
   void (*kern)(TraceParams<kScenes>);
-  if (coop)
-    kern = k_form_factors_coop<kSkip, kScenes>;
-  else if (p.stats)
+  if (p.stats)
     kern = hash ? k_form_factors<kSkip, kScenes, true, true> : k_form_factors<kSkip, kScenes, true, false>;
   else
     kern = hash ? k_form_factors<kSkip, kScenes, false, true> : k_form_factors<kSkip, kScenes, false, false>;
-  const size_t smem = (!coop && hash) ? kHashSmem : 0;
+  const size_t smem = hash ? kHashSmem : 0;
   int per_sm = 0;
   FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, smem));
   // persistent blocks: a full wave, fewer when there are fewer chunks than warps
@@ -699,7 +700,7 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
     GridView g = make_view(s);
     FFB_TRY(ensure(c, c->ray_cursor, sizeof(unsigned long long)));
     FFB_CUDA(cudaMemsetAsync(c->ray_cursor.ptr, 0, sizeof(unsigned long long), c->stream));
-    auto kern = g.empty_dist ? k_cast<true> : k_cast<false>;
+    auto kern = s.info.skip_empty ? k_cast<true> : k_cast<false>;
     int per_sm = 0;
     FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
     const int blocks = grid_blocks(n_rays, kTraceThreads, std::max(1, per_sm) * c->n_sm);
@@ -840,7 +841,7 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
     p.scenes[0].face_base = 0;
     p.scenes[0].n_cols = n_rows;
-    if (p.scenes[0].g.empty_dist)
+    if (s.info.skip_empty)
       FFB_TRY((launch_fused<true, 1>(c, p, 1, true)));
     else
       FFB_TRY((launch_fused<false, 1>(c, p, 1, true)));
@@ -1024,7 +1025,7 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     slot.face_to_row = nullptr;
     slot.face_base = (int)c->batch_offsets[s];
     slot.n_cols = c->batch[s].n_faces;
-    skip = skip && slot.g.empty_dist != nullptr;
+    skip = skip && c->batch[s].info.skip_empty;
   }
   if (skip)
     FFB_TRY((launch_fused<true, kMaxBatchScenes>(c, p, n_scenes, false)));
@@ -1098,6 +1099,7 @@ extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)
     out->cells = s[kStatCells];
     out->rays = s[kStatRays];
     out->hits = s[kStatHits];
+    out->jumps = s[kStatJumps];
   }
   if (c->timed)
     cudaEventElapsedTime(&out->kernel_ms, c->ev0, c->ev1);

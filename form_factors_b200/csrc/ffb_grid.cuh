@@ -21,17 +21,31 @@
 
 namespace ffb {
 
+#ifndef FFB_CELL_REC
+#define FFB_CELL_REC 1
+#endif
+
 struct GridView {
   float3 lo, hi;        // grid box
   float3 cs;            // cell size
   float3 inv_cs;        // 1 / cell size
   int nx, ny, nz;
   float slack;          // 2 * margin, world units
-  const uint32_t* __restrict__ cell_start;  // ncells + 1
   const int32_t* __restrict__ ref_tri;      // triangle index per reference
   const TriRec* __restrict__ ref_rec;       // triangle record per reference (a copy of tri[ref_tri[i]])
+#if FFB_CELL_REC
+  const uint2* __restrict__ cell_rec;       // per cell: {start, end} of its references, or {0, kCellEmpty | jump}
+#else
+  const uint32_t* __restrict__ cell_start;  // ncells + 1
   const uint8_t* __restrict__ empty_dist;   // Chebyshev distance to the nearest occupied cell, or null
+#endif
 };
+
+// Packed cell record: an occupied cell holds {first reference, end}; an
+// empty one {0, kCellEmpty | d} with d its empty-space distance (1 when the
+// grid has no distance map).  One 8-byte load replaces the distance byte and
+// the two offsets.
+constexpr uint32_t kCellEmpty = 0x80000000u;
 
 // Ordered-integer image of a float for atomicMin/atomicMax reductions.
 __device__ __forceinline__ uint32_t f2ord(float f)
@@ -391,6 +405,15 @@ __global__ void k_empty_pass(uint8_t* __restrict__ d, int nx, int ny, int nz, in
   }
 }
 
+__global__ void k_cell_rec(const uint32_t* __restrict__ cell_start, const uint8_t* __restrict__ empty_dist, int n_cells,
+                           uint2* __restrict__ rec)
+{
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+    const uint32_t b = cell_start[c], e = cell_start[c + 1];
+    rec[c] = e > b ? make_uint2(b, e) : make_uint2(0u, kCellEmpty | (empty_dist ? (uint32_t)empty_dist[c] : 1u));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Nearest hit through the grid.  Returns the face index or -1 and writes the
 // hit point of the reference's test for a hit.
@@ -462,6 +485,9 @@ __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, fl
 #ifndef FFB_PREFETCH
 #define FFB_PREFETCH 0
 #endif
+#ifndef FFB_UNIFIED_ADVANCE
+#define FFB_UNIFIED_ADVANCE 1
+#endif
 
 struct Tracer {
   float3 o, dir, inv;
@@ -482,6 +508,13 @@ template <bool kSkip>
 __device__ __forceinline__ void tracer_enter(Tracer& T, const GridView& g)
 {
   const int cell = (T.cz * g.ny + T.cy) * g.nx + T.cx;
+#if FFB_CELL_REC
+  const uint2 r = __ldg(g.cell_rec + cell);
+  const bool empty = (r.y & kCellEmpty) != 0;
+  T.jump = kSkip && empty ? (int)(r.y & 0xFFu) : 0;
+  T.i = r.x;
+  T.en = empty ? 0u : r.y;
+#else
   T.jump = kSkip ? (int)__ldg(g.empty_dist + cell) : 0;
   if (T.jump == 0) {
     T.i = __ldg(g.cell_start + cell);
@@ -489,6 +522,7 @@ __device__ __forceinline__ void tracer_enter(Tracer& T, const GridView& g)
   } else {
     T.i = T.en = 0;
   }
+#endif
 }
 
 // Sets up a ray; false when it misses the grid box (no hit possible).
@@ -575,7 +609,7 @@ __device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
 // The current cell is exhausted: stop, or move to the next cell.  Returns
 // false when the ray is finished.
 template <bool kSkip>
-__device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells)
+__device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells, uint32_t& n_jumps)
 {
   const float tx = fminf(fminf(T.tnx, T.tny), T.tnz);
   if (T.best_ref >= 0) {
@@ -586,6 +620,48 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
   if (!(tx < T.t1) || --T.iters <= 0)
     return false;
   const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
+#if FFB_UNIFIED_ADVANCE
+  if (kSkip) {
+    // Every move leaves the empty cube of half-width jump-1 around the cell
+    // (the cell itself when jump <= 1, where the exit parameter is the DDA's
+    // next boundary) and lands in the cell where the ray crosses the cube's
+    // boundary.  A diagonal landing skips only cells that the ray touches
+    // within rounding of the landing cell, whose triangles the binning margin
+    // puts into the landing cell as well.  Lanes that step and lanes that
+    // jump run the same instructions.
+    const int jump = max(T.jump, 1);
+    const float bx = boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x);
+    const float by = boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y);
+    const float bz = boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z);
+    const float tj = fminf(fminf(sx ? bx : INFINITY, sy ? by : INFINITY), sz ? bz : INFINITY);
+    if (!(tj < T.t1))
+      return false;
+    int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
+    int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
+    int nz = land(sz, T.cz, jump, T.o.z, T.dir.z, tj, g.lo.z, g.inv_cs.z);
+    if (nx == T.cx && ny == T.cy && nz == T.cz) {
+      // the landing point rounded back into the cell: one DDA step along the
+      // axis whose boundary comes first
+      const bool ax = T.tnx <= T.tny && T.tnx <= T.tnz;
+      const bool ay = !ax && T.tny <= T.tnz;
+      nx += ax ? sx : 0;
+      ny += ay ? sy : 0;
+      nz += (ax || ay) ? 0 : sz;
+    }
+    if ((unsigned)nx >= (unsigned)g.nx || (unsigned)ny >= (unsigned)g.ny || (unsigned)nz >= (unsigned)g.nz)
+      return false;
+    n_jumps += jump >= 2;
+    T.cx = nx;
+    T.cy = ny;
+    T.cz = nz;
+    T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
+    T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
+    T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
+    ++n_cells;
+    tracer_enter<kSkip>(T, g);
+    return true;
+  }
+#endif
   if (kSkip && T.jump >= 2) {
     // every cell within Chebyshev distance jump-1 is empty: leave that cube
     const int jump = T.jump;
@@ -608,6 +684,7 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
       T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
       T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
       ++n_cells;
+      ++n_jumps;
       tracer_enter<kSkip>(T, g);
       return true;
     }

@@ -19,7 +19,7 @@ struct Chunk {
 };
 
 // Statistics slots (uint64 each), accumulated once per warp.
-enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatSlots = 4 };
+enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatJumps = 4, kStatSlots = 5 };
 
 // One scene of a fused launch: its grid, its count matrix and where its faces
 // start in the launch's frame table.
@@ -61,13 +61,13 @@ constexpr size_t kHashSmem = sizeof(uint32_t) * 2 * kWarpHash * kWarpsPerBlock; 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 __device__ __forceinline__ void warp_stats(unsigned long long* stats, uint32_t tests, uint32_t cells, uint32_t rays,
-                                           uint32_t hits)
+                                           uint32_t hits, uint32_t jumps)
 {
   if (!stats)
     return;
-  unsigned long long v[4] = {tests, cells, rays, hits};
+  unsigned long long v[kStatSlots] = {tests, cells, rays, hits, jumps};
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < kStatSlots; ++k) {
     unsigned long long x = v[k];
     for (int o = 16; o > 0; o >>= 1)
       x += __shfl_xor_sync(kFull, x, o);
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
   Tracer T;
   bool active = false;
   int my_row = 0;
-  uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0;
+  uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0, n_jumps = 0;
   for (;;) {
     unsigned need = __ballot_sync(kFull, !active);
     if (__popc(need) < kRefillMin && need != kFull)
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     int hit = -1;
     if (active) {
 #if FFB_IFIF
-      if (T.i >= T.en && !tracer_advance<kSkip>(T, S.g, n_cells)) {
+      if (T.i >= T.en && !tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
         active = false;
         hit = tracer_result(T, S.g);
       } else if (T.i < T.en) {
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
 #else
       if (T.i < T.en) {
         tracer_test(T, S.g, n_tests);
-      } else if (!tracer_advance<kSkip>(T, S.g, n_cells)) {
+      } else if (!tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
         active = false;
         hit = tracer_result(T, S.g);
       }
@@ -280,210 +280,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
   if (kHash)
     warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
   if (kStats)
-    warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
-}
-
-// ---------------------------------------------------------------------------
-// Cooperative variant of the fused kernel.  Per round, every lane whose
-// current cell is exhausted advances its own ray (DDA, empty-space jumps,
-// stopping rule) until it reaches a cell with triangle references, finishes,
-// or is refilled with a new ray; then the warp pools the pending (ray,
-// reference) pairs of all its lanes in shared memory and tests them with all
-// 32 lanes at once.  A hit is merged into its ray's best with a 64-bit
-// atomicMin on (squared-distance bits, face index): squared distances are
-// non-negative, so the bit order is the numeric order, and the minimum of
-// the pairs is the lexicographic minimum the reference's strict '<' scan in
-// index order selects.  The stopping rule reads the merged best after every
-// cell, as in the per-lane kernel, so the set of tested triangles and the
-// result are the same.
-// ---------------------------------------------------------------------------
-constexpr int kCoopQueue = 128;  // pooled tests per warp and round
-
-struct CoopWarp {
-  float ray[32][6];          // origin, direction of each lane's ray
-  unsigned long long best[32];
-  uint32_t ref[kCoopQueue];
-  uint8_t owner[kCoopQueue];
-};
-
-__device__ __forceinline__ unsigned long long best_key(float d, int face)
-{
-  return ((unsigned long long)__float_as_uint(d) << 32) | (uint32_t)face;
-}
-
-template <bool kSkip, int kScenes>
-__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
-    k_form_factors_coop(const __grid_constant__ TraceParams<kScenes> p)
-{
-  __shared__ uint32_t s_keys[kWarpsPerBlock][kWarpHash];
-  __shared__ uint32_t s_vals[kWarpsPerBlock][kWarpHash];
-  __shared__ CoopWarp s_coop[kWarpsPerBlock];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* keys = s_keys[warp];
-  uint32_t* vals = s_vals[warp];
-  CoopWarp& W = s_coop[warp];
-  for (int i = lane; i < kWarpHash; i += 32) {
-    keys[i] = kEmptyKey;
-    vals[i] = 0;
-  }
-  __syncwarp();
-  const uint32_t epoch = p.epoch_ptr ? *p.epoch_ptr : p.epoch;
-  const unsigned lane_below = (1u << lane) - 1u;
-  const unsigned long long no_hit = best_key(3.40282347e+38f, 0x7FFFFFFF);
-  int fill = 0;
-  int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0;
-  int scene = 0;
-  uint32_t key0 = p.key0, key1 = p.key1;
-  if (p.scene_keys) {
-    const uint2 k = p.scene_keys[0];
-    key0 = k.x;
-    key1 = k.y;
-  }
-  int pending = -1;
-  bool exhausted = false;
-  Tracer T;
-  bool active = false;
-  int my_row = 0;
-  unsigned long long my_best = no_hit;
-  uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0;
-  for (;;) {
-    const SceneSlot* S = &p.scenes[kScenes > 1 ? scene : 0];
-    // 1. lanes with an exhausted cell move on; a finished ray is counted
-    int hit = -1;
-    if (active && T.i >= T.en) {
-      for (;;) {
-        if (!tracer_advance<kSkip>(T, S->g, n_cells)) {
-          active = false;
-          hit = T.best_ref;
-          break;
-        }
-        if (T.i < T.en)
-          break;
-      }
-    }
-    bool fresh = false;
-    if (hit >= 0) {
-      ++n_hits;
-      const int col = S->face_to_row ? __ldg(S->face_to_row + hit) : hit;
-      fresh = warp_hash_add(keys, vals, (uint32_t)my_row * (uint32_t)S->n_cols + (uint32_t)col, S->counts);
-    }
-    fill += __popc(__ballot_sync(kFull, fresh));
-    if (fill > kWarpHash / 2) {
-      warp_hash_flush(keys, vals, S->counts, lane);
-      fill = 0;
-    }
-    // 2. idle lanes take new rays (a chunk of another scene waits for the warp to drain)
-    unsigned need = __ballot_sync(kFull, !active);
-    while (need && !exhausted) {
-      if (c_left == 0) {
-        int k = pending;
-        if (k < 0) {
-          if (lane == 0)
-            k = (int)atomicAdd(p.chunk_cursor, 1u);
-          k = __shfl_sync(kFull, k, 0);
-          if (k >= p.n_chunks) {
-            exhausted = true;
-            break;
-          }
-        }
-        const Chunk ch = p.chunks[k];
-        if (kScenes > 1 && ch.scene != scene) {
-          if (__any_sync(kFull, active)) {
-            pending = k;
-            break;
-          }
-          warp_hash_flush(keys, vals, p.scenes[scene].counts, lane);
-          fill = 0;
-          scene = ch.scene;
-          S = &p.scenes[scene];
-          if (p.scene_keys) {
-            const uint2 sk = p.scene_keys[scene];
-            key0 = sk.x;
-            key1 = sk.y;
-          }
-        }
-        pending = -1;
-        c_face = ch.face;
-        c_j = ch.j0;
-        c_left = ch.count;
-        c_front = ch.front;
-        c_row = S->face_to_row ? __ldg(S->face_to_row + ch.face) : ch.face;
-      }
-      const int take = min(__popc(need), c_left);
-      const int rank = __popc(need & lane_below);
-      const bool mine = ((need >> lane) & 1u) && rank < take;
-      if (mine) {
-        float3 o, e;
-        emit_ray(p.frames + 20 * ((size_t)S->face_base + c_face), (uint32_t)c_face, (uint32_t)(c_j + rank), c_front,
-                 key0, key1, epoch, o, e);
-        ++n_rays;
-        my_row = c_row;
-        active = tracer_begin<kSkip>(T, S->g, o, e, n_cells);
-        my_best = no_hit;
-      }
-      need &= ~__ballot_sync(kFull, mine);
-      c_j += take;
-      c_left -= take;
-    }
-    if (exhausted && !__any_sync(kFull, active))
-      break;
-    // 3. pooled tests of the pending references of every lane's cell
-    const int k_mine = active ? (int)min(T.en - T.i, (uint32_t)kCoopQueue) : 0;
-    int incl = k_mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o)
-        incl += y;
-    }
-    const int total = __shfl_sync(kFull, incl, 31);
-    if (total == 0)
-      continue;
-    const int base = incl - k_mine;
-    const int take = max(0, min(k_mine, kCoopQueue - base));  // this round's share of my references
-    if (active) {
-      W.ray[lane][0] = T.o.x;
-      W.ray[lane][1] = T.o.y;
-      W.ray[lane][2] = T.o.z;
-      W.ray[lane][3] = T.dir.x;
-      W.ray[lane][4] = T.dir.y;
-      W.ray[lane][5] = T.dir.z;
-      W.best[lane] = my_best;
-      for (int q = 0; q < take; ++q) {
-        W.ref[base + q] = T.i + q;
-        W.owner[base + q] = (uint8_t)lane;
-      }
-    }
-    __syncwarp();
-    const int n_items = min(total, kCoopQueue);
-    const GridView& g = S->g;
-    for (int t = lane; t < n_items; t += 32) {
-      const uint32_t ref = W.ref[t];
-      const int own = W.owner[t];
-      const float3 o = f3(W.ray[own][0], W.ray[own][1], W.ray[own][2]);
-      const float3 dir = f3(W.ray[own][3], W.ray[own][4], W.ray[own][5]);
-      const float4* rec = reinterpret_cast<const float4*>(g.ref_rec + ref);
-      float3 pt;
-      ++n_tests;
-      if (tri_hit_regs(__ldg(rec), __ldg(rec + 1), __ldg(rec + 2), __ldg(rec + 3), o, dir, pt)) {
-        const float d = dist2(pt, o);
-        if (d < 3.40282347e+38f)
-          atomicMin(&W.best[own], best_key(d, __ldg(g.ref_tri + ref)));
-      }
-    }
-    __syncwarp();
-    if (active) {
-      T.i += take;
-      my_best = W.best[lane];
-      if (my_best != no_hit) {
-        T.best = __uint_as_float((uint32_t)(my_best >> 32));
-        T.best_ref = (int)(uint32_t)my_best;  // the face of the best hit
-      }
-    }
-    __syncwarp();
-  }
-  warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
-  warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits);
+    warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits, n_jumps);
 }
 
 // Advances the device-resident Philox epoch of a captured launch, so that every
@@ -508,7 +305,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
 {
   const int lane = threadIdx.x & 31;
   const unsigned lane_below = (1u << lane) - 1u;
-  uint32_t n_tests = 0, n_cells = 0, n_done = 0, n_hits = 0;
+  uint32_t n_tests = 0, n_cells = 0, n_done = 0, n_hits = 0, n_jumps = 0;
   Tracer T;
   bool active = false;
   long id = -1;
@@ -552,13 +349,13 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
     if (active) {
       if (T.i < T.en) {
         tracer_test(T, g, n_tests);
-      } else if (!tracer_advance<kSkip>(T, g, n_cells)) {
+      } else if (!tracer_advance<kSkip>(T, g, n_cells, n_jumps)) {
         active = false;
         finish(id, tracer_result(T, g), T.best_pt);
       }
     }
   }
-  warp_stats(stats, n_tests, n_cells, n_done, n_hits);
+  warp_stats(stats, n_tests, n_cells, n_done, n_hits, n_jumps);
 }
 
 // Brute force: every ray against every face (the naive_cpu definition),

@@ -43,7 +43,7 @@ class GridInfo(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("tests", C.c_ulonglong), ("cells", C.c_ulonglong), ("rays", C.c_ulonglong),
-                ("hits", C.c_ulonglong), ("kernel_ms", C.c_float)]
+                ("hits", C.c_ulonglong), ("kernel_ms", C.c_float), ("jumps", C.c_ulonglong)]
 
 
 class RequestInfo(C.Structure):

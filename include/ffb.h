@@ -68,6 +68,7 @@ typedef struct {
   unsigned long long rays;  /* rays traced */
   unsigned long long hits;  /* rays that hit a face */
   float kernel_ms;          /* device time of the trace kernel (CUDA events) */
+  unsigned long long jumps; /* empty-space jumps among the cells visited */
 } ffb_stats;
 
 /* Context: one device, one stream, resident scene and grid.
