@@ -146,7 +146,16 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 #endif
 constexpr int kRefillMin = FFB_REFILL_MIN;
 #ifndef FFB_IFIF
-#define FFB_IFIF 0
+#define FFB_IFIF 1
+#endif
+#ifndef FFB_PHASE
+#define FFB_PHASE 0
+#endif
+#ifndef FFB_PHASE_TEST_COST
+#define FFB_PHASE_TEST_COST 100
+#endif
+#ifndef FFB_PHASE_ADV_COST
+#define FFB_PHASE_ADV_COST 160
 #endif
 
 template <bool kSkip, int kScenes, bool kStats, bool kHash>
@@ -242,6 +251,26 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
       break;
     const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
     int hit = -1;
+#if FFB_PHASE
+    // One body per iteration for the whole warp: the triangle test or the
+    // cell advance, whichever moves more lanes per instruction; lanes in the
+    // other state wait one iteration.
+    {
+      const bool want_test = active && T.i < T.en;
+      const int n_test = __popc(__ballot_sync(kFull, want_test));
+      const int n_adv = __popc(__ballot_sync(kFull, active && !want_test));
+      const bool test_phase = n_test * FFB_PHASE_ADV_COST >= n_adv * FFB_PHASE_TEST_COST;
+      if (active) {
+        if (test_phase) {
+          if (want_test)
+            tracer_test(T, S.g, n_tests);
+        } else if (!want_test && !tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
+          active = false;
+          hit = tracer_result(T, S.g);
+        }
+      }
+    }
+#else
     if (active) {
 #if FFB_IFIF
       if (T.i >= T.en && !tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
@@ -259,6 +288,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
       }
 #endif
     }
+#endif
     bool fresh = false;
     if (hit >= 0) {
       ++n_hits;
