@@ -221,12 +221,7 @@ GridView make_view(SceneData& s)
   g.slack = 2.f * I.margin;
   g.ref_tri = dptr<int32_t>(s.ref_tri);
   g.ref_rec = dptr<TriRec>(s.ref_rec);
-#if FFB_CELL_REC
   g.cell_rec = dptr<uint2>(s.cell_rec);
-#else
-  g.cell_start = dptr<uint32_t>(s.cell_start);
-  g.empty_dist = I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr;
-#endif
   return g;
 }
 
@@ -320,7 +315,7 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
   if (params)
     P = *params;
   if (P.cells_per_face <= 0.f)
-    P.cells_per_face = 2.f;
+    P.cells_per_face = 32.f;
   if (P.nx < 0 || P.ny < 0 || P.nz < 0 || P.nx > kMaxDim || P.ny > kMaxDim || P.nz > kMaxDim)
     return fail(FFB_ERR_TOO_LARGE, "grid dims %dx%dx%d outside [0, %d]", P.nx, P.ny, P.nz, kMaxDim);
 

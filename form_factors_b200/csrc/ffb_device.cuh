@@ -70,10 +70,6 @@ __device__ inline TriRec make_trirec(float3 p0, float3 p1, float3 p2)
 // Anything not decided this way goes through the IEEE division.  NaN inputs
 // fail every comparison and always take the division path.
 // ---------------------------------------------------------------------------
-#ifndef FFB_FLAT_TEST
-#define FFB_FLAT_TEST 1
-#endif
-
 __device__ __forceinline__ bool surely_negative(float num, float den)
 {
   return ((num < 0.f) != (den < 0.f)) && num != 0.f && fabsf(num) > fabsf(den) * 0x1p-100f;
@@ -95,7 +91,6 @@ __device__ __forceinline__ bool surely_above_one(float num, float den)
 __device__ __forceinline__ bool tri_hit_regs(const float4 q0, const float4 q1, const float4 q2, const float4 q3,
                                              float3 o, float3 dir, float3& pt)
 {
-#if FFB_FLAT_TEST
   // Every rejection that needs no division beyond r decided by one branch:
   // lanes of a warp that leave at different stages then run the same
   // instructions.  r, p, s and t numerators are computed as below; when
@@ -123,37 +118,6 @@ __device__ __forceinline__ bool tri_hit_regs(const float4 q0, const float4 q1, c
     return false;
   pt = p;
   return true;
-#else
-  float3 w0 = f3(o.x - q0.x, o.y - q0.y, o.z - q0.z);
-  float a = -(q1.x * w0.x + q1.y * w0.y + q1.z * w0.z);
-  float b = q1.x * dir.x + q1.y * dir.y + q1.z * dir.z;
-  if (fabsf(b) < FFB_EPS_ABOVE_1E8)
-    return false;
-  if (surely_negative(a, b))  // r = a / b < 0
-    return false;
-  float r = a / b;
-  if (r < 0.f)
-    return false;
-  float3 p = f3(o.x + r * dir.x, o.y + r * dir.y, o.z + r * dir.z);
-  float3 w = f3(p.x - q0.x, p.y - q0.y, p.z - q0.z);
-  float wu = w.x * q2.x + w.y * q2.y + w.z * q2.z;
-  float wv = w.x * q3.x + w.y * q3.y + w.z * q3.z;
-  const float uu = q0.w, uv = q1.w, vv = q2.w, D = q3.w;
-  const float ns = uv * wv - vv * wu;
-  if (surely_negative(ns, D) || surely_above_one(ns, D))  // s < 0 || s > 1
-    return false;
-  const float nt = uv * wu - uu * wv;
-  if (surely_negative(nt, D))  // t < 0: rejected whatever s decides
-    return false;
-  float s = ns / D;
-  if (s < 0.f || s > 1.f)
-    return false;
-  float t = nt / D;
-  if (t < 0.f || (s + t) > 1.f)
-    return false;
-  pt = p;
-  return true;
-#endif
 }
 
 // Same test on a record in memory (global or shared).

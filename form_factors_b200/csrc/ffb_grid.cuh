@@ -21,10 +21,6 @@
 
 namespace ffb {
 
-#ifndef FFB_CELL_REC
-#define FFB_CELL_REC 1
-#endif
-
 struct GridView {
   float3 lo, hi;        // grid box
   float3 cs;            // cell size
@@ -33,12 +29,7 @@ struct GridView {
   float slack;          // 2 * margin, world units
   const int32_t* __restrict__ ref_tri;      // triangle index per reference
   const TriRec* __restrict__ ref_rec;       // triangle record per reference (a copy of tri[ref_tri[i]])
-#if FFB_CELL_REC
   const uint2* __restrict__ cell_rec;       // per cell: {start, end} of its references, or {0, kCellEmpty | jump}
-#else
-  const uint32_t* __restrict__ cell_start;  // ncells + 1
-  const uint8_t* __restrict__ empty_dist;   // Chebyshev distance to the nearest occupied cell, or null
-#endif
 };
 
 // Packed cell record: an occupied cell holds {first reference, end}; an
@@ -476,19 +467,6 @@ __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, fl
 // the binning margin; any triangle not yet tested lies in unvisited cells and
 // cannot compute a smaller distance.
 // ---------------------------------------------------------------------------
-#ifndef FFB_MAILBOX
-#define FFB_MAILBOX 0
-#endif
-#ifndef FFB_SELECT_STEP
-#define FFB_SELECT_STEP 1
-#endif
-#ifndef FFB_PREFETCH
-#define FFB_PREFETCH 0
-#endif
-#ifndef FFB_UNIFIED_ADVANCE
-#define FFB_UNIFIED_ADVANCE 1
-#endif
-
 struct Tracer {
   float3 o, dir, inv;
   float t1, dlen, best;
@@ -499,30 +477,17 @@ struct Tracer {
   int jump;          // empty-space distance of the current cell
   uint32_t i, en;    // pending references of the current cell
   int iters;         // cells left before the hard stop
-#if FFB_MAILBOX > 0
-  int mb[FFB_MAILBOX];  // faces tested most recently (a face repeats in neighbouring cells)
-#endif
 };
 
 template <bool kSkip>
 __device__ __forceinline__ void tracer_enter(Tracer& T, const GridView& g)
 {
   const int cell = (T.cz * g.ny + T.cy) * g.nx + T.cx;
-#if FFB_CELL_REC
   const uint2 r = __ldg(g.cell_rec + cell);
   const bool empty = (r.y & kCellEmpty) != 0;
   T.jump = kSkip && empty ? (int)(r.y & 0xFFu) : 0;
   T.i = r.x;
   T.en = empty ? 0u : r.y;
-#else
-  T.jump = kSkip ? (int)__ldg(g.empty_dist + cell) : 0;
-  if (T.jump == 0) {
-    T.i = __ldg(g.cell_start + cell);
-    T.en = __ldg(g.cell_start + cell + 1);
-  } else {
-    T.i = T.en = 0;
-  }
-#endif
 }
 
 // Sets up a ray; false when it misses the grid box (no hit possible).
@@ -546,11 +511,6 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
   T.best_ref = -1;
   T.iters = g.nx + g.ny + g.nz + 3;
-#if FFB_MAILBOX > 0
-#pragma unroll
-  for (int k = 0; k < FFB_MAILBOX; ++k)
-    T.mb[k] = -1;
-#endif
   ++n_cells;
   tracer_enter<kSkip>(T, g);
   return true;
@@ -563,25 +523,8 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
 __device__ __forceinline__ void tracer_test(Tracer& T, const GridView& g, uint32_t& n_tests)
 {
   const uint32_t i = T.i++;
-#if FFB_MAILBOX > 0
-  const int f = __ldg(g.ref_tri + i);
-  bool seen = false;
-#pragma unroll
-  for (int k = 0; k < FFB_MAILBOX; ++k)
-    seen |= T.mb[k] == f;
-  if (seen)
-    return;  // same face, same ray: the same test result as before
-#pragma unroll
-  for (int k = FFB_MAILBOX - 1; k > 0; --k)
-    T.mb[k] = T.mb[k - 1];
-  T.mb[0] = f;
-#endif
   ++n_tests;
   const float4* rec = reinterpret_cast<const float4*>(g.ref_rec + i);
-#if FFB_PREFETCH
-  if (T.i < T.en)  // the next record of the cell, while this one is tested
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.ref_rec + T.i));
-#endif
   float3 pt;
   if (tri_hit_regs(__ldg(rec), __ldg(rec + 1), __ldg(rec + 2), __ldg(rec + 3), T.o, T.dir, pt)) {
     const float d = dist2(pt, T.o);
@@ -620,7 +563,6 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
   if (!(tx < T.t1) || --T.iters <= 0)
     return false;
   const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
-#if FFB_UNIFIED_ADVANCE
   if (kSkip) {
     // Every move leaves the empty cube of half-width jump-1 around the cell
     // (the cell itself when jump <= 1, where the exit parameter is the DDA's
@@ -661,38 +603,9 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
     tracer_enter<kSkip>(T, g);
     return true;
   }
-#endif
-  if (kSkip && T.jump >= 2) {
-    // every cell within Chebyshev distance jump-1 is empty: leave that cube
-    const int jump = T.jump;
-    float tj = INFINITY;
-    if (sx) tj = fminf(tj, boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x));
-    if (sy) tj = fminf(tj, boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y));
-    if (sz) tj = fminf(tj, boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z));
-    if (!(tj < T.t1))
-      return false;
-    const int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
-    const int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
-    const int nz = land(sz, T.cz, jump, T.o.z, T.dir.z, tj, g.lo.z, g.inv_cs.z);
-    if (nx != T.cx || ny != T.cy || nz != T.cz) {
-      T.cx = nx;
-      T.cy = ny;
-      T.cz = nz;
-      if ((unsigned)nx >= (unsigned)g.nx || (unsigned)ny >= (unsigned)g.ny || (unsigned)nz >= (unsigned)g.nz)
-        return false;
-      T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
-      T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
-      T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
-      ++n_cells;
-      ++n_jumps;
-      tracer_enter<kSkip>(T, g);
-      return true;
-    }
-  }
-  // one DDA step along the axis whose boundary comes first
-#if FFB_SELECT_STEP
-  // the axis is chosen with selects, so that lanes stepping along different
-  // axes run the same instructions
+  // one DDA step along the axis whose boundary comes first, the axis chosen
+  // with selects so that lanes stepping along different axes run the same
+  // instructions
   const bool ax = T.tnx <= T.tny && T.tnx <= T.tnz;
   const bool ay = !ax && T.tny <= T.tnz;
   const int s = ax ? sx : (ay ? sy : sz);
@@ -707,24 +620,6 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
   T.tnx = ax ? tn : T.tnx;
   T.tny = ay ? tn : T.tny;
   T.tnz = (ax || ay) ? T.tnz : tn;
-#else
-  if (T.tnx <= T.tny && T.tnx <= T.tnz) {
-    T.cx += sx;
-    if ((unsigned)T.cx >= (unsigned)g.nx)
-      return false;
-    T.tnx = next_t(sx, T.cx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
-  } else if (T.tny <= T.tnz) {
-    T.cy += sy;
-    if ((unsigned)T.cy >= (unsigned)g.ny)
-      return false;
-    T.tny = next_t(sy, T.cy, g.lo.y, g.cs.y, T.o.y, T.inv.y);
-  } else {
-    T.cz += sz;
-    if ((unsigned)T.cz >= (unsigned)g.nz)
-      return false;
-    T.tnz = next_t(sz, T.cz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
-  }
-#endif
   ++n_cells;
   tracer_enter<kSkip>(T, g);
   return true;

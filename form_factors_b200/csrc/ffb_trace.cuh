@@ -124,8 +124,11 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // refilled together once at least kRefillMin of them wait (or the whole warp
 // is idle): emission and ray setup then run with several lanes at once
 // instead of one lane at a time.  Each iteration a lane whose cell is
-// exhausted moves on (stop, DDA step or empty-space jump) and, if its cell
-// has references left, tests one of them.  A finished hit adds one to the
+// exhausted moves on (stop, DDA step or empty-space jump; up to
+// FFB_ADV_PER_ITER moves while it lands in empty cells) and then tests up to
+// FFB_TEST_PER_ITER references of its cell.  Doing both kinds of work in one
+// iteration keeps lanes of a warp in the same code more of the time than
+// one kind per iteration does.  A finished hit adds one to the
 // warp's shared-memory hash histogram keyed by the matrix index
 // row(f) * n_cols + row(h); the warp flushes the table to the global uint32
 // matrix with atomic adds when it is half full, when it changes scene and at
@@ -142,20 +145,15 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // histogram merges little) and leaves the shared memory to the L1 cache.
 // ---------------------------------------------------------------------------
 #ifndef FFB_REFILL_MIN
-#define FFB_REFILL_MIN 4
+#define FFB_REFILL_MIN 6
 #endif
 constexpr int kRefillMin = FFB_REFILL_MIN;
-#ifndef FFB_IFIF
-#define FFB_IFIF 1
+// cell advances and triangle tests a lane may do per iteration
+#ifndef FFB_ADV_PER_ITER
+#define FFB_ADV_PER_ITER 2
 #endif
-#ifndef FFB_PHASE
-#define FFB_PHASE 0
-#endif
-#ifndef FFB_PHASE_TEST_COST
-#define FFB_PHASE_TEST_COST 100
-#endif
-#ifndef FFB_PHASE_ADV_COST
-#define FFB_PHASE_ADV_COST 160
+#ifndef FFB_TEST_PER_ITER
+#define FFB_TEST_PER_ITER 2
 #endif
 
 template <bool kSkip, int kScenes, bool kStats, bool kHash>
@@ -251,44 +249,22 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
       break;
     const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
     int hit = -1;
-#if FFB_PHASE
-    // One body per iteration for the whole warp: the triangle test or the
-    // cell advance, whichever moves more lanes per instruction; lanes in the
-    // other state wait one iteration.
-    {
-      const bool want_test = active && T.i < T.en;
-      const int n_test = __popc(__ballot_sync(kFull, want_test));
-      const int n_adv = __popc(__ballot_sync(kFull, active && !want_test));
-      const bool test_phase = n_test * FFB_PHASE_ADV_COST >= n_adv * FFB_PHASE_TEST_COST;
-      if (active) {
-        if (test_phase) {
-          if (want_test)
-            tracer_test(T, S.g, n_tests);
-        } else if (!want_test && !tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
-          active = false;
-          hit = tracer_result(T, S.g);
-        }
-      }
-    }
-#else
     if (active) {
-#if FFB_IFIF
-      if (T.i >= T.en && !tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
+      bool live = true;
+#pragma unroll
+      for (int k = 0; k < FFB_ADV_PER_ITER; ++k)
+        if (live && T.i >= T.en)
+          live = tracer_advance<kSkip>(T, S.g, n_cells, n_jumps);
+      if (!live) {
         active = false;
         hit = tracer_result(T, S.g);
-      } else if (T.i < T.en) {
-        tracer_test(T, S.g, n_tests);
+      } else {
+#pragma unroll
+        for (int k = 0; k < FFB_TEST_PER_ITER; ++k)
+          if (T.i < T.en)
+            tracer_test(T, S.g, n_tests);
       }
-#else
-      if (T.i < T.en) {
-        tracer_test(T, S.g, n_tests);
-      } else if (!tracer_advance<kSkip>(T, S.g, n_cells, n_jumps)) {
-        active = false;
-        hit = tracer_result(T, S.g);
-      }
-#endif
     }
-#endif
     bool fresh = false;
     if (hit >= 0) {
       ++n_hits;
@@ -354,7 +330,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
   };
   for (;;) {
     const unsigned need = __ballot_sync(kFull, !active);
-    if (need && !exhausted) {
+    if ((__popc(need) >= kRefillMin || need == kFull) && !exhausted) {
       unsigned long long base = 0;
       if (lane == 0)
         base = atomicAdd(cursor, (unsigned long long)__popc(need));
@@ -377,11 +353,19 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
     if (exhausted && !__any_sync(kFull, active))
       break;
     if (active) {
-      if (T.i < T.en) {
-        tracer_test(T, g, n_tests);
-      } else if (!tracer_advance<kSkip>(T, g, n_cells, n_jumps)) {
+      bool live = true;
+#pragma unroll
+      for (int k = 0; k < FFB_ADV_PER_ITER; ++k)
+        if (live && T.i >= T.en)
+          live = tracer_advance<kSkip>(T, g, n_cells, n_jumps);
+      if (!live) {
         active = false;
         finish(id, tracer_result(T, g), T.best_pt);
+      } else {
+#pragma unroll
+        for (int k = 0; k < FFB_TEST_PER_ITER; ++k)
+          if (T.i < T.en)
+            tracer_test(T, g, n_tests);
       }
     }
   }

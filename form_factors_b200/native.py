@@ -203,8 +203,10 @@ class Context:
         _check(self._lib.ffb_scene_set(self._h, _ptr(faces) if n else None, n))
         self.n_faces = n
 
-    def grid_build(self, dims=None, cells_per_face=2.0, skip_empty=True):
-        p = GridParams(0, 0, 0, float(cells_per_face), int(bool(skip_empty)))
+    def grid_build(self, dims=None, cells_per_face=None, skip_empty=True):
+        """Builds the grid: explicit dims, else about cells_per_face cells per
+        face (None: the library default, 32)."""
+        p = GridParams(0, 0, 0, float(cells_per_face or 0.0), int(bool(skip_empty)))
         if dims is not None:
             p.nx, p.ny, p.nz = [int(d) for d in dims]
         _check(self._lib.ffb_grid_build(self._h, C.byref(p)))

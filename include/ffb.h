@@ -48,7 +48,7 @@ typedef struct ffb_ctx ffb_ctx;
 
 typedef struct {
   int nx, ny, nz;          /* cells per axis, each <= 256; 0 = choose from cells_per_face */
-  float cells_per_face;    /* automatic sizing target (cells ~ this * faces); <= 0 means 2 */
+  float cells_per_face;    /* automatic sizing target (cells ~ this * faces); <= 0 means 32 */
   int skip_empty;          /* 1 = jump through empty space (distance map), 0 = plain DDA */
 } ffb_grid_params;
 
