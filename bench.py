@@ -319,6 +319,14 @@ def fp32_peak(device):
     return best
 
 
+def measured_hbm_gbs():
+    """Copy bandwidth of this pool's B200s, measured by the driver (GB/s)."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0  # earlier measurement on this pool
+
+
 def traffic_per_launch():
     """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
@@ -424,7 +432,9 @@ def ours(args):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    n_chunks = sum((int(f) + 1023) // 1024 for f in (front + rear))  # hash-histogram chunks of 1024 rays
+    # host -> device per step: the 16-byte work chunks (256 rays each) built
+    # from the host ray counts
+    n_chunks = sum((int(f) + 255) // 256 for f in (front + rear))
     h2d = 16 * n_chunks
     d2h = 4 * n * n
 
@@ -463,7 +473,11 @@ def ours(args):
                          "kernel": "k_form_factors", "kernel_ms": k_ms,
                          "work": "%d FP32 ops per ray/triangle test x %.4g tests per launch" % (
                              FLOPS_PER_TEST, tests_per_launch),
-                         "peak_source": "measured live: FMUL+FADD issue probe (libffb200_probe.so)"},
+                         "peak_source": "measured live: FMUL+FADD issue probe (libffb200_probe.so)",
+                         "hbm": {"achieved_gbs": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9,
+                                 "peak_gbs": measured_hbm_gbs(),
+                                 "frac": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
+                                 "note": "DRAM bytes per launch (ncu) / kernel time, of measured copy bandwidth"}},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,
             "hit_fraction": hits / rays_per_step,
