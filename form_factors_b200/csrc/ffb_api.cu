@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "ffb.h"
+#include "ffb_csv.cuh"
 #include "ffb_trace.cuh"
 
 using namespace ffb;
@@ -100,6 +101,9 @@ struct ffb_ctx {
 
   // per-call scratch
   DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
+  DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
+  void* csv_pinned[2] = {nullptr, nullptr};     // double-buffered text on its way to a file
+  size_t csv_pinned_cap[2] = {0, 0};
   void* pinned = nullptr;
   size_t pinned_cap = 0;
   cudaEvent_t pinned_free = nullptr;  // recorded after the last copy out of `pinned`
@@ -554,12 +558,15 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   DevBuf* bufs[] = {&c->frames,   &c->batch_frames, &c->batch_chunks, &c->batch_keys, &c->batch_epoch,
                     &c->scan_sums, &c->chunks,      &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
-                    &c->ray_cursor, &c->ff_counts};
+                    &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
   if (c->pinned)
     cudaFreeHost(c->pinned);
+  for (void* p : c->csv_pinned)
+    if (p)
+      cudaFreeHost(p);
   if (c->pinned_free) cudaEventDestroy(c->pinned_free);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -577,6 +584,13 @@ extern "C" int ffb_ctx_set_stream(ffb_ctx* c, void* stream)
 }
 
 extern "C" void* ffb_ctx_stream(ffb_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int ffb_ctx_synchronize(ffb_ctx* c)
+{
+  FFB_TRY(check_ctx(c));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  return FFB_OK;
+}
 
 extern "C" int ffb_ctx_set_budget(ffb_ctx* c, unsigned long long bytes)
 {
@@ -890,6 +904,174 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   FFB_TRY(ffb_form_factor_counts(c, front, rear, seed, epoch, flags, face_to_row, n_rows,
                                  dptr<uint32_t>(c->ff_counts)));
   return ffb_normalise(c, dptr<uint32_t>(c->ff_counts), outgoing, n_rows, ff);
+}
+
+// ===========================================================================
+// CSV text of the matrix (csv_export::export_csv, import_export/csv_export.cpp:26-46)
+// ===========================================================================
+namespace {
+
+constexpr long long kCsvSegment = 1ll << 24;  // entries per segment (a multiple of csv::kTile)
+
+// Formats the n x n matrix of `src` segment by segment.  Exactly one of the
+// sinks is used: text (device or host buffer of cap bytes), file, or neither
+// (length only).  *total gets the text length.
+int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FILE* file, unsigned long long* total)
+{
+  // per device (the attribute belongs to the current device); cheap to repeat
+  FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_write, cudaFuncAttributeMaxDynamicSharedMemorySize, csv::kTileBytes));
+  const long long n_entries = (long long)src.n * src.n;
+  const int seg_tiles = (int)(kCsvSegment / csv::kTile);
+  FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * seg_tiles));
+  FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (seg_tiles + 1)));
+  const bool dev_text = text && is_device_ptr(text);
+  unsigned long long running = 0, prev_len = 0;
+  int prev = -1, cur = 0;
+  for (long long e0 = 0; e0 < n_entries; e0 += kCsvSegment) {
+    src.e0 = e0;
+    src.n_entries = std::min(kCsvSegment, n_entries - e0);
+    const int tiles = (int)((src.n_entries + csv::kTile - 1) / csv::kTile);
+    csv::k_csv_len<<<tiles, csv::kThreads, 0, c->stream>>>(src, dptr<unsigned long long>(c->csv_tile_len));
+    csv::k_csv_scan<<<1, csv::kScanThreads, 0, c->stream>>>(dptr<unsigned long long>(c->csv_tile_len), tiles,
+                                                              dptr<unsigned long long>(c->csv_tile_off));
+    FFB_CUDA(cudaGetLastError());
+    unsigned long long seg = 0;
+    FFB_CUDA(cudaMemcpyAsync(&seg, dptr<unsigned long long>(c->csv_tile_off) + tiles, sizeof seg,
+                             cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));  // also completes the previous segment's copy out
+    if (!text && !file) {
+      running += seg;
+      continue;
+    }
+    if (text && running + seg > cap)
+      return fail(FFB_ERR_ARG, "CSV text needs more than the %llu-byte buffer", cap);
+    char* out;
+    if (dev_text) {
+      out = text + running;
+    } else {
+      FFB_TRY(ensure(c, c->csv_text, std::max<size_t>(seg, 16)));
+      out = dptr<char>(c->csv_text);
+    }
+    csv::k_csv_write<<<tiles, csv::kThreads, csv::kTileBytes, c->stream>>>(
+        src, dptr<unsigned long long>(c->csv_tile_off), out);
+    FFB_CUDA(cudaGetLastError());
+    if (text && !dev_text) {
+      FFB_CUDA(cudaMemcpyAsync(text + running, out, seg, cudaMemcpyDeviceToHost, c->stream));
+    } else if (file) {
+      if (seg > c->csv_pinned_cap[cur]) {
+        if (c->csv_pinned[cur])
+          cudaFreeHost(c->csv_pinned[cur]);
+        c->csv_pinned[cur] = nullptr;
+        c->csv_pinned_cap[cur] = 0;
+        FFB_CUDA(cudaMallocHost(&c->csv_pinned[cur], seg));
+        c->csv_pinned_cap[cur] = seg;
+      }
+      FFB_CUDA(cudaMemcpyAsync(c->csv_pinned[cur], out, seg, cudaMemcpyDeviceToHost, c->stream));
+      // the host writes the previous segment while the GPU formats this one
+      if (prev >= 0 && fwrite(c->csv_pinned[prev], 1, prev_len, file) != prev_len)
+        return fail(FFB_ERR_FILE, "CSV write failed");
+      prev = cur;
+      prev_len = seg;
+      cur ^= 1;
+    }
+    running += seg;
+  }
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  if (file && prev >= 0 && fwrite(c->csv_pinned[prev], 1, prev_len, file) != prev_len)
+    return fail(FFB_ERR_FILE, "CSV write failed");
+  *total = running;
+  return FFB_OK;
+}
+
+int csv_source(ffb_ctx* c, const float* ff, const uint32_t* counts, const int32_t* outgoing, int n, csv::Source* src)
+{
+  FFB_TRY(check_ctx(c));
+  if (n < 0 || (!ff && (!counts || !outgoing)))
+    return fail(FFB_ERR_ARG, "bad CSV arguments");
+  if (n > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "n %d above %d", n, kMaxRows);
+  const size_t mat = (size_t)n * n;
+  memset(src, 0, sizeof *src);
+  src->n = n;
+  if (!n)
+    return FFB_OK;
+  if (ff) {
+    const void* d;
+    FFB_TRY(input_ptr(c, ff, sizeof(float) * mat, c->tmp_in, &d));
+    src->ff = (const float*)d;
+  } else {
+    const void* d;
+    FFB_TRY(input_ptr(c, counts, sizeof(uint32_t) * mat, c->tmp_in, &d));
+    src->counts = (const uint32_t*)d;
+    const void* o;
+    FFB_TRY(input_ptr(c, outgoing, sizeof(int32_t) * (size_t)n, c->front_dev, &o));
+    src->outgoing = (const int32_t*)o;
+  }
+  return FFB_OK;
+}
+
+int csv_format(ffb_ctx* c, const float* ff, const uint32_t* counts, const int32_t* outgoing, int n, char* text,
+               unsigned long long text_cap, unsigned long long* text_len)
+{
+  if (!text_len)
+    return fail(FFB_ERR_ARG, "null text_len");
+  csv::Source src;
+  FFB_TRY(csv_source(c, ff, counts, outgoing, n, &src));
+  unsigned long long total = 0;
+  if (n)
+    FFB_TRY(csv_run(c, src, text, text_cap, nullptr, &total));
+  *text_len = total;
+  return FFB_OK;
+}
+
+int csv_export(ffb_ctx* c, const char* filename, const float* ff, const uint32_t* counts, const int32_t* outgoing,
+               int n)
+{
+  if (!filename)
+    return fail(FFB_ERR_ARG, "null file name");
+  csv::Source src;
+  FFB_TRY(csv_source(c, ff, counts, outgoing, n, &src));
+  FILE* f = fopen(filename, "wb");
+  if (!f)
+    return fail(FFB_ERR_FILE, "cannot open %s for writing", filename);
+  unsigned long long total = 0;
+  const int rc = n ? csv_run(c, src, nullptr, 0, f, &total) : FFB_OK;
+  if (fclose(f) != 0 && rc == FFB_OK)
+    return fail(FFB_ERR_FILE, "closing %s failed", filename);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int ffb_csv_format(ffb_ctx* c, const float* ff, int n, char* text, unsigned long long text_cap,
+                              unsigned long long* text_len)
+{
+  if (!ff && n)
+    return fail(FFB_ERR_ARG, "null matrix");
+  return csv_format(c, ff, nullptr, nullptr, n, text, text_cap, text_len);
+}
+
+extern "C" int ffb_csv_format_counts(ffb_ctx* c, const uint32_t* counts, const int32_t* outgoing, int n, char* text,
+                                     unsigned long long text_cap, unsigned long long* text_len)
+{
+  if ((!counts || !outgoing) && n)
+    return fail(FFB_ERR_ARG, "null counts or outgoing");
+  return csv_format(c, nullptr, counts, outgoing, n, text, text_cap, text_len);
+}
+
+extern "C" int ffb_csv_export(ffb_ctx* c, const char* filename, const float* ff, int n)
+{
+  if (!ff && n)
+    return fail(FFB_ERR_ARG, "null matrix");
+  return csv_export(c, filename, ff, nullptr, nullptr, n);
+}
+
+extern "C" int ffb_csv_export_counts(ffb_ctx* c, const char* filename, const uint32_t* counts, const int32_t* outgoing,
+                                     int n)
+{
+  if ((!counts || !outgoing) && n)
+    return fail(FFB_ERR_ARG, "null counts or outgoing");
+  return csv_export(c, filename, nullptr, counts, outgoing, n);
 }
 
 // ===========================================================================

@@ -21,6 +21,7 @@ FFB_EMIT_REF_NORMAL = 1
 ERRORS = {
     -301: "FFB_ERR_ARG", -302: "FFB_ERR_CUDA", -303: "FFB_ERR_NO_SCENE", -304: "FFB_ERR_NO_GRID",
     -305: "FFB_ERR_NO_MEMORY", -306: "FFB_ERR_TOO_LARGE", -307: "FFB_ERR_NO_DEVICE", -308: "FFB_ERR_TIMEOUT",
+    -309: "FFB_ERR_FILE",
 }
 
 
@@ -80,6 +81,7 @@ def load(path=LIB_PATH):
         "ffb_ctx_destroy": (None, [vp]),
         "ffb_ctx_set_stream": (i32, [vp, vp]),
         "ffb_ctx_stream": (vp, [vp]),
+        "ffb_ctx_synchronize": (i32, [vp]),
         "ffb_ctx_set_budget": (i32, [vp, C.c_ulonglong]),
         "ffb_ctx_set_stats": (i32, [vp, i32]),
         "ffb_ctx_bytes": (C.c_ulonglong, [vp]),
@@ -92,6 +94,10 @@ def load(path=LIB_PATH):
         "ffb_emit": (i32, [vp, vp, vp, u64, u32, i32, vp]),
         "ffb_form_factor_counts": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp]),
         "ffb_normalise": (i32, [vp, vp, vp, i32, vp]),
+        "ffb_csv_format": (i32, [vp, vp, i32, vp, C.c_ulonglong, C.POINTER(C.c_ulonglong)]),
+        "ffb_csv_format_counts": (i32, [vp, vp, vp, i32, vp, C.c_ulonglong, C.POINTER(C.c_ulonglong)]),
+        "ffb_csv_export": (i32, [vp, C.c_char_p, vp, i32]),
+        "ffb_csv_export_counts": (i32, [vp, C.c_char_p, vp, vp, i32]),
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
         "ffb_cast_bruteforce_static": (i32, [vp, i32, vp, i64, vp, vp, vp]),
         "ffb_form_factors": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp, vp]),
@@ -181,6 +187,10 @@ class Context:
     def set_stream(self, stream_ptr):
         """Use a cudaStream_t (an int address); 0/None restores the context's own stream."""
         _check(self._lib.ffb_ctx_set_stream(self._h, stream_ptr or None))
+
+    def synchronize(self):
+        """Waits for the context stream (batched launches only enqueue)."""
+        _check(self._lib.ffb_ctx_synchronize(self._h))
 
     def stream_ptr(self):
         return int(self._lib.ffb_ctx_stream(self._h) or 0)
@@ -297,6 +307,55 @@ class Context:
             out = np.empty((n, n), np.float32)
         _check(self._lib.ffb_normalise(self._h, _ptr(counts), _ptr(outgoing), n, _ptr(out)))
         return out
+
+    @staticmethod
+    def _csv_args(ff, counts, outgoing):
+        if ff is not None:
+            if isinstance(ff, np.ndarray):
+                ff = np.ascontiguousarray(ff, np.float32)
+            n = int(ff.shape[0]) if ff.ndim == 2 else int(round(ff.shape[0] ** 0.5))
+            return ff, None, None, n
+        outgoing = np.ascontiguousarray(outgoing, np.int32) if isinstance(outgoing, (np.ndarray, list)) else outgoing
+        if isinstance(counts, np.ndarray):
+            counts = np.ascontiguousarray(counts, np.uint32)
+        return None, counts, outgoing, int(len(outgoing))
+
+    def csv_length(self, ff=None, counts=None, outgoing=None):
+        """Length in bytes of the CSV text of the matrix (ff, or counts
+        normalised by outgoing)."""
+        ff, counts, outgoing, n = self._csv_args(ff, counts, outgoing)
+        ln = C.c_ulonglong()
+        if ff is not None:
+            _check(self._lib.ffb_csv_format(self._h, _ptr(ff), n, None, 0, C.byref(ln)))
+        else:
+            _check(self._lib.ffb_csv_format_counts(self._h, _ptr(counts), _ptr(outgoing), n, None, 0, C.byref(ln)))
+        return ln.value
+
+    def csv_format(self, ff=None, counts=None, outgoing=None, out=None):
+        """CSV text of the matrix as the reference's csv_export writes it.
+        Returns bytes, or, with `out` (a host or device byte buffer), the
+        number of bytes written into it."""
+        ff, counts, outgoing, n = self._csv_args(ff, counts, outgoing)
+        ret_bytes = out is None
+        if out is None:
+            out = np.empty(max(self.csv_length(ff=ff, counts=counts, outgoing=outgoing), 1), np.uint8)
+        cap = out.nbytes if isinstance(out, np.ndarray) else out.numel() * out.element_size()
+        ln = C.c_ulonglong()
+        if ff is not None:
+            _check(self._lib.ffb_csv_format(self._h, _ptr(ff), n, _ptr(out), cap, C.byref(ln)))
+        else:
+            _check(self._lib.ffb_csv_format_counts(self._h, _ptr(counts), _ptr(outgoing), n, _ptr(out), cap,
+                                                   C.byref(ln)))
+        return out[:ln.value].tobytes() if ret_bytes else ln.value
+
+    def csv_export(self, filename, ff=None, counts=None, outgoing=None):
+        """Writes the CSV file (ffb_csv_export / ffb_csv_export_counts)."""
+        ff, counts, outgoing, n = self._csv_args(ff, counts, outgoing)
+        name = os.fsencode(filename)
+        if ff is not None:
+            _check(self._lib.ffb_csv_export(self._h, name, _ptr(ff), n))
+        else:
+            _check(self._lib.ffb_csv_export_counts(self._h, name, _ptr(counts), _ptr(outgoing), n))
 
     def form_factors(self, front, rear, seed, epoch=0, flags=0, face_to_row=None, n_rows=None, outgoing=None,
                      out=None):

@@ -38,6 +38,7 @@ extern "C" {
 #define FFB_ERR_TOO_LARGE (-306) /* a size beyond a documented limit */
 #define FFB_ERR_NO_DEVICE (-307) /* no CUDA device / not an sm_100 device */
 #define FFB_ERR_TIMEOUT (-308)   /* a wait ended before the work finished */
+#define FFB_ERR_FILE (-309)      /* a file could not be opened or written */
 
 /* Emission flag: rotate +z towards the raw cross-product normal, as the
  * reference's emission/malley_cpu.cpp:125-129 does.  Without it the normal is
@@ -78,6 +79,10 @@ void ffb_ctx_destroy(ffb_ctx* ctx);
 /* Use `stream` (a cudaStream_t) instead of the context's own; NULL restores it. */
 int ffb_ctx_set_stream(ffb_ctx* ctx, void* stream);
 void* ffb_ctx_stream(ffb_ctx* ctx);
+/* Waits for all work enqueued on the context's stream (the batched launch
+ * and calls with device outputs return without waiting).  No reference
+ * counterpart: the reference's calls are synchronous. */
+int ffb_ctx_synchronize(ffb_ctx* ctx);
 /* Device-memory budget of the context in bytes (0 = unlimited). */
 int ffb_ctx_set_budget(ffb_ctx* ctx, unsigned long long bytes);
 unsigned long long ffb_ctx_bytes(ffb_ctx* ctx);
@@ -214,6 +219,27 @@ int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts
 /* Frees a finished request's resident matrix and its budget reservation. */
 int ffb_server_release(ffb_server* server, long long request_id);
 int ffb_server_stats(ffb_server* server, ffb_server_info* out);
+
+/* CSV text of an n x n form-factor matrix, byte for byte the file of
+ * csv_export::export_csv (import_export/csv_export.cpp:26-46): row i is the n
+ * entries of matrix row i as `std::ostream << float` prints them ("%g",
+ * 6 significant digits), separated by ';', each row ended by '\n'.
+ *
+ * ffb_csv_format: ff is host or device (n*n floats); text is a host or device
+ * buffer of text_cap bytes, or NULL to get only the length in *text_len.
+ * ffb_csv_format_counts: the same for counts normalised on the fly by their
+ * row's outgoing rays, as ffb_normalise computes them (no float matrix is
+ * formed).  FFB_ERR_ARG if the text does not fit text_cap.
+ * ffb_csv_export / ffb_csv_export_counts: write the text to `filename`
+ * (created or truncated); FFB_ERR_FILE when it cannot be opened or written,
+ * where the reference returns -CSV_EXPORT_FILE_ERROR.  n == 0 writes an empty
+ * file, as the reference does for a scene without meshes. */
+int ffb_csv_format(ffb_ctx* ctx, const float* ff, int n, char* text, unsigned long long text_cap,
+                   unsigned long long* text_len);
+int ffb_csv_format_counts(ffb_ctx* ctx, const uint32_t* counts, const int32_t* outgoing, int n, char* text,
+                          unsigned long long text_cap, unsigned long long* text_len);
+int ffb_csv_export(ffb_ctx* ctx, const char* filename, const float* ff, int n);
+int ffb_csv_export_counts(ffb_ctx* ctx, const char* filename, const uint32_t* counts, const int32_t* outgoing, int n);
 
 /* Grid autotuner: builds the grid with each candidate (resolution,
  * cells_per_face, empty-space jumps), times the fused kernel on a sample of

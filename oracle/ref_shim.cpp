@@ -13,7 +13,9 @@
 //   form_factors::system_create / set_scene / prepare / calculate  form_factors/system.cpp:45-106
 //   math::triangle_intersect                                  math/triangle.cpp:28-79
 //   math::rotate_towards                                      math/mat.cpp:25-49
+//   csv_export::export_csv                                    import_export/csv_export.cpp:26-46
 #include "ray_caster/system.h"
+#include "import_export/csv_export.h"
 #include "emission/system.h"
 #include "emission/malley_emission.h"
 #include "form_factors/system.h"
@@ -269,6 +271,20 @@ long ffref_step_run(void* handle, int n_rays, const float* weights2, float total
   task.rays = 0;
   emission::system_free(em);
   return n_cast;
+}
+
+// The reference's CSV export of an n x n matrix (n meshes, row-major floats).
+int ffref_export_csv(const char* filename, int n, const float* ff)
+{
+  form_factors::scene_t scene;
+  scene.n_faces = 0;
+  scene.faces = 0;
+  scene.n_meshes = n;
+  scene.meshes = 0;
+  form_factors::task_t task;
+  task.n_rays = 0;
+  task.form_factors = const_cast<float*>(ff);
+  return csv_export::export_csv(filename, &scene, &task);
 }
 
 void ffref_step_close(void* handle)

@@ -17,6 +17,12 @@ Fixtures (compressed .npz, all seeded):
   ff_ref.npz      the reference form-factor calculator (cpu_form_factors +
                   malley_cpu + naive_cpu, 40 000 rays) on the test scenes of
                   test/form_factors.cpp:78-186
+  csv_ref.npz     a 24 x 24 float matrix of edge values (signed zeros,
+                  infinities, NaNs, extremes, subnormals, ties at the seventh
+                  digit, count / outgoing ratios, random magnitudes) and the
+                  bytes csv_export::export_csv writes for it
+
+`python tests/golden/make_golden.py csv` writes csv_ref.npz only.
 """
 import os
 import sys
@@ -75,7 +81,32 @@ def kat_scenes():
     return out
 
 
+def csv_matrix(rng):
+    """24 x 24 float32 matrix exercising every branch of "%g" formatting."""
+    special = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, -np.nan, 3.4028235e38, -3.4028235e38,
+                        1.17549435e-38, 1e-45, -1e-45, 1e-40, 0.5, 1.0, 100000.0, 999999.0, 999999.5, 1e6,
+                        0.0001, 9.99999e-05, 1e-05, 123456.7, 0.1, 1.0 / 3.0], np.float32)
+    ties = np.ldexp(np.float32(1.0), np.arange(-149, 128, 3)).astype(np.float32)  # 93 powers of two
+    out = rng.integers(1, 5000, 150)
+    ratios = (rng.integers(0, 5000, 150) % (out + 1)).astype(np.float32) * (np.float32(1.0) / out.astype(np.float32))
+    mags = (rng.standard_normal(309) * np.float32(10.0) ** rng.integers(-40, 38, 309)).astype(np.float32)
+    v = np.concatenate([special, ties, ratios.astype(np.float32), mags])[:576]
+    return v.reshape(24, 24).astype(np.float32)
+
+
+def csv_fixture(ref, rng):
+    import tempfile
+    ff = csv_matrix(rng)
+    with tempfile.TemporaryDirectory() as d:
+        text = ref.csv_text(ff, d)
+    np.savez_compressed(os.path.join(HERE, "csv_ref.npz"), ff=ff, text=np.frombuffer(text, np.uint8))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "csv":
+        csv_fixture(Reference(), np.random.default_rng(20261204))
+        print("csv_ref.npz written to", HERE)
+        return
     if not Reference.available():
         sys.exit("oracle/_ref/libffref.so is missing: make -C oracle ref")
     ref = Reference()
@@ -162,6 +193,7 @@ def main():
     ff["box_faces"] = faces
     ff["box_ff"] = mat
     np.savez_compressed(os.path.join(HERE, "ff_ref.npz"), **ff)
+    csv_fixture(ref, np.random.default_rng(20261204))
     print("fixtures written to", HERE)
 
 

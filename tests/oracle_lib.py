@@ -153,7 +153,22 @@ class Reference:
                                        C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.ffref_step_run.restype = C.c_long
         lib.ffref_step_close.argtypes = [C.c_void_p]
+        lib.ffref_export_csv.argtypes = [C.c_char_p, C.c_int, _f32p]
+        lib.ffref_export_csv.restype = C.c_int
         self.lib = lib
+
+    def export_csv(self, filename, ff):
+        """csv_export::export_csv of an n x n float matrix; returns the
+        reference's status (0, or -31 when the file cannot be opened)."""
+        ff = np.ascontiguousarray(ff, np.float32)
+        return self.lib.ffref_export_csv(os.fsencode(filename), int(ff.shape[0]), ff)
+
+    def csv_text(self, ff, tmpdir):
+        path = os.path.join(str(tmpdir), "ref_%d.csv" % os.getpid())
+        rc = self.export_csv(path, ff)
+        assert rc == 0, rc
+        with open(path, "rb") as f:
+            return f.read()
 
     def triangle_intersect(self, ray6, tri9):
         pt = np.zeros(3, np.float32)

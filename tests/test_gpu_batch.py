@@ -28,6 +28,7 @@ def test_batch_equals_single_scene_path(ctx):
     offs, words = ctx.batch_counts_layout()
     counts = torch.empty(words, dtype=torch.int32, device="cuda")
     ctx.batch_launch(counts, offs, advance_epoch=True)  # epoch 1
+    ctx.synchronize()  # the launch only enqueues on the context stream
     got_all = counts.cpu().numpy().view(np.uint32)
     for i, f in enumerate(sl):
         n = len(f)
