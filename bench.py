@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
+    ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
     ap.add_argument("--served-requests", type=int, default=16)
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     return ap.parse_args()
@@ -304,6 +305,73 @@ def served_section(args):
 
 
 # ---------------------------------------------------------------------------
+# CSV export of the step's matrix (csv_export::export_csv)
+# ---------------------------------------------------------------------------
+def csv_section(ctx, stream, counts, front, rear, n):
+    """Formatting on the device from the resident counts (normalised on the
+    fly), and the reference-facing export of a host float matrix to a file,
+    against the reference's csv_export on a block of the same matrix."""
+    import shutil
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Reference
+    outgoing = (front.astype(np.int64) + rear).astype(np.int32)
+    d_out = torch.from_numpy(outgoing).cuda()
+    n_text = ctx.csv_length(counts=counts, outgoing=d_out)
+    text = torch.empty(n_text, dtype=torch.uint8, device="cuda")
+    ctx.csv_format(counts=counts, outgoing=d_out, out=text)  # warm-up
+    reps = 3
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.csv_format(counts=counts, outgoing=d_out, out=text)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fmt_s = ev0.elapsed_time(ev1) * 1e-3 / reps
+    entries = n * n
+    alg_bytes = 4 * entries + n_text  # each count read once, the text written once
+    del text
+    # end to end: host float matrix -> file, as csv_export::export_csv takes it
+    ff = ctx.normalise(counts, outgoing)
+    shm = "/dev/shm"
+    where = shm if os.path.isdir(shm) and shutil.disk_usage(shm).free > 3 * n_text else tempfile.gettempdir()
+    path = os.path.join(where, "ffb_bench_%d.csv" % os.getpid())
+    times = []
+    for _ in range(3):  # median: a new file's pages make single runs noisy
+        t0 = time.perf_counter()
+        ctx.csv_export(path, ff=ff)
+        times.append(time.perf_counter() - t0)
+        size = os.path.getsize(path)
+        os.remove(path)
+    exp_s = statistics.median(times)
+    ref = None
+    if Reference.available():
+        k = 2048  # a k x k block of the same matrix: the reference's export is single-threaded
+        block = np.ascontiguousarray(ff[:k, :k])
+        rpath = os.path.join(where, "ffb_bench_ref_%d.csv" % os.getpid())
+        r = Reference()
+        t0 = time.perf_counter()
+        rc = r.export_csv(rpath, block)
+        ref_s = time.perf_counter() - t0
+        os.remove(rpath)
+        if rc == 0:
+            ref = {"entries_per_s": k * k / ref_s, "cores": 1, "kind": "reference",
+                   "sample": "csv_export::export_csv (oracle/_ref) of the top-left %dx%d block of the same matrix "
+                             "to the same file system" % (k, k)}
+    return {
+        "workload": "CSV text of the %dx%d matrix of this step (csv_export::export_csv format)" % (n, n),
+        "entries": entries, "text_bytes": int(n_text),
+        "format_ms": fmt_s * 1e3, "format_entries_per_s": entries / fmt_s,
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / fmt_s / 1e9, "peak": measured_hbm_gbs(), "unit": "GB/s",
+                     "frac": alg_bytes / fmt_s / 1e9 / measured_hbm_gbs(),
+                     "work": "4 B count read + text bytes written per entry (algorithmic)"},
+        "export_s": exp_s, "export_entries_per_s": entries / exp_s, "export_bytes": size, "export_dir": where,
+        "export_path": "host float matrix -> H2D -> format -> D2H (pipelined) -> fwrite; median of 3",
+        "cpu_baseline": ref,
+    }
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def fp32_peak(device):
@@ -438,7 +506,9 @@ def ours(args):
     h2d = 16 * n_chunks
     d2h = 4 * n * n
 
-    batched = served = None
+    batched = served = csv = None
+    if rank == 0 and world == 1 and not args.no_csv:
+        csv = csv_section(ctx, stream, counts, front, rear, n)
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_section(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_served:
@@ -489,6 +559,8 @@ def ours(args):
             line["batched"] = batched
         if served is not None:
             line["served"] = served
+        if csv is not None:
+            line["csv"] = csv
         print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -911,75 +911,91 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
 // ===========================================================================
 namespace {
 
-constexpr long long kCsvSegment = 1ll << 24;  // entries per segment (a multiple of csv::kTile)
+constexpr int kCsvSegmentTiles = 4096;  // tiles per staged segment (16.8 M entries, <= 218 MB of text)
 
-// Formats the n x n matrix of `src` segment by segment.  Exactly one of the
-// sinks is used: text (device or host buffer of cap bytes), file, or neither
-// (length only).  *total gets the text length.
+// Formats the n x n matrix of `src`.  One length pass and one scan cover the
+// whole matrix; then the text goes to a device buffer in one launch, or, for
+// a host buffer or a file, segment by segment through a device staging
+// buffer (a file gets pinned double buffers: the host writes one segment
+// while the GPU formats the next).  Exactly one sink is used: text (device
+// or host, cap bytes), file, or neither (length only).  *total gets the
+// text length.
 int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FILE* file, unsigned long long* total)
 {
   // per device (the attribute belongs to the current device); cheap to repeat
-  FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_write, cudaFuncAttributeMaxDynamicSharedMemorySize, csv::kTileBytes));
-  const long long n_entries = (long long)src.n * src.n;
-  const int seg_tiles = (int)(kCsvSegment / csv::kTile);
-  FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * seg_tiles));
-  FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (seg_tiles + 1)));
-  const bool dev_text = text && is_device_ptr(text);
-  unsigned long long running = 0, prev_len = 0;
-  int prev = -1, cur = 0;
-  for (long long e0 = 0; e0 < n_entries; e0 += kCsvSegment) {
-    src.e0 = e0;
-    src.n_entries = std::min(kCsvSegment, n_entries - e0);
-    const int tiles = (int)((src.n_entries + csv::kTile - 1) / csv::kTile);
-    csv::k_csv_len<<<tiles, csv::kThreads, 0, c->stream>>>(src, dptr<unsigned long long>(c->csv_tile_len));
-    csv::k_csv_scan<<<1, csv::kScanThreads, 0, c->stream>>>(dptr<unsigned long long>(c->csv_tile_len), tiles,
-                                                              dptr<unsigned long long>(c->csv_tile_off));
+  FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_write, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)csv::write_smem(csv::kTileBytes)));
+  src.n_entries = (long long)src.n * src.n;
+  const long long n_tiles = (src.n_entries + csv::kTile - 1) / csv::kTile;
+  FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * (size_t)n_tiles));
+  FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (size_t)(n_tiles + 2)));
+  auto* tile_len = dptr<unsigned long long>(c->csv_tile_len);
+  auto* tile_off = dptr<unsigned long long>(c->csv_tile_off);
+  csv::k_csv_len<<<(unsigned)n_tiles, csv::kThreads, 0, c->stream>>>(src, tile_len);
+  csv::k_csv_scan<<<1, csv::kScanThreads, 0, c->stream>>>(tile_len, (int)n_tiles, tile_off);
+  FFB_CUDA(cudaGetLastError());
+  unsigned long long tail[2] = {0, 0};  // total, longest tile
+  FFB_CUDA(cudaMemcpyAsync(tail, tile_off + n_tiles, sizeof tail, cudaMemcpyDeviceToHost, c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  const unsigned long long all = tail[0];
+  *total = all;
+  // shared text region sized for the longest tile (sparse matrices: a few KB)
+  const size_t smem = csv::write_smem(tail[1]);
+  const uint32_t region = (uint32_t)(smem - csv::kIndexSmem);
+  if (!text && !file)
+    return FFB_OK;
+  if (text && all > cap)
+    return fail(FFB_ERR_ARG, "CSV text of %llu bytes does not fit the %llu-byte buffer", all, cap);
+  if (text && is_device_ptr(text)) {
+    csv::k_csv_write<<<(unsigned)n_tiles, csv::kThreads, smem, c->stream>>>(src, tile_off, 0, 0, region, text);
     FFB_CUDA(cudaGetLastError());
-    unsigned long long seg = 0;
-    FFB_CUDA(cudaMemcpyAsync(&seg, dptr<unsigned long long>(c->csv_tile_off) + tiles, sizeof seg,
-                             cudaMemcpyDeviceToHost, c->stream));
-    FFB_CUDA(cudaStreamSynchronize(c->stream));  // also completes the previous segment's copy out
-    if (!text && !file) {
-      running += seg;
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+    return FFB_OK;
+  }
+  // staged: segment byte ranges from the tile offsets
+  std::vector<unsigned long long> off((size_t)n_tiles + 1);
+  FFB_CUDA(cudaMemcpy(off.data(), tile_off, sizeof(unsigned long long) * off.size(), cudaMemcpyDeviceToHost));
+
+  unsigned long long seg_max = 0;
+  for (long long t = 0; t < n_tiles; t += kCsvSegmentTiles)
+    seg_max = std::max(seg_max, off[(size_t)std::min(n_tiles, t + kCsvSegmentTiles)] - off[(size_t)t]);
+  FFB_TRY(ensure(c, c->csv_text, std::max<size_t>(seg_max, 16)));
+  char* stage = dptr<char>(c->csv_text);
+  if (file) {
+    for (int k = 0; k < 2; ++k) {
+      if (seg_max > c->csv_pinned_cap[k]) {
+        if (c->csv_pinned[k])
+          cudaFreeHost(c->csv_pinned[k]);
+        c->csv_pinned[k] = nullptr;
+        c->csv_pinned_cap[k] = 0;
+        FFB_CUDA(cudaMallocHost(&c->csv_pinned[k], seg_max));
+        c->csv_pinned_cap[k] = seg_max;
+      }
+    }
+  }
+  int prev = -1, cur = 0;
+  unsigned long long prev_len = 0;
+  for (long long t = 0; t < n_tiles; t += kCsvSegmentTiles) {
+    const long long te = std::min(n_tiles, t + kCsvSegmentTiles);
+    const unsigned long long b0 = off[(size_t)t], len = off[(size_t)te] - b0;
+    csv::k_csv_write<<<(unsigned)(te - t), csv::kThreads, smem, c->stream>>>(src, tile_off, t, b0, region, stage);
+    FFB_CUDA(cudaGetLastError());
+    if (text) {
+      FFB_CUDA(cudaMemcpyAsync(text + b0, stage, len, cudaMemcpyDeviceToHost, c->stream));
       continue;
     }
-    if (text && running + seg > cap)
-      return fail(FFB_ERR_ARG, "CSV text needs more than the %llu-byte buffer", cap);
-    char* out;
-    if (dev_text) {
-      out = text + running;
-    } else {
-      FFB_TRY(ensure(c, c->csv_text, std::max<size_t>(seg, 16)));
-      out = dptr<char>(c->csv_text);
-    }
-    csv::k_csv_write<<<tiles, csv::kThreads, csv::kTileBytes, c->stream>>>(
-        src, dptr<unsigned long long>(c->csv_tile_off), out);
-    FFB_CUDA(cudaGetLastError());
-    if (text && !dev_text) {
-      FFB_CUDA(cudaMemcpyAsync(text + running, out, seg, cudaMemcpyDeviceToHost, c->stream));
-    } else if (file) {
-      if (seg > c->csv_pinned_cap[cur]) {
-        if (c->csv_pinned[cur])
-          cudaFreeHost(c->csv_pinned[cur]);
-        c->csv_pinned[cur] = nullptr;
-        c->csv_pinned_cap[cur] = 0;
-        FFB_CUDA(cudaMallocHost(&c->csv_pinned[cur], seg));
-        c->csv_pinned_cap[cur] = seg;
-      }
-      FFB_CUDA(cudaMemcpyAsync(c->csv_pinned[cur], out, seg, cudaMemcpyDeviceToHost, c->stream));
-      // the host writes the previous segment while the GPU formats this one
-      if (prev >= 0 && fwrite(c->csv_pinned[prev], 1, prev_len, file) != prev_len)
-        return fail(FFB_ERR_FILE, "CSV write failed");
-      prev = cur;
-      prev_len = seg;
-      cur ^= 1;
-    }
-    running += seg;
+    FFB_CUDA(cudaMemcpyAsync(c->csv_pinned[cur], stage, len, cudaMemcpyDeviceToHost, c->stream));
+    // the host writes the previous segment while the GPU formats this one
+    if (prev >= 0 && fwrite(c->csv_pinned[prev], 1, prev_len, file) != prev_len)
+      return fail(FFB_ERR_FILE, "CSV write failed");
+    FFB_CUDA(cudaStreamSynchronize(c->stream));  // this segment is in pinned[cur]; stage is free again
+    prev = cur;
+    prev_len = len;
+    cur ^= 1;
   }
   FFB_CUDA(cudaStreamSynchronize(c->stream));
   if (file && prev >= 0 && fwrite(c->csv_pinned[prev], 1, prev_len, file) != prev_len)
     return fail(FFB_ERR_FILE, "CSV write failed");
-  *total = running;
   return FFB_OK;
 }
 

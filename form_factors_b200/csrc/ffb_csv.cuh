@@ -200,19 +200,28 @@ __host__ __device__ inline Dec6 round6_general(uint32_t m, int q)
   return round6_from_7(n7, !big_zero(a), exp10);
 }
 
-__host__ __device__ inline int put_text(char* out, const char* t)
+// Text sinks of the formatter: a pointer (host buffers, shared memory) or a
+// counter (lengths only; the compiler drops the character work).
+struct PtrOut {
+  char* p;
+  int n;
+  __host__ __device__ void put(char c) { p[n++] = c; }
+};
+struct CountOut {
+  int n;
+  __host__ __device__ void put(char) { ++n; }
+};
+
+template <class Out>
+__host__ __device__ inline void put_text(Out& out, const char* t)
 {
-  int n = 0;
-  while (t[n]) {
-    out[n] = t[n];
-    ++n;
-  }
-  return n;
+  for (int i = 0; t[i]; ++i)
+    out.put(t[i]);
 }
 
-// Writes "%g" of f (precision 6) to out (no terminator); returns the length
-// (at most 12).
-__host__ __device__ inline int format_g6(float f, char* out)
+// Appends "%g" of f (precision 6) to out: at most 12 characters.
+template <class Out>
+__host__ __device__ inline void format_g6_to(float f, Out& out)
 {
   uint32_t bits;
 #ifdef __CUDA_ARCH__
@@ -222,117 +231,233 @@ __host__ __device__ inline int format_g6(float f, char* out)
 #endif
   const bool neg = bits >> 31;
   const uint32_t ex = (bits >> 23) & 0xFFu, fr = bits & 0x7FFFFFu;
-  int n = 0;
-  if (ex == 0xFFu)
-    return put_text(out, fr ? (neg ? "-nan" : "nan") : (neg ? "-inf" : "inf"));
+  if (ex == 0xFFu) {
+    put_text(out, fr ? (neg ? "-nan" : "nan") : (neg ? "-inf" : "inf"));
+    return;
+  }
   if (neg)
-    out[n++] = '-';
+    out.put('-');
   if (ex == 0 && fr == 0) {
-    out[n++] = '0';
-    return n;
+    out.put('0');
+    return;
   }
   const uint32_t m = ex ? (fr | 0x800000u) : fr;
   const int q = ex ? (int)ex - 150 : -149;
   const Dec6 d = (q < 0 && q >= -59) ? round6_small(m, -q) : round6_general(m, q);
-  char dg[6];
+  // digits of d.digits, most significant first, without trailing zeros
   uint32_t v = d.digits;
-  for (int i = 5; i >= 0; --i) {
-    dg[i] = (char)('0' + v % 10u);
+  int last = 5;
+  while (last > 0 && v % 10u == 0u) {
     v /= 10u;
-  }
-  int last = 5;  // last significant digit kept after stripping trailing zeros
-  while (last > 0 && dg[last] == '0')
     --last;
+  }
+  // v now holds digits 0..last; divisor picks them from the top
+  uint32_t div = 1;
+  for (int i = 0; i < last; ++i)
+    div *= 10u;
   const int X = d.exp10;
+  auto next_digit = [&]() {
+    const uint32_t dg = v / div;
+    v -= dg * div;
+    div /= 10u;
+    return (char)('0' + dg);
+  };
   if (X < -4 || X >= 6) {
-    out[n++] = dg[0];
+    out.put(next_digit());
     if (last > 0) {
-      out[n++] = '.';
+      out.put('.');
       for (int i = 1; i <= last; ++i)
-        out[n++] = dg[i];
+        out.put(next_digit());
     }
-    out[n++] = 'e';
-    out[n++] = X < 0 ? '-' : '+';
+    out.put('e');
+    out.put(X < 0 ? '-' : '+');
     const int ax = X < 0 ? -X : X;
     if (ax >= 100)
-      out[n++] = (char)('0' + ax / 100);
-    out[n++] = (char)('0' + (ax / 10) % 10);
-    out[n++] = (char)('0' + ax % 10);
-    return n;
+      out.put((char)('0' + ax / 100));
+    out.put((char)('0' + (ax / 10) % 10));
+    out.put((char)('0' + ax % 10));
+    return;
   }
   if (X >= 0) {
+    // integer digits 0..X (digits past `last` are zeros)
     for (int i = 0; i <= X; ++i)
-      out[n++] = dg[i];
+      out.put(i <= last ? next_digit() : '0');
     if (last > X) {
-      out[n++] = '.';
+      out.put('.');
       for (int i = X + 1; i <= last; ++i)
-        out[n++] = dg[i];
+        out.put(next_digit());
     }
-    return n;
+    return;
   }
-  out[n++] = '0';
-  out[n++] = '.';
+  out.put('0');
+  out.put('.');
   for (int i = 0; i < -X - 1; ++i)
-    out[n++] = '0';
+    out.put('0');
   for (int i = 0; i <= last; ++i)
-    out[n++] = dg[i];
-  return n;
+    out.put(next_digit());
+}
+
+// Writes "%g" of f to out (no terminator); returns the length.
+__host__ __device__ inline int format_g6(float f, char* out)
+{
+  PtrOut o{out, 0};
+  format_g6_to(f, o);
+  return o.n;
+}
+
+__host__ __device__ inline int format_g6_len(float f)
+{
+  CountOut o{0};
+  format_g6_to(f, o);
+  return o.n;
 }
 
 #ifdef __CUDACC__
 // ---------------------------------------------------------------------------
-// Kernels.  The matrix is processed in segments of consecutive entries
-// (row-major); a segment is cut into tiles of kTile entries, one block each.
-//  1. k_csv_len: the text length of every tile (entries + separators).
+// Kernels.  The matrix (row-major entries) is cut into tiles of kTile
+// entries, one block each.
+//  1. k_csv_len: the text length of every tile.
 //  2. k_csv_scan: exclusive prefix sums of the tile lengths (64-bit) and the
-//     segment's total.
-//  3. k_csv_write: each block formats its tile again into shared memory at
-//     its block-local offsets (a block-wide scan of the entry lengths), then
-//     copies the tile's text to its global offset with 16-byte stores.  The
-//     shared buffer starts at the destination's offset modulo 16, so shared
-//     and global addresses line up for the vector copy; only the ragged head
-//     and tail go byte by byte.
-// Reads: the 4-byte entry twice (plus the row's outgoing count); writes: the
-// text once.
+//     total.
+//  3. k_csv_write: each block lays its tile's text out in shared memory and
+//     copies it to its global offset with 16-byte stores (the shared buffer
+//     starts at the destination's offset modulo 16, so both sides line up;
+//     only the ragged head and tail go byte by byte).
+// In both passes an entry that is +0 costs a load and a compare ("0" plus
+// separator); the other entries go to a per-block queue and are formatted by
+// all threads together, so that a sparse matrix does not leave warps running
+// the formatter with one lane.  Per-entry offsets come from a block scan of
+// the entry lengths (16-bit: a tile's text is below 64 KB).
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
 constexpr int kPerThread = 16;
 constexpr int kTile = kThreads * kPerThread;            // entries per block
 constexpr int kTileBytes = kTile * (kMaxEntry - 3) + 16;  // 13 bytes per entry at most, + alignment shift
+constexpr size_t kIndexSmem = 2 * sizeof(uint16_t) * kTile;  // offsets + queue of k_csv_write
+// Dynamic shared memory of k_csv_write for tiles of at most max_tile bytes.
+__host__ __device__ inline size_t write_smem(unsigned long long max_tile)
+{
+  return (size_t)((max_tile + 16u + 15u) & ~15ull) + kIndexSmem;
+}
 
-// Entries [e0, e0 + n_entries) of an n x n matrix: floats, or counts
-// normalised by their row's outgoing rays as ffb_normalise does
-// ((float)count * (1.f / (float)outgoing[row]), cpu_system.cpp:193-195).
+// The n x n matrix: floats, or counts normalised by their row's outgoing
+// rays as ffb_normalise does ((float)count * (1.f / (float)outgoing[row]),
+// cpu_system.cpp:193-195).
 struct Source {
   const float* __restrict__ ff;
   const uint32_t* __restrict__ counts;
   const int32_t* __restrict__ outgoing;
   int n;
-  long long e0, n_entries;
+  long long n_entries;
 };
 
-__device__ __forceinline__ float entry_value(const Source& s, long long e, int row)
+__device__ __forceinline__ float row_ratio(const Source& s, int row)
 {
-  if (s.ff)
-    return __ldg(s.ff + e);
-  const float ratio = 1.f / (float)__ldg(s.outgoing + row);
-  return (float)__ldg(s.counts + e) * ratio;
+  return s.ff ? 1.f : 1.f / (float)__ldg(s.outgoing + row);
 }
 
-__global__ void __launch_bounds__(kThreads) k_csv_len(Source s, unsigned long long* __restrict__ tile_len)
+__device__ __forceinline__ float entry_value(const Source& s, long long e, float ratio)
 {
-  __shared__ uint32_t warp_sum[kThreads / 32];
-  const long long t0 = (long long)blockIdx.x * kTile;
-  const long long g0 = s.e0 + t0;
-  const int r0 = (int)(g0 / s.n), c0 = (int)(g0 - (long long)r0 * s.n);
-  uint32_t sum = 0;
-  char buf[kMaxEntry];
+  return s.ff ? __ldg(s.ff + e) : (float)__ldg(s.counts + e) * ratio;
+}
+
+// A thread's entries o = k * kThreads + tid of one tile, held in registers
+// for both walks of a kernel: the 16 loads are issued together.
+struct TileRegs {
+  float v[kPerThread];
+  int col0;  // column of the first entry
+};
+
+__device__ __forceinline__ void load_tile(const Source& s, long long tile, TileRegs& r)
+{
+  const long long e0 = tile * kTile + threadIdx.x;
+  uint32_t raw[kPerThread];
+#pragma unroll
+  for (int k = 0; k < kPerThread; ++k) {
+    const long long e = e0 + (long long)k * kThreads;
+    raw[k] = 0u;
+    if (e < s.n_entries)
+      raw[k] = s.ff ? __float_as_uint(__ldg(s.ff + e)) : __ldg(s.counts + e);
+  }
+  int row = (int)(e0 / s.n), col = (int)(e0 - (long long)row * s.n);
+  r.col0 = col;
+  float ratio = (!s.ff && row < s.n) ? row_ratio(s, row) : 1.f;
+#pragma unroll
+  for (int k = 0; k < kPerThread; ++k) {
+    r.v[k] = s.ff ? __uint_as_float(raw[k]) : (float)raw[k] * ratio;
+    col += kThreads;
+    if (col >= s.n) {
+      while (col >= s.n) {
+        col -= s.n;
+        ++row;
+      }
+      if (!s.ff && row < s.n)
+        ratio = row_ratio(s, row);
+    }
+  }
+}
+
+// fn(o, valid, value, col) for the thread's entries; it runs on every lane
+// of the warp each step (callers use warp votes); entries past the matrix end
+// come with valid = false.
+template <class Fn>
+__device__ __forceinline__ void walk_tile(const Source& s, long long tile, const TileRegs& r, Fn fn)
+{
+  int col = r.col0;
+#pragma unroll
   for (int k = 0; k < kPerThread; ++k) {
     const int o = k * kThreads + (int)threadIdx.x;
-    if (t0 + o < s.n_entries) {
-      const int row = r0 + (c0 + o) / s.n;
-      sum += (uint32_t)format_g6(entry_value(s, g0 + o, row), buf) + 1u;
-    }
+    fn(o, tile * kTile + o < s.n_entries, r.v[k], col);
+    col += kThreads;
+    while (col >= s.n)
+      col -= s.n;
+  }
+}
+
+// Value and column of entry o of the tile (queue work, one division).
+__device__ __forceinline__ float tile_value(const Source& s, long long tile, int o, int* col)
+{
+  const long long e = tile * kTile + o;
+  const int row = (int)(e / s.n);
+  *col = (int)(e - (long long)row * s.n);
+  return entry_value(s, e, row_ratio(s, row));
+}
+
+__device__ __forceinline__ void enqueue(uint16_t* queue, uint32_t* qn, bool take, int o)
+{
+  const unsigned mask = __ballot_sync(0xFFFFFFFFu, take);
+  if (!mask)
+    return;
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == __ffs(mask) - 1)
+    base = atomicAdd(qn, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xFFFFFFFFu, base, __ffs(mask) - 1);
+  if (take)
+    queue[base + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)o;
+}
+
+__global__ void __launch_bounds__(kThreads, 4) k_csv_len(Source s, unsigned long long* __restrict__ tile_len)
+{
+  __shared__ uint16_t queue[kTile];
+  __shared__ uint32_t qn;
+  __shared__ uint32_t warp_sum[kThreads / 32];
+  if (threadIdx.x == 0)
+    qn = 0;
+  __syncthreads();
+  uint32_t sum = 0;
+  TileRegs r;
+  load_tile(s, blockIdx.x, r);
+  walk_tile(s, blockIdx.x, r, [&](int o, bool valid, float v, int) {
+    const bool zero = __float_as_uint(v) == 0u;
+    sum += valid && zero ? 2u : 0u;
+    enqueue(queue, &qn, valid && !zero, o);
+  });
+  __syncthreads();
+  const uint32_t n_q = qn;
+  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+    int col;
+    sum += (uint32_t)format_g6_len(tile_value(s, blockIdx.x, queue[q], &col)) + 1u;
   }
   for (int off = 16; off > 0; off >>= 1)
     sum += __shfl_xor_sync(0xFFFFFFFFu, sum, off);
@@ -348,17 +473,25 @@ __global__ void __launch_bounds__(kThreads) k_csv_len(Source s, unsigned long lo
 }
 
 // Exclusive scan of n tile lengths (one block; each thread a contiguous run)
-// into out[0..n), and the total into out[n].
+// into out[0..n), the total into out[n] and the longest tile into out[n + 1].
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads) k_csv_scan(const unsigned long long* __restrict__ in, int n,
                                                            unsigned long long* __restrict__ out)
 {
   __shared__ unsigned long long warp_sum[kScanThreads / 32];
+  __shared__ unsigned long long warp_max[kScanThreads / 32];
   const int per = (n + kScanThreads - 1) / kScanThreads;
   const int b = (int)threadIdx.x * per, e = min(n, b + per);
-  unsigned long long s = 0;
-  for (int i = b; i < e; ++i)
-    s += in[i];
+  unsigned long long s = 0, mx = 0;
+  for (int i = b; i < e; ++i) {
+    const unsigned long long x = in[i];
+    s += x;
+    mx = x > mx ? x : mx;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xFFFFFFFFu, mx, off);
+    mx = y > mx ? y : mx;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long incl = s;
   for (int off = 1; off < 32; off <<= 1) {
@@ -368,6 +501,8 @@ __global__ void __launch_bounds__(kScanThreads) k_csv_scan(const unsigned long l
   }
   if (lane == 31)
     warp_sum[warp] = incl;
+  if (lane == 0)
+    warp_max[warp] = mx;
   __syncthreads();
   unsigned long long before = 0;
   for (int w = 0; w < warp; ++w)
@@ -377,55 +512,99 @@ __global__ void __launch_bounds__(kScanThreads) k_csv_scan(const unsigned long l
     out[i] = run;
     run += in[i];
   }
-  if (threadIdx.x == kScanThreads - 1)
+  if (threadIdx.x == kScanThreads - 1) {
     out[n] = run;
+    unsigned long long m = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w)
+      m = warp_max[w] > m ? warp_max[w] : m;
+    out[n + 1] = m;
+  }
 }
 
-__global__ void __launch_bounds__(kThreads) k_csv_write(Source s, const unsigned long long* __restrict__ tile_off,
+// Writes tiles tile0 + blockIdx.x; their text goes to text + (tile_off[t] -
+// base).  The dynamic shared memory is write_smem(longest tile): the text
+// region first (text_region bytes), then offsets and queue.
+__global__ void __launch_bounds__(kThreads, 4) k_csv_write(Source s, const unsigned long long* __restrict__ tile_off,
+                                                        long long tile0, unsigned long long base, uint32_t text_region,
                                                         char* __restrict__ text)
 {
-  extern __shared__ __align__(16) unsigned char sbuf[];
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* sbuf = smem;                                         // text_region bytes
+  uint16_t* off = reinterpret_cast<uint16_t*>(smem + text_region);    // per entry: length, then offset
+  uint16_t* queue = off + kTile;
+  __shared__ uint32_t qn;
   __shared__ uint32_t warp_sum[kThreads / 32];
+  const long long tile = tile0 + blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long t0 = (long long)blockIdx.x * kTile;
-  const long long g0 = s.e0 + t0;
-  const int r0 = (int)(g0 / s.n), c0 = (int)(g0 - (long long)r0 * s.n);
-  char* dst = text + tile_off[blockIdx.x];
-  const uint32_t shift = (uint32_t)((uintptr_t)dst & 15u);
-  uint32_t run = shift;  // next free byte of sbuf
-  char buf[kMaxEntry];
-  for (int k = 0; k < kPerThread; ++k) {
-    const int o = k * kThreads + (int)threadIdx.x;
-    uint32_t len = 0;
-    if (t0 + o < s.n_entries) {
-      const int cc = c0 + o;
-      const int row = r0 + cc / s.n, col = cc % s.n;
-      len = (uint32_t)format_g6(entry_value(s, g0 + o, row), buf);
-      buf[len++] = col == s.n - 1 ? '\n' : ';';
-    }
-    uint32_t incl = len;
-    for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-      if (lane >= off)
-        incl += y;
-    }
-    if (lane == 31)
-      warp_sum[warp] = incl;
-    __syncthreads();
-    uint32_t before = 0, total = 0;
-    for (int w = 0; w < kThreads / 32; ++w) {
-      const uint32_t u = warp_sum[w];
-      before += w < warp ? u : 0u;
-      total += u;
-    }
-    const uint32_t pos = run + before + incl - len;
-    for (uint32_t i = 0; i < len; ++i)
-      sbuf[pos + i] = (unsigned char)buf[i];
-    run += total;
-    __syncthreads();
+  if (threadIdx.x == 0)
+    qn = 0;
+  for (int o = threadIdx.x; o < kTile; o += kThreads)
+    off[o] = 0;  // entries past the matrix end
+  __syncthreads();
+  // 1. lengths: zeros directly, the others through the queue
+  TileRegs r;
+  load_tile(s, tile, r);
+  walk_tile(s, tile, r, [&](int o, bool valid, float v, int) {
+    const bool zero = __float_as_uint(v) == 0u;
+    if (valid && zero)
+      off[o] = 2;
+    enqueue(queue, &qn, valid && !zero, o);
+  });
+  __syncthreads();
+  const uint32_t n_q = qn;
+  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+    const int o = queue[q];
+    int col;
+    off[o] = (uint16_t)(format_g6_len(tile_value(s, tile, o, &col)) + 1);
   }
-  // copy [shift, run) of sbuf to dst: ragged head, 16-byte body, ragged tail
-  const uint32_t L = run - shift;
+  __syncthreads();
+  // 2. offsets: thread t scans entries [16t, 16t + 16)
+  char* dst = text + (tile_off[tile] - base);
+  const uint32_t shift = (uint32_t)((uintptr_t)dst & 15u);
+  uint32_t mine = 0;
+  for (int i = 0; i < kPerThread; ++i)
+    mine += off[threadIdx.x * kPerThread + i];
+  uint32_t incl = mine;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= d)
+      incl += y;
+  }
+  if (lane == 31)
+    warp_sum[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+  for (int w = 0; w < kThreads / 32; ++w) {
+    const uint32_t u = warp_sum[w];
+    before += w < warp ? u : 0u;
+    total += u;
+  }
+  uint32_t run = shift + before + incl - mine;
+  for (int i = 0; i < kPerThread; ++i) {
+    const int o = threadIdx.x * kPerThread + i;
+    const uint32_t len = off[o];
+    off[o] = (uint16_t)run;  // below 64 KB
+    run += len;
+  }
+  __syncthreads();
+  // 3. text: zeros, then the queued entries
+  walk_tile(s, tile, r, [&](int o, bool valid, float v, int col) {
+    if (valid && __float_as_uint(v) == 0u) {
+      sbuf[off[o]] = '0';
+      sbuf[off[o] + 1] = col == s.n - 1 ? '\n' : ';';
+    }
+  });
+  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+    const int o = queue[q];
+    int col;
+    const float v = tile_value(s, tile, o, &col);
+    PtrOut w{reinterpret_cast<char*>(sbuf + off[o]), 0};
+    format_g6_to(v, w);
+    w.put(col == s.n - 1 ? '\n' : ';');
+  }
+  __syncthreads();
+  // 4. copy [shift, shift + total) of sbuf to dst
+  const uint32_t L = total;
   const uint32_t head = min(L, (16u - shift) & 15u);
   const uint32_t body = (L - head) >> 4;
   for (uint32_t i = threadIdx.x; i < head; i += kThreads)

@@ -584,3 +584,22 @@ int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells
 }
 
 }  // namespace b200_form_factors
+
+// ===========================================================================
+// CSV export
+// ===========================================================================
+namespace b200_csv_export {
+
+int export_csv(const char* filename, form_factors::scene_t* scene, form_factors::task_t* task)
+{
+  if (!filename || !scene || !task || scene->n_meshes < 0 || (scene->n_meshes && !task->form_factors))
+    return FFB_ERR_ARG;
+  ffb_ctx* ctx = nullptr;
+  int rc = ffb_ctx_create(device_from_env(), &ctx);
+  if (rc == FFB_OK)
+    rc = ffb_csv_export(ctx, filename, task->form_factors, scene->n_meshes);
+  ffb_ctx_destroy(ctx);
+  return rc == FFB_ERR_FILE ? -CSV_EXPORT_FILE_ERROR : rc;
+}
+
+}  // namespace b200_csv_export

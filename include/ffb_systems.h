@@ -27,6 +27,7 @@
 #include "emission/system.h"
 #include "emission/malley_emission.h"
 #include "form_factors/system.h"
+#include "import_export/csv_export.h"
 #else
 
 namespace math {
@@ -132,6 +133,10 @@ struct system_methods_t {
 };
 }  // namespace form_factors
 
+/* import_export/csv_export.h:27-28 */
+#define CSV_EXPORT_OK 0
+#define CSV_EXPORT_FILE_ERROR 31
+
 #endif  // FFB_USE_REFERENCE_HEADERS
 
 /* Type IDs beside the reference's (ray_caster/system.h:106-109,
@@ -188,5 +193,15 @@ int set_seed(form_factors::system_t* system, uint64_t seed);
 int set_flags(form_factors::system_t* system, int flags);
 int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells_per_face);
 }  // namespace b200_form_factors
+
+namespace b200_csv_export {
+/* csv_export::export_csv (import_export/csv_export.cpp:26-46) with the text
+ * formatted on the GPU: the same file, byte for byte, for the n_meshes x
+ * n_meshes matrix task->form_factors (host memory).  Returns CSV_EXPORT_OK,
+ * -CSV_EXPORT_FILE_ERROR when the file cannot be opened or written (as the
+ * reference), or a negative FFB_ERR_* code of include/ffb.h for a device
+ * failure.  Each call uses its own context on device FFB_DEVICE (default 0). */
+int export_csv(const char* filename, form_factors::scene_t* scene, form_factors::task_t* task);
+}  // namespace b200_csv_export
 
 #endif /* FFB_SYSTEMS_H */

@@ -392,8 +392,51 @@ static void emission_suite()
   b200_ray_caster::destroy(r);
 }
 
+// CSV export (import_export/csv_export.cpp:26-46): the B200 export writes
+// the reference's bytes; with the reference built in, the two files are
+// compared whole.
+static std::string read_file(const char* path)
+{
+  std::string out;
+  FILE* f = std::fopen(path, "rb");
+  if (!f)
+    return out;
+  char buf[4096];
+  size_t k;
+  while ((k = std::fread(buf, 1, sizeof buf, f)) > 0)
+    out.append(buf, k);
+  std::fclose(f);
+  return out;
+}
+
+static void csv_suite()
+{
+  g_case = "B200 csv export";
+  float ff[9] = {0.5f, 0.25f, 0.f, 1.f, 1e-5f, 1.f / 3.f, 123456.7f, -0.f, 2.f};
+  form_factors::scene_t scene = {0, 0, 3, 0};
+  form_factors::task_t task = {0, ff};
+  const char* path = "test_systems_b200.csv";
+  CHECK(b200_csv_export::export_csv(path, &scene, &task) == CSV_EXPORT_OK);
+  CHECK(read_file(path) == "0.5;0.25;0\n1;1e-05;0.333333\n123457;-0;2\n");
+  CHECK(b200_csv_export::export_csv("no_such_dir/x.csv", &scene, &task) == -CSV_EXPORT_FILE_ERROR);
+#ifdef FFB_WITH_REFERENCE
+  std::vector<float> big(257 * 257);
+  for (size_t i = 0; i < big.size(); ++i)
+    big[i] = (float)((i * 2654435761u) % 10007u) * (1.f / (float)(1 + i % 977u));
+  form_factors::scene_t s2 = {0, 0, 257, 0};
+  form_factors::task_t t2 = {0, big.data()};
+  CHECK(csv_export::export_csv("test_systems_ref.csv", &s2, &t2) == CSV_EXPORT_OK);
+  CHECK(b200_csv_export::export_csv(path, &s2, &t2) == CSV_EXPORT_OK);
+  CHECK(read_file(path) == read_file("test_systems_ref.csv"));
+  CHECK(csv_export::export_csv("no_such_dir/x.csv", &s2, &t2) == -CSV_EXPORT_FILE_ERROR);
+  std::remove("test_systems_ref.csv");
+#endif
+  std::remove(path);
+}
+
 int main()
 {
+  csv_suite();
   for (const Caster& c : casters())
     ray_caster_suite(c);
   emission_suite();
