@@ -102,6 +102,7 @@ struct ffb_ctx {
   // per-call scratch
   DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
+  DevBuf power_tab, absorb;                     // radiance sink
   void* csv_pinned[2] = {nullptr, nullptr};     // double-buffered text on its way to a file
   size_t csv_pinned_cap[2] = {0, 0};
   void* pinned = nullptr;
@@ -491,6 +492,12 @@ int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, int n_scenes, bool t
     kern = hash ? k_form_factors<kSkip, kScenes, true, true> : k_form_factors<kSkip, kScenes, true, false>;
   else
     kern = hash ? k_form_factors<kSkip, kScenes, false, true> : k_form_factors<kSkip, kScenes, false, false>;
+  if constexpr (kScenes == 1) {
+    if (p.power) {  // radiance sink: no matrix, no histogram
+      kern = p.stats ? k_form_factors<kSkip, 1, true, false, true> : k_form_factors<kSkip, 1, false, false, true>;
+      hash = false;
+    }
+  }
   const size_t smem = hash ? kHashSmem : 0;
   int per_sm = 0;
   FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, smem));
@@ -558,7 +565,8 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   DevBuf* bufs[] = {&c->frames,   &c->batch_frames, &c->batch_chunks, &c->batch_keys, &c->batch_epoch,
                     &c->scan_sums, &c->chunks,      &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
-                    &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text};
+                    &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
+                    &c->power_tab, &c->absorb};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
@@ -842,6 +850,8 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     p.scene_keys = nullptr;
     p.chunk_cursor = dptr<uint32_t>(c->cursor);
     p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
+    p.power = nullptr;
+    p.absorb = nullptr;
     p.scenes[0].g = make_view(s);
     // the kernel adds at row * n_rows + col; the block holds rows from
     // row_begin, so its base is moved back by row_begin rows (only rows of
@@ -904,6 +914,175 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   FFB_TRY(ffb_form_factor_counts(c, front, rear, seed, epoch, flags, face_to_row, n_rows,
                                  dptr<uint32_t>(c->ff_counts)));
   return ffb_normalise(c, dptr<uint32_t>(c->ff_counts), outgoing, n_rows, ff);
+}
+
+// ===========================================================================
+// Radiance equation step (thermal_equation/radiance_cpu.cpp:96-190)
+// ===========================================================================
+extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const int32_t* rear, const float* power_front,
+                                       const float* power_rear, const int32_t* face_to_mesh, int n_meshes,
+                                       uint64_t seed, uint32_t epoch, int flags, double* absorption)
+{
+  FFB_TRY(check_ctx(c));
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!s.grid_ok)
+    return fail(FFB_ERR_NO_GRID, "radiance before ffb_grid_build");
+  long long total = 0;
+  FFB_TRY(check_counts(s.n_faces, front, rear, &total));
+  if (!power_front || !power_rear || !face_to_mesh || !absorption || n_meshes <= 0)
+    return fail(FFB_ERR_ARG, "bad radiance arguments");
+  for (int f = 0; f < s.n_faces; ++f)
+    if (face_to_mesh[f] < 0 || face_to_mesh[f] >= n_meshes)
+      return fail(FFB_ERR_ARG, "face_to_mesh[%d] = %d outside [0, %d)", f, face_to_mesh[f], n_meshes);
+  // 64-bit fixed point with 2^scale_exp units per watt, the largest power of
+  // two that keeps the sum of all rays' powers below 2^62
+  double bound = 0.0;
+  for (int f = 0; f < s.n_faces; ++f) {
+    if (!std::isfinite(power_front[f]) || !std::isfinite(power_rear[f]))
+      return fail(FFB_ERR_ARG, "non-finite ray power at face %d", f);
+    bound += (double)front[f] * std::fabs((double)power_front[f]) + (double)rear[f] * std::fabs((double)power_rear[f]);
+  }
+  int scale_exp = 0;
+  if (bound > 0.0)
+    scale_exp = std::min(1000, (int)std::floor(62.0 - std::log2(bound)));
+  std::vector<long long> fixed(2 * (size_t)s.n_faces);
+  for (int f = 0; f < s.n_faces; ++f) {
+    fixed[2 * (size_t)f] = std::llround(std::ldexp((double)power_front[f], scale_exp));
+    fixed[2 * (size_t)f + 1] = std::llround(std::ldexp((double)power_rear[f], scale_exp));
+  }
+  FFB_TRY(ensure_frames(c, flags));
+  std::vector<Chunk> chunks;
+  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
+  add_chunks(chunks, front, rear, s.n_faces, 0);
+  FFB_TRY(ensure(c, c->absorb, sizeof(unsigned long long) * (size_t)n_meshes));
+  FFB_CUDA(cudaMemsetAsync(c->absorb.ptr, 0, sizeof(unsigned long long) * (size_t)n_meshes, c->stream));
+  FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
+  FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
+  if (!chunks.empty()) {
+    FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
+    FFB_TRY(upload(c, c->power_tab, fixed.data(), sizeof(long long) * fixed.size()));
+    FFB_TRY(upload(c, c->rows, face_to_mesh, sizeof(int32_t) * (size_t)s.n_faces));
+    FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
+    FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
+    TraceParams<1> p;
+    p.frames = dptr<float>(c->frames);
+    p.chunks = dptr<Chunk>(c->chunks);
+    p.n_chunks = (int)chunks.size();
+    p.key0 = (uint32_t)seed;
+    p.key1 = (uint32_t)(seed >> 32);
+    p.epoch = epoch;
+    p.epoch_ptr = nullptr;
+    p.scene_keys = nullptr;
+    p.chunk_cursor = dptr<uint32_t>(c->cursor);
+    p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
+    p.power = dptr<unsigned long long>(c->power_tab);
+    p.absorb = dptr<unsigned long long>(c->absorb);
+    p.scenes[0].g = make_view(s);
+    p.scenes[0].counts = nullptr;
+    p.scenes[0].face_to_row = dptr<int32_t>(c->rows);
+    p.scenes[0].face_base = 0;
+    p.scenes[0].n_cols = n_meshes;
+    if (s.info.skip_empty)
+      FFB_TRY((launch_fused<true, 1>(c, p, 1, true)));
+    else
+      FFB_TRY((launch_fused<false, 1>(c, p, 1, true)));
+  }
+  std::vector<long long> sums((size_t)n_meshes);
+  FFB_CUDA(cudaMemcpyAsync(sums.data(), c->absorb.ptr, sizeof(long long) * sums.size(), cudaMemcpyDeviceToHost,
+                           c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  for (int m = 0; m < n_meshes; ++m)
+    absorption[m] = std::ldexp((double)sums[(size_t)m], -scale_exp);
+  return FFB_OK;
+}
+
+// ===========================================================================
+// Parallel rays from a disc (emission/parallel_rays_cpu.cpp:88-106,
+// thermal_equation/parallel_rays_cpu.cpp:92-131)
+// ===========================================================================
+namespace {
+
+int disc_source(const ffb_disc_source* src, DiscSource* out)
+{
+  if (!src)
+    return fail(FFB_ERR_ARG, "null source");
+  *out = make_disc_source(f3(src->direction[0], src->direction[1], src->direction[2]),
+                          f3(src->center[0], src->center[1], src->center[2]), src->distance, src->radius);
+  return FFB_OK;
+}
+
+}  // namespace
+
+extern "C" int ffb_emit_parallel(ffb_ctx* c, const ffb_disc_source* src, long long n_rays, uint64_t seed,
+                                 uint32_t epoch, float* rays6)
+{
+  FFB_TRY(check_ctx(c));
+  if (n_rays < 0 || (n_rays && !rays6))
+    return fail(FFB_ERR_ARG, "bad parallel emission arguments");
+  DiscSource d;
+  FFB_TRY(disc_source(src, &d));
+  void* d_rays;
+  bool host_out;
+  FFB_TRY(output_ptr(c, rays6, sizeof(float) * 6 * (size_t)n_rays, c->tmp_out, &d_rays, &host_out));
+  if (n_rays) {
+    k_emit_disc<<<grid_blocks(n_rays, 256, c->n_sm * 16), 256, 0, c->stream>>>(
+        d, (unsigned long long)n_rays, (uint32_t)seed, (uint32_t)(seed >> 32), epoch, (float*)d_rays);
+    FFB_CUDA(cudaGetLastError());
+  }
+  if (host_out) {
+    FFB_TRY(finish_output(c, rays6, d_rays, sizeof(float) * 6 * (size_t)n_rays));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return FFB_OK;
+}
+
+extern "C" int ffb_parallel_rays(ffb_ctx* c, const ffb_disc_source* src, long long n_rays, uint64_t seed,
+                                 uint32_t epoch, uint32_t* side_counts)
+{
+  FFB_TRY(check_ctx(c));
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!s.grid_ok)
+    return fail(FFB_ERR_NO_GRID, "parallel rays before ffb_grid_build");
+  if (n_rays < 0 || !side_counts)
+    return fail(FFB_ERR_ARG, "bad parallel-ray arguments");
+  DiscSource d;
+  FFB_TRY(disc_source(src, &d));
+  const size_t bytes = sizeof(uint32_t) * 2 * (size_t)s.n_faces;
+  void* d_counts;
+  bool host_out;
+  FFB_TRY(output_ptr(c, side_counts, bytes, c->tmp_out, &d_counts, &host_out));
+  FFB_CUDA(cudaMemsetAsync(d_counts, 0, bytes, c->stream));
+  FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
+  FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
+  FFB_TRY(ensure(c, c->ray_cursor, sizeof(unsigned long long)));
+  FFB_CUDA(cudaMemsetAsync(c->ray_cursor.ptr, 0, sizeof(unsigned long long), c->stream));
+  if (n_rays) {
+    const GridView g = make_view(s);
+    const bool stats = c->stats_on;
+    auto kern = s.info.skip_empty ? (stats ? k_parallel_rays<true, true> : k_parallel_rays<true, false>)
+                                  : (stats ? k_parallel_rays<false, true> : k_parallel_rays<false, false>);
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceThreads, 0));
+    const long long wave = (long long)std::max(per_sm, 1) * c->n_sm;
+    const long long by_work = (n_rays + kTraceThreads - 1) / kTraceThreads;
+    const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
+    timing_begin(c);
+    kern<<<blocks, kTraceThreads, 0, c->stream>>>(g, d, dptr<float>(s.faces), (unsigned long long)n_rays,
+                                                  (uint32_t)seed, (uint32_t)(seed >> 32), epoch, (uint32_t*)d_counts,
+                                                  dptr<unsigned long long>(c->ray_cursor),
+                                                  dptr<unsigned long long>(c->stats));
+    timing_end(c);
+    FFB_CUDA(cudaGetLastError());
+  }
+  if (host_out) {
+    FFB_TRY(finish_output(c, side_counts, d_counts, bytes));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return FFB_OK;
 }
 
 // ===========================================================================
@@ -1205,6 +1384,8 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
   p.scene_keys = dptr<uint2>(c->batch_keys);
   p.chunk_cursor = dptr<uint32_t>(c->cursor);
   p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
+  p.power = nullptr;
+  p.absorb = nullptr;
   // all scenes share one kernel variant: empty-space jumps need every
   // scene's distance map
   bool skip = true;

@@ -199,7 +199,7 @@ struct FaceFrame {
   float v[20];
 };
 
-__device__ inline void rotate_towards(float3 s, float3 t, float* m)
+__host__ __device__ inline void rotate_towards(float3 s, float3 t, float* m)
 {
   float3 v = cross3(s, t);
   float s2 = dot3(v, v);
@@ -267,6 +267,51 @@ __device__ __forceinline__ void emit_ray(const float* __restrict__ fr, uint32_t 
                 (m[2] * mv.x + m[5] * mv.y) + m[8] * mv.z);
   o = add3(origin, mul3(d, 0.0001f));
   e = add3(origin, d);
+}
+
+// ---------------------------------------------------------------------------
+// Parallel rays from a disc (a distant source such as the Sun,
+// emission/parallel_rays_cpu.cpp:88-106): a point uniform on the disc of
+// `radius` in the plane z = -distance of the source frame, rotated by the
+// rotation of +z towards `direction` and moved to `center`; the ray's end
+// point is origin + direction * 0.1 (the reference's ray_t holds an end
+// point).  Draws are Philox keyed by (seed, epoch, ray index).
+// ---------------------------------------------------------------------------
+struct DiscSource {
+  float m[9];     // rotate_towards(+z, direction), row-major
+  float3 center;
+  float3 direction;
+  float distance;
+  float radius;
+};
+
+__host__ __device__ inline DiscSource make_disc_source(float3 direction, float3 center, float distance, float radius)
+{
+  DiscSource d;
+  rotate_towards(f3(0.f, 0.f, 1.f), direction, d.m);
+  d.center = center;
+  d.direction = direction;
+  d.distance = distance;
+  d.radius = radius;
+  return d;
+}
+
+constexpr uint32_t kDiscTag = 0x50415241u;  // Philox counter word distinguishing disc rays from face rays
+
+__host__ __device__ inline void emit_disc_ray(const DiscSource& d, unsigned long long j, uint32_t key0, uint32_t key1,
+                                              uint32_t epoch, float3& o, float3& e)
+{
+  const uint4 x = philox4x32_10(make_uint4((uint32_t)j, (uint32_t)(j >> 32), epoch, kDiscTag), key0, key1);
+  const float rad = d.radius * sqrtf(u01(x.x));
+  float st, ct;
+  sincos_turn24(x.y >> 8, st, ct);
+  const float px = rad * ct, py = rad * st, pz = -d.distance;
+  // mat33 * vec3 (math/mat.h:30-37): column j of the row-major m times the vector
+  const float3 v = f3((d.m[0] * px + d.m[3] * py) + d.m[6] * pz,
+                      (d.m[1] * px + d.m[4] * py) + d.m[7] * pz,
+                      (d.m[2] * px + d.m[5] * py) + d.m[8] * pz);
+  o = add3(v, d.center);
+  e = add3(o, mul3(d.direction, 0.1f));
 }
 
 }  // namespace ffb

@@ -44,6 +44,11 @@ struct TraceParams {
   const uint2* __restrict__ scene_keys;      // per-scene Philox key, or null for (key0, key1)
   uint32_t* __restrict__ chunk_cursor;        // work counter, zero before the launch
   unsigned long long* __restrict__ stats;     // kStatSlots, or null
+  // radiance sink (kPower): per-ray power of each (face, side) as 64-bit
+  // fixed point, and the per-mesh absorbed power it adds to (mesh = the
+  // scene's face_to_row of the hit face)
+  const unsigned long long* __restrict__ power;
+  unsigned long long* __restrict__ absorb;
   SceneSlot scenes[kScenes];
 };
 
@@ -138,6 +143,10 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // chunk of another scene is taken only once every lane is idle (drain before
 // switch), so that the scene's grid is warp-uniform.
 //
+// kPower (the radiance equation, thermal_equation/radiance_cpu.cpp:142-180)
+// replaces the matrix: a hit adds the per-ray power of the ray's (source
+// face, side) to the absorbed power of the hit face's mesh, in 64-bit fixed
+// point (integer sums: the same result whatever the order of the hits).
 // kStats adds the test / cell / ray / hit counters (four live registers per
 // lane); without it p.stats is ignored.  kHash selects the warp histogram;
 // without it each hit is one global reduction (red.global.add) into the
@@ -156,7 +165,7 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 #define FFB_TEST_PER_ITER 2
 #endif
 
-template <bool kSkip, int kScenes, bool kStats, bool kHash>
+template <bool kSkip, int kScenes, bool kStats, bool kHash, bool kPower = false>
 __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams<kScenes> p)
 {
   extern __shared__ uint32_t s_hash[];  // kWarpsPerBlock x (keys, values) when kHash
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
         emit_ray(p.frames + 20 * ((size_t)S.face_base + c_face), (uint32_t)c_face, (uint32_t)(c_j + rank), c_front,
                  key0, key1, epoch, o, e);
         ++n_rays;
-        my_row = c_row;
+        my_row = kPower ? 2 * c_face + (c_j + rank >= c_front ? 1 : 0) : c_row;
         active = tracer_begin<kSkip>(T, S.g, o, e, n_cells);
       }
       need &= ~__ballot_sync(kFull, mine);
@@ -269,11 +278,15 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     if (hit >= 0) {
       ++n_hits;
       const int col = S.face_to_row ? __ldg(S.face_to_row + hit) : hit;
-      const uint32_t key = (uint32_t)my_row * (uint32_t)S.n_cols + (uint32_t)col;
-      if (kHash)
-        fresh = warp_hash_add(keys, vals, key, S.counts);
-      else
-        atomicAdd(S.counts + key, 1u);
+      if (kPower) {
+        atomicAdd(p.absorb + col, __ldg(p.power + my_row));
+      } else {
+        const uint32_t key = (uint32_t)my_row * (uint32_t)S.n_cols + (uint32_t)col;
+        if (kHash)
+          fresh = warp_hash_add(keys, vals, key, S.counts);
+        else
+          atomicAdd(S.counts + key, 1u);
+      }
     }
     if (kHash) {
       fill += __popc(__ballot_sync(kFull, fresh));
@@ -287,6 +300,95 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
   if (kStats)
     warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits, n_jumps);
+}
+
+// ---------------------------------------------------------------------------
+// Parallel rays from a disc (a distant source): the thermal_equation
+// parallel_rays_cpu path (thermal_equation/parallel_rays_cpu.cpp:92-131)
+// with emission, trace and the per-face tally fused.  Persistent warps take
+// ray indices from a global cursor (one atomic per refill of at least
+// kRefillMin idle lanes); a hit on face h adds one to side_counts[2h] when
+// the ray meets its front (dot(triangle_normal(h), direction) < 0, as the
+// reference chooses the front absorbance) and to side_counts[2h + 1]
+// otherwise.
+// ---------------------------------------------------------------------------
+template <bool kSkip, bool kStats>
+__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS)
+    k_parallel_rays(GridView g, const __grid_constant__ DiscSource src, const float* __restrict__ faces9,
+                    unsigned long long n_rays, uint32_t key0, uint32_t key1, uint32_t epoch,
+                    uint32_t* __restrict__ side_counts, unsigned long long* __restrict__ cursor,
+                    unsigned long long* __restrict__ stats)
+{
+  const int lane = threadIdx.x & 31;
+  const unsigned lane_below = (1u << lane) - 1u;
+  uint32_t n_tests = 0, n_cells = 0, n_done = 0, n_hits = 0, n_jumps = 0;
+  Tracer T;
+  bool active = false;
+  bool exhausted = false;
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !active);
+    if ((__popc(need) >= kRefillMin || need == kFull) && !exhausted) {
+      unsigned long long base = 0;
+      if (lane == 0)
+        base = atomicAdd(cursor, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= n_rays)
+        exhausted = true;
+      if ((need >> lane) & 1u) {
+        const unsigned long long j = base + __popc(need & lane_below);
+        if (j < n_rays) {
+          float3 o, e;
+          emit_disc_ray(src, j, key0, key1, epoch, o, e);
+          ++n_done;
+          active = tracer_begin<kSkip>(T, g, o, e, n_cells);
+        }
+      }
+    }
+    if (exhausted && !__any_sync(kFull, active))
+      break;
+    if (active) {
+      bool live = true;
+#pragma unroll
+      for (int k = 0; k < FFB_ADV_PER_ITER; ++k)
+        if (live && T.i >= T.en)
+          live = tracer_advance<kSkip>(T, g, n_cells, n_jumps);
+      if (!live) {
+        active = false;
+        const int h = tracer_result(T, g);
+        if (h >= 0) {
+          ++n_hits;
+          // triangle_normal (math/triangle.cpp:114-119), dot with the direction
+          const float* q = faces9 + 9 * (size_t)h;
+          const float3 p0 = f3(__ldg(q + 0), __ldg(q + 1), __ldg(q + 2));
+          const float3 nrm = cross3(sub3(f3(__ldg(q + 3), __ldg(q + 4), __ldg(q + 5)), p0),
+                                    sub3(f3(__ldg(q + 6), __ldg(q + 7), __ldg(q + 8)), p0));
+          const float side = dot3(nrm, src.direction);
+          atomicAdd(side_counts + 2 * (size_t)h + (side < 0.f ? 0 : 1), 1u);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < FFB_TEST_PER_ITER; ++k)
+          if (T.i < T.en)
+            tracer_test(T, g, n_tests);
+      }
+    }
+  }
+  if (kStats)
+    warp_stats(stats, n_tests, n_cells, n_done, n_hits, n_jumps);
+}
+
+// Materialises rays [0, n_rays) of a disc source (parallel_rays_cpu.cpp:88-106).
+__global__ void k_emit_disc(const __grid_constant__ DiscSource src, unsigned long long n_rays, uint32_t key0,
+                            uint32_t key1, uint32_t epoch, float* __restrict__ rays6)
+{
+  for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < n_rays;
+       j += (unsigned long long)gridDim.x * blockDim.x) {
+    float3 o, e;
+    emit_disc_ray(src, j, key0, key1, epoch, o, e);
+    float* r = rays6 + 6 * j;
+    r[0] = o.x; r[1] = o.y; r[2] = o.z;
+    r[3] = e.x; r[4] = e.y; r[5] = e.z;
+  }
 }
 
 // Advances the device-resident Philox epoch of a captured launch, so that every

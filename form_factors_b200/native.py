@@ -47,6 +47,48 @@ class Stats(C.Structure):
                 ("hits", C.c_ulonglong), ("kernel_ms", C.c_float), ("jumps", C.c_ulonglong)]
 
 
+class DiscSource(C.Structure):
+    """ffb_disc_source: the fields of parallel_rays_emission_cpu::task_t."""
+    _fields_ = [("direction", C.c_float * 3), ("center", C.c_float * 3), ("distance", C.c_float),
+                ("radius", C.c_float)]
+
+    @classmethod
+    def make(cls, direction, center, distance, radius):
+        return cls((C.c_float * 3)(*direction), (C.c_float * 3)(*center), float(distance), float(radius))
+
+
+class Mesh(C.Structure):
+    _fields_ = [("first_idx", C.c_int), ("n_faces", C.c_int), ("material_idx", C.c_int)]
+
+
+class Optics(C.Structure):
+    _fields_ = [("front_emissivity", C.c_float), ("rear_emissivity", C.c_float), ("front_absorbance", C.c_float),
+                ("rear_absorbance", C.c_float)]
+
+
+def _meshes(meshes):
+    arr = (Mesh * len(meshes))()
+    for i, (first, n, mat) in enumerate(meshes):
+        arr[i] = Mesh(int(first), int(n), int(mat))
+    return arr
+
+
+def _optics(materials):
+    arr = (Optics * len(materials))()
+    for i, m in enumerate(materials):
+        arr[i] = Optics(*[float(x) for x in m])
+    return arr
+
+
+def bounding_sphere(faces):
+    """math::triangles_bsphere of a (n, 9) float32 face array: (center, radius)."""
+    faces = np.ascontiguousarray(faces, np.float32)
+    c = (C.c_float * 3)()
+    r = C.c_float()
+    _check(load().ffb_bounding_sphere(_ptr(faces), len(faces), c, C.byref(r)))
+    return np.array(list(c), np.float32), np.float32(r.value)
+
+
 class RequestInfo(C.Structure):
     _fields_ = [("state", C.c_int), ("error", C.c_int), ("n_faces", C.c_int), ("queue_s", C.c_double),
                 ("latency_s", C.c_double), ("gpu_ms", C.c_double)]
@@ -99,6 +141,12 @@ def load(path=LIB_PATH):
         "ffb_csv_export": (i32, [vp, C.c_char_p, vp, i32]),
         "ffb_csv_export_counts": (i32, [vp, C.c_char_p, vp, vp, i32]),
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
+        "ffb_radiance_absorption": (i32, [vp, vp, vp, vp, vp, vp, i32, u64, u32, i32, vp]),
+        "ffb_emit_parallel": (i32, [vp, C.POINTER(DiscSource), i64, u64, u32, vp]),
+        "ffb_parallel_rays": (i32, [vp, C.POINTER(DiscSource), i64, u64, u32, vp]),
+        "ffb_bounding_sphere": (i32, [vp, i32, vp, C.POINTER(C.c_float)]),
+        "ffb_radiance_step": (i32, [vp, vp, i32, vp, i32, vp, i32, vp, i32, u64, u32, i32, vp, vp]),
+        "ffb_distant_source_step": (i32, [vp, vp, i32, vp, i32, vp, i32, i32, C.c_float, vp, u64, u32, vp]),
         "ffb_cast_bruteforce_static": (i32, [vp, i32, vp, i64, vp, vp, vp]),
         "ffb_form_factors": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp, vp]),
         "ffb_form_factor_counts_rows": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, i32, i32, vp]),
@@ -356,6 +404,62 @@ class Context:
             _check(self._lib.ffb_csv_export(self._h, name, _ptr(ff), n))
         else:
             _check(self._lib.ffb_csv_export_counts(self._h, name, _ptr(counts), _ptr(outgoing), n))
+
+    def radiance_absorption(self, front, rear, power_front, power_rear, face_to_mesh, n_meshes, seed, epoch=0,
+                            flags=0):
+        """ffb_radiance_absorption: absorbed power per mesh (float64)."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        pf = np.ascontiguousarray(power_front, np.float32)
+        pr = np.ascontiguousarray(power_rear, np.float32)
+        f2m = np.ascontiguousarray(face_to_mesh, np.int32)
+        out = np.zeros(int(n_meshes), np.float64)
+        _check(self._lib.ffb_radiance_absorption(self._h, _ptr(front), _ptr(rear), _ptr(pf), _ptr(pr), _ptr(f2m),
+                                                 int(n_meshes), int(seed), int(epoch), int(flags), _ptr(out)))
+        return out
+
+    def emit_parallel(self, source, n_rays, seed, epoch=0, out=None):
+        """Rays of a disc source (ffb_emit_parallel), (n_rays, 6) float32."""
+        if out is None:
+            out = np.empty((int(n_rays), 6), np.float32)
+        _check(self._lib.ffb_emit_parallel(self._h, C.byref(source), int(n_rays), int(seed), int(epoch), _ptr(out)))
+        return out
+
+    def parallel_rays(self, source, n_rays, seed, epoch=0, out=None):
+        """Hits of a disc source per (face, side) (ffb_parallel_rays), (n_faces, 2) uint32."""
+        if out is None:
+            out = np.empty((self.n_faces, 2), np.uint32)
+        _check(self._lib.ffb_parallel_rays(self._h, C.byref(source), int(n_rays), int(seed), int(epoch), _ptr(out)))
+        return out
+
+    def radiance_step(self, faces, meshes, materials, temperatures, n_rays, seed, epoch=0, flags=0,
+                      emission=None, absorption=None):
+        """One radiance-equation calculate(): (emission, absorption) per mesh,
+        added to the given float32 arrays (zeros by default).  meshes: (first,
+        count, material) triples; materials: (front emissivity, rear
+        emissivity, front absorbance, rear absorbance)."""
+        faces = np.ascontiguousarray(faces, np.float32)
+        t = np.ascontiguousarray(temperatures, np.float32)
+        n_m = len(meshes)
+        emission = np.zeros(n_m, np.float32) if emission is None else emission
+        absorption = np.zeros(n_m, np.float32) if absorption is None else absorption
+        _check(self._lib.ffb_radiance_step(self._h, _ptr(faces), len(faces), _meshes(meshes), n_m,
+                                           _optics(materials), len(materials), _ptr(t), int(n_rays), int(seed),
+                                           int(epoch), int(flags), _ptr(emission), _ptr(absorption)))
+        return emission, absorption
+
+    def distant_source_step(self, faces, meshes, materials, n_rays, power, direction, seed, epoch=0,
+                            absorption=None):
+        """One distant-source calculate(): absorbed power per mesh added to
+        `absorption` (zeros by default)."""
+        faces = np.ascontiguousarray(faces, np.float32)
+        d = np.ascontiguousarray(direction, np.float32)
+        n_m = len(meshes)
+        absorption = np.zeros(n_m, np.float32) if absorption is None else absorption
+        _check(self._lib.ffb_distant_source_step(self._h, _ptr(faces), len(faces), _meshes(meshes), n_m,
+                                                 _optics(materials), len(materials), int(n_rays), float(power),
+                                                 _ptr(d), int(seed), int(epoch), _ptr(absorption)))
+        return absorption
 
     def form_factors(self, front, rear, seed, epoch=0, flags=0, face_to_row=None, n_rows=None, outgoing=None,
                      out=None):

@@ -150,7 +150,8 @@ def _orient_inward(faces, center):
 
 def clutter(n_tris=2000, edge=0.05, seed=1, enclosure_cells=13):
     """n_tris random equilateral triangles (centres uniform in the unit cube,
-    uniform orientation) inside a unit-cube enclosure with inward normals."""
+    uniform orientation) inside a unit-cube enclosure with inward normals
+    (enclosure_cells = 0: no enclosure)."""
     rng = np.random.default_rng(seed)
     r = edge / math.sqrt(3.0)
     ang = np.array([0, 2 * math.pi / 3, 4 * math.pi / 3])
@@ -161,6 +162,8 @@ def clutter(n_tris=2000, edge=0.05, seed=1, enclosure_cells=13):
     centers = r + centers * (1 - 2 * r)
     pts = np.einsum("nij,kj->nki", R, local) + centers[:, None, :]
     tris = pts.reshape(-1, 9).astype(np.float32)
+    if enclosure_cells <= 0:
+        return tris
     return np.concatenate([tris, unit_cube_enclosure(enclosure_cells)])
 
 

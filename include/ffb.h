@@ -220,6 +220,78 @@ int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts
 int ffb_server_release(ffb_server* server, long long request_id);
 int ffb_server_stats(ffb_server* server, ffb_server_info* out);
 
+/* One step of the radiance equation (thermal_equation/radiance_cpu.cpp:96-190)
+ * on the resident scene and grid: every face emits front[f] + rear[f] Malley
+ * rays (seed, epoch, flags as ffb_form_factor_counts); a ray of face f that
+ * hits face h adds power_front[f] (front rays) or power_rear[f] (rear rays)
+ * to absorption[face_to_mesh[h]] (host arrays, n_faces and n_meshes long).
+ * The sums are exact integer sums of the powers rounded to a fixed point of
+ * 2^k units per watt, k the largest that keeps the total of every ray's power
+ * below 2^62; absorption[] is set (not added to).  The caller computes the
+ * ray counts and per-ray powers as the reference does (calculate_weights,
+ * emitted_front/rear, front_emission / face_rays_front). */
+int ffb_radiance_absorption(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, const float* power_front,
+                            const float* power_rear, const int32_t* face_to_mesh, int n_meshes, uint64_t seed,
+                            uint32_t epoch, int flags, double* absorption);
+
+/* A disc of parallel rays (a distant source; the fields of
+ * parallel_rays_emission_cpu::task_t, emission/parallel_rays_cpu.h:27-33). */
+typedef struct {
+  float direction[3]; /* ray direction (the reference does not normalise it) */
+  float center[3];    /* the point the disc's axis passes through */
+  float distance;     /* the disc lies at -distance along direction from center */
+  float radius;       /* disc radius */
+} ffb_disc_source;
+
+/* Rays [0, n_rays) of the disc (emission/parallel_rays_cpu.cpp:88-106):
+ * origin uniform on the disc, end point origin + 0.1 * direction, Philox
+ * draws keyed by (seed, epoch, ray index).  rays6 host or device. */
+int ffb_emit_parallel(ffb_ctx* ctx, const ffb_disc_source* src, long long n_rays, uint64_t seed, uint32_t epoch,
+                      float* rays6);
+/* The same rays cast through the resident grid, tallied per hit face and
+ * side (the loop of thermal_equation/parallel_rays_cpu.cpp:110-122, fused):
+ * side_counts[2h] counts rays meeting face h from its front
+ * (dot(triangle_normal(h), direction) < 0), side_counts[2h + 1] the others.
+ * side_counts is host or device, 2 * n_faces entries. */
+int ffb_parallel_rays(ffb_ctx* ctx, const ffb_disc_source* src, long long n_rays, uint64_t seed, uint32_t epoch,
+                      uint32_t* side_counts);
+
+/* A mesh (subject::mesh_t, subject/system.h:64-69) and the optical
+ * properties the ray-traced thermal equations read from its material
+ * (subject::material_t front / rear, subject/system.h:41-59). */
+typedef struct {
+  int first_idx;
+  int n_faces;
+  int material_idx;
+} ffb_mesh;
+typedef struct {
+  float front_emissivity, rear_emissivity;
+  float front_absorbance, rear_absorbance;
+} ffb_optics;
+
+/* math::triangles_bsphere (math/triangle.cpp:361-384), host arithmetic op for
+ * op (including the radius loop starting at the second triangle). */
+int ffb_bounding_sphere(const float* faces9, int n_faces, float* center3, float* radius);
+
+/* One calculate() of the radiance equation (thermal_equation/radiance_cpu.cpp
+ * :96-190) on the resident scene and grid (faces9 / n_faces: the same scene
+ * on the host, for areas).  Weights, ray budgets (n_rays), emission and
+ * per-ray powers follow the reference in float; the rays run through
+ * ffb_radiance_absorption.  emission[m] and absorption[m] are ADDED to, as the
+ * reference's thermal_equation::task_t asks.  Meshes must cover every face
+ * exactly once; FFB_ERR_ARG otherwise. */
+int ffb_radiance_step(ffb_ctx* ctx, const float* faces9, int n_faces, const ffb_mesh* meshes, int n_meshes,
+                      const ffb_optics* materials, int n_materials, const float* temperatures, int n_rays,
+                      uint64_t seed, uint32_t epoch, int flags, float* emission, float* absorption);
+/* One calculate() of the distant-source equation (thermal_equation/
+ * parallel_rays_cpu.cpp:92-131): a disc of n_rays parallel rays of radius
+ * 1.1 * bounding radius, 1.1 + radius in front of the bounding sphere's
+ * centre along `direction`; each hit adds absorbance(side) * ray_power to its
+ * mesh, ray_power = power * pi * radius^2 / n_rays.  absorption[m] is ADDED to. */
+int ffb_distant_source_step(ffb_ctx* ctx, const float* faces9, int n_faces, const ffb_mesh* meshes, int n_meshes,
+                            const ffb_optics* materials, int n_materials, int n_rays, float power,
+                            const float* direction3, uint64_t seed, uint32_t epoch, float* absorption);
+
 /* CSV text of an n x n form-factor matrix, byte for byte the file of
  * csv_export::export_csv (import_export/csv_export.cpp:26-46): row i is the n
  * entries of matrix row i as `std::ostream << float` prints them ("%g",

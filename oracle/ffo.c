@@ -411,6 +411,151 @@ void ffo_form_factor_counts(int n_faces, const float* faces9, const int32_t* fro
 }
 
 /* ------------------------------------------------------------------ */
+/* Parallel rays from a disc (emission/parallel_rays_cpu.cpp:88-106):     */
+/* disc17 = rotation m9 (rotate_towards(+z, direction)), center3,        */
+/* direction3, distance, radius.  Draws: Philox keyed by (seed, epoch,   */
+/* ray index) -- u for the radius (radius * sqrt(u)), a 24-bit turn for   */
+/* the angle.  origin = m * (x, y, -distance) + center, end = origin +    */
+/* direction * 0.1.                                                       */
+/* ------------------------------------------------------------------ */
+void ffo_disc_source(const float* direction3, const float* center3, float distance, float radius, float* disc17)
+{
+  const float z[3] = {0, 0, 1};
+  ffo_rotate_towards(z, direction3, disc17);
+  memcpy(disc17 + 9, center3, 3 * sizeof(float));
+  memcpy(disc17 + 12, direction3, 3 * sizeof(float));
+  disc17[15] = distance;
+  disc17[16] = radius;
+}
+
+void ffo_emit_disc_ray(const float* disc17, uint64_t j, uint64_t seed, uint32_t epoch, float* ray6)
+{
+  uint32_t ctr[4] = {(uint32_t)j, (uint32_t)(j >> 32), epoch, 0x50415241u};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t x[4];
+  ffo_philox4x32_10(ctr, key, x);
+  float rad = disc17[16] * sqrtf(u01(x[0]));
+  float st, ct;
+  ffo_sincos_turn24(x[1] >> 8, &st, &ct);
+  v3 v = mat_vec(disc17, mk(rad * ct, rad * st, -disc17[15]));
+  v3 o = add(v, ld(disc17 + 9));
+  v3 e = add(o, scl(ld(disc17 + 12), 0.1f));
+  ray6[0] = o.x; ray6[1] = o.y; ray6[2] = o.z;
+  ray6[3] = e.x; ray6[4] = e.y; ray6[5] = e.z;
+}
+
+void ffo_emit_parallel(const float* disc17, long n_rays, uint64_t seed, uint32_t epoch, float* rays6)
+{
+  for (long j = 0; j < n_rays; ++j)
+    ffo_emit_disc_ray(disc17, (uint64_t)j, seed, epoch, rays6 + 6 * j);
+}
+
+/* Emission + brute-force cast + per-(hit face, side) tally of
+ * thermal_equation/parallel_rays_cpu.cpp:110-122: side_counts[2h] counts
+ * rays with dot(triangle_normal(h), direction) < 0 (the reference's front),
+ * side_counts[2h + 1] the others.  Zeroed here. */
+typedef struct {
+  int n_faces;
+  const float* faces9;
+  const float* disc;
+  uint64_t seed;
+  uint32_t epoch;
+  long n_rays;
+  uint32_t* side_counts;
+} par_ctx_t;
+
+static void par_body(long chunk, void* arg)
+{
+  par_ctx_t* c = (par_ctx_t*)arg;
+  long b = chunk * 256, e = b + 256 < c->n_rays ? b + 256 : c->n_rays;
+  for (long j = b; j < e; ++j) {
+    float ray[6];
+    int32_t h;
+    ffo_emit_disc_ray(c->disc, (uint64_t)j, c->seed, c->epoch, ray);
+    cast_one(c->n_faces, c->faces9, ray, &h, 0);
+    if (h < 0)
+      continue;
+    const float* t = c->faces9 + 9 * (size_t)h;
+    v3 p0 = ld(t);
+    v3 n = cross(sub(ld(t + 3), p0), sub(ld(t + 6), p0)); /* math/triangle.cpp:114-119 */
+    float side = dot(n, ld(c->disc + 12));
+    __atomic_fetch_add(c->side_counts + 2 * (size_t)h + (side < 0 ? 0 : 1), 1u, __ATOMIC_RELAXED);
+  }
+}
+
+void ffo_parallel_rays(int n_faces, const float* faces9, const float* disc17, long n_rays, uint64_t seed,
+                       uint32_t epoch, uint32_t* side_counts)
+{
+  memset(side_counts, 0, sizeof(uint32_t) * 2 * (size_t)n_faces);
+  par_ctx_t c = {n_faces, faces9, disc17, seed, epoch, n_rays, side_counts};
+  parallel_for((n_rays + 255) / 256, 1, par_body, &c);
+}
+
+/* ------------------------------------------------------------------ */
+/* Radiance equation step (thermal_equation/radiance_cpu.cpp:142-180):    */
+/* a ray of face f that hits face h adds the per-ray power of f's side    */
+/* to absorption[face_to_mesh[h]].  The sums are integers: each power is  */
+/* rounded to 2^k units per watt, k the largest that keeps the sum of all */
+/* rays' |power| below 2^62 (the fixed point of the CUDA path, so the     */
+/* results compare exactly).                                              */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int n_faces;
+  const float* faces9;
+  const int32_t *front, *rear;
+  const long long* fixed;
+  const int32_t* face_to_mesh;
+  uint64_t seed;
+  uint32_t epoch;
+  int flags;
+  long long* sums;
+} rad_ctx_t;
+
+static void rad_body(long f, void* arg)
+{
+  rad_ctx_t* c = (rad_ctx_t*)arg;
+  float frame[18];
+  ffo_face_frame(c->faces9 + 9 * (size_t)f, c->flags, frame);
+  int nf = c->front[f] + c->rear[f];
+  for (int j = 0; j < nf; ++j) {
+    float ray[6];
+    int32_t h;
+    ffo_emit_ray(frame, (uint32_t)f, (uint32_t)j, c->front[f], c->seed, c->epoch, ray);
+    cast_one(c->n_faces, c->faces9, ray, &h, 0);
+    if (h >= 0)
+      __atomic_fetch_add(c->sums + c->face_to_mesh[h], c->fixed[2 * (size_t)f + (j < c->front[f] ? 0 : 1)],
+                         __ATOMIC_RELAXED);
+  }
+}
+
+void ffo_radiance_absorption(int n_faces, const float* faces9, const int32_t* front, const int32_t* rear,
+                             const float* power_front, const float* power_rear, const int32_t* face_to_mesh,
+                             int n_meshes, uint64_t seed, uint32_t epoch, int flags, double* absorption)
+{
+  double bound = 0.0;
+  for (int f = 0; f < n_faces; ++f)
+    bound += (double)front[f] * fabs((double)power_front[f]) + (double)rear[f] * fabs((double)power_rear[f]);
+  int k = 0;
+  if (bound > 0.0) {
+    k = (int)floor(62.0 - log2(bound));
+    if (k > 1000)
+      k = 1000;
+  }
+  long long* fixed = (long long*)malloc(sizeof(long long) * 2 * (size_t)n_faces);
+  long long* sums = (long long*)calloc((size_t)n_meshes, sizeof(long long));
+  for (int f = 0; f < n_faces; ++f) {
+    fixed[2 * (size_t)f] = llround(ldexp((double)power_front[f], k));
+    fixed[2 * (size_t)f + 1] = llround(ldexp((double)power_rear[f], k));
+  }
+  rad_ctx_t c = {n_faces, faces9, front, rear, fixed, face_to_mesh, seed, epoch, flags, sums};
+  parallel_for(n_faces, 1, rad_body, &c);
+  for (int m = 0; m < n_meshes; ++m)
+    absorption[m] = ldexp((double)sums[m], -k);
+  free(fixed);
+  free(sums);
+}
+
+/* ------------------------------------------------------------------ */
 /* Analytic view factors in double (textbook, one-sided).               */
 /* Equal coaxial parallel rectangles a x b at distance c and two          */
 /* perpendicular rectangles sharing an edge; the same formulas the       */

@@ -43,6 +43,14 @@ void ffo_emit(int n_faces, const float* faces9, const int32_t* front, const int3
 void ffo_form_factor_counts(int n_faces, const float* faces9, const int32_t* front,
                             const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
                             uint32_t* counts);
+void ffo_disc_source(const float* direction3, const float* center3, float distance, float radius, float* disc17);
+void ffo_emit_disc_ray(const float* disc17, uint64_t j, uint64_t seed, uint32_t epoch, float* ray6);
+void ffo_emit_parallel(const float* disc17, long n_rays, uint64_t seed, uint32_t epoch, float* rays6);
+void ffo_parallel_rays(int n_faces, const float* faces9, const float* disc17, long n_rays, uint64_t seed,
+                       uint32_t epoch, uint32_t* side_counts);
+void ffo_radiance_absorption(int n_faces, const float* faces9, const int32_t* front, const int32_t* rear,
+                             const float* power_front, const float* power_rear, const int32_t* face_to_mesh,
+                             int n_meshes, uint64_t seed, uint32_t epoch, int flags, double* absorption);
 double ffo_vf_parallel(double a, double b, double c);
 double ffo_vf_perpendicular(double H, double W, double L);
 

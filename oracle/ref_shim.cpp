@@ -14,8 +14,17 @@
 //   math::triangle_intersect                                  math/triangle.cpp:28-79
 //   math::rotate_towards                                      math/mat.cpp:25-49
 //   csv_export::export_csv                                    import_export/csv_export.cpp:26-46
+//   radiance_equation::system_create / calculate              thermal_equation/radiance_cpu.cpp:96-190
+//   parallel_rays_cpu::system_create / calculate              thermal_equation/parallel_rays_cpu.cpp:66-131
+//   parallel_rays_emission_cpu::system_create                 emission/parallel_rays_cpu.cpp:88-138
+//   math::triangles_bsphere                                   math/triangle.cpp:361-384
 #include "ray_caster/system.h"
 #include "import_export/csv_export.h"
+#include "subject/system.h"
+#include "thermal_equation/system.h"
+#include "thermal_equation/radiance_cpu.h"
+#include "thermal_equation/parallel_rays_cpu.h"
+#include "emission/parallel_rays_cpu.h"
 #include "emission/system.h"
 #include "emission/malley_emission.h"
 #include "form_factors/system.h"
@@ -271,6 +280,116 @@ long ffref_step_run(void* handle, int n_rays, const float* weights2, float total
   task.rays = 0;
   emission::system_free(em);
   return n_cast;
+}
+
+// A subject scene: meshes3 = (first, count, material) per mesh; optics4 =
+// (front emissivity, rear emissivity, front absorbance, rear absorbance)
+// per material, the other properties those of the reference's black body.
+static subject::scene_t make_subject(int n_faces, const float* faces9, int n_meshes, const int* meshes3,
+                                     int n_materials, const float* optics4, std::vector<subject::mesh_t>& meshes,
+                                     std::vector<subject::material_t>& materials)
+{
+  meshes.resize(n_meshes);
+  for (int m = 0; m < n_meshes; ++m)
+    meshes[m] = subject::make_mesh(meshes3[3 * m], meshes3[3 * m + 1], meshes3[3 * m + 2]);
+  materials.resize(n_materials);
+  for (int k = 0; k < n_materials; ++k) {
+    materials[k] = subject::black_body();
+    materials[k].front.emissivity = optics4[4 * k];
+    materials[k].rear.emissivity = optics4[4 * k + 1];
+    materials[k].front.absorbance = optics4[4 * k + 2];
+    materials[k].rear.absorbance = optics4[4 * k + 3];
+  }
+  subject::scene_t s;
+  s.n_faces = n_faces;
+  s.faces = (subject::face_t*)faces9;
+  s.n_meshes = n_meshes;
+  s.meshes = meshes.data();
+  s.n_materials = n_materials;
+  s.materials = materials.data();
+  return s;
+}
+
+// One calculate() of the reference's radiance equation with malley_cpu over
+// caster `type`: emission and absorption per mesh (added to zeros).
+int ffref_radiance(int type, int n_faces, const float* faces9, int n_meshes, const int* meshes3, int n_materials,
+                   const float* optics4, const float* temperatures, int n_rays, float* emission_out,
+                   float* absorption_out)
+{
+  std::vector<subject::mesh_t> meshes;
+  std::vector<subject::material_t> materials;
+  subject::scene_t scene = make_subject(n_faces, faces9, n_meshes, meshes3, n_materials, optics4, meshes, materials);
+  ray_caster::system_t* caster = ray_caster::system_create(type);
+  emission::system_t* emitter = emission::system_create(EMISSION_MALLEY_CPU, caster);
+  radiance_equation::params_t params = {emitter, n_rays};
+  // the factory (thermal_equation/factory.cpp) would pull in every equation type
+  thermal_equation::system_t* eq = radiance_equation::system_create();
+  int r = thermal_equation::system_init(eq, &params);
+  if (r >= 0)
+    r = thermal_equation::system_set_scene(eq, &scene);
+  std::memset(emission_out, 0, sizeof(float) * n_meshes);
+  std::memset(absorption_out, 0, sizeof(float) * n_meshes);
+  if (r >= 0) {
+    thermal_equation::task_t task = {temperatures, emission_out, absorption_out};
+    r = thermal_equation::system_calculate(eq, &task);
+  }
+  thermal_equation::system_free(eq);
+  emission::system_free(emitter);
+  ray_caster::system_free(caster);
+  return r;
+}
+
+struct ffref_source_param {
+  float power;
+  float direction[3];
+};
+
+static parallel_rays_cpu::source_t ffref_source(void* param)
+{
+  const ffref_source_param* p = (const ffref_source_param*)param;
+  parallel_rays_cpu::source_t s;
+  s.power = p->power;
+  s.direction = math::make_vec3(p->direction[0], p->direction[1], p->direction[2]);
+  return s;
+}
+
+// One calculate() of the reference's distant-source (parallel rays)
+// equation: absorbed power per mesh.
+int ffref_parallel_rays(int type, int n_faces, const float* faces9, int n_meshes, const int* meshes3,
+                        int n_materials, const float* optics4, int n_rays, float power, const float* direction3,
+                        float* absorption_out)
+{
+  std::vector<subject::mesh_t> meshes;
+  std::vector<subject::material_t> materials;
+  subject::scene_t scene = make_subject(n_faces, faces9, n_meshes, meshes3, n_materials, optics4, meshes, materials);
+  ray_caster::system_t* caster = ray_caster::system_create(type);
+  emission::system_t* emitter = emission::system_create(EMISSION_PARALLEL_RAYS_CPU, caster);
+  ffref_source_param sp = {power, {direction3[0], direction3[1], direction3[2]}};
+  parallel_rays_cpu::params_t params = {n_rays, emitter, &sp, &ffref_source};
+  thermal_equation::system_t* eq = parallel_rays_cpu::system_create();
+  int r = thermal_equation::system_init(eq, &params);
+  if (r >= 0)
+    r = thermal_equation::system_set_scene(eq, &scene);
+  std::memset(absorption_out, 0, sizeof(float) * n_meshes);
+  if (r >= 0) {
+    std::vector<float> em(n_meshes, 0.f);
+    std::vector<float> temps(n_meshes, 0.f);
+    thermal_equation::task_t task = {temps.data(), em.data(), absorption_out};
+    r = thermal_equation::system_calculate(eq, &task);
+  }
+  thermal_equation::system_free(eq);
+  emission::system_free(emitter);
+  ray_caster::system_free(caster);
+  return r;
+}
+
+void ffref_bsphere(int n_faces, const float* faces9, float* center3, float* radius)
+{
+  math::sphere_t s = math::triangles_bsphere((const math::triangle_t*)faces9, n_faces);
+  center3[0] = s.center.x;
+  center3[1] = s.center.y;
+  center3[2] = s.center.z;
+  *radius = s.radius;
 }
 
 // The reference's CSV export of an n x n matrix (n meshes, row-major floats).

@@ -22,6 +22,7 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
 def _f32(a):
@@ -56,7 +57,37 @@ class Oracle:
         lib.ffo_vf_parallel.restype = C.c_double
         lib.ffo_vf_perpendicular.argtypes = [C.c_double] * 3
         lib.ffo_vf_perpendicular.restype = C.c_double
+        lib.ffo_disc_source.argtypes = [_f32p, _f32p, C.c_float, C.c_float, _f32p]
+        lib.ffo_emit_parallel.argtypes = [_f32p, C.c_long, C.c_uint64, C.c_uint32, _f32p]
+        lib.ffo_parallel_rays.argtypes = [C.c_int, _f32p, _f32p, C.c_long, C.c_uint64, C.c_uint32, _u32p]
+        lib.ffo_radiance_absorption.argtypes = [C.c_int, _f32p, _i32p, _i32p, _f32p, _f32p, _i32p, C.c_int,
+                                                C.c_uint64, C.c_uint32, C.c_int, _f64p]
         self.lib = lib
+
+    def disc_source(self, direction, center, distance, radius):
+        d = np.zeros(17, np.float32)
+        self.lib.ffo_disc_source(_f32(direction), _f32(center), float(distance), float(radius), d)
+        return d
+
+    def emit_parallel(self, disc, n_rays, seed, epoch=0):
+        rays = np.zeros((int(n_rays), 6), np.float32)
+        self.lib.ffo_emit_parallel(_f32(disc), int(n_rays), int(seed), int(epoch), rays)
+        return rays
+
+    def parallel_rays(self, faces, disc, n_rays, seed, epoch=0):
+        faces = _f32(faces).reshape(-1, 9)
+        out = np.zeros((len(faces), 2), np.uint32)
+        self.lib.ffo_parallel_rays(len(faces), faces, _f32(disc), int(n_rays), int(seed), int(epoch), out)
+        return out
+
+    def radiance_absorption(self, faces, front, rear, power_front, power_rear, face_to_mesh, n_meshes, seed,
+                            epoch=0, flags=0):
+        faces = _f32(faces).reshape(-1, 9)
+        out = np.zeros(int(n_meshes), np.float64)
+        self.lib.ffo_radiance_absorption(len(faces), faces, _i32(front), _i32(rear), _f32(power_front),
+                                         _f32(power_rear), _i32(face_to_mesh), int(n_meshes), int(seed), int(epoch),
+                                         int(flags), out)
+        return out
 
     def set_threads(self, n):
         self.lib.ffo_set_threads(int(n))
@@ -155,7 +186,43 @@ class Reference:
         lib.ffref_step_close.argtypes = [C.c_void_p]
         lib.ffref_export_csv.argtypes = [C.c_char_p, C.c_int, _f32p]
         lib.ffref_export_csv.restype = C.c_int
+        lib.ffref_radiance.argtypes = [C.c_int, C.c_int, _f32p, C.c_int, _i32p, C.c_int, _f32p, _f32p, C.c_int,
+                                       _f32p, _f32p]
+        lib.ffref_radiance.restype = C.c_int
+        lib.ffref_parallel_rays.argtypes = [C.c_int, C.c_int, _f32p, C.c_int, _i32p, C.c_int, _f32p, C.c_int,
+                                            C.c_float, _f32p, _f32p]
+        lib.ffref_parallel_rays.restype = C.c_int
+        lib.ffref_bsphere.argtypes = [C.c_int, _f32p, _f32p, C.POINTER(C.c_float)]
         self.lib = lib
+
+    def radiance(self, faces, meshes, materials, temperatures, n_rays, caster=3):
+        """radiance_equation calculate() with malley_cpu over caster `caster`:
+        (status, emission, absorption) per mesh."""
+        faces = _f32(faces).reshape(-1, 9)
+        m3 = np.ascontiguousarray(np.asarray(meshes, np.int32).reshape(-1, 3))
+        opt = _f32(np.asarray(materials, np.float32).reshape(-1, 4))
+        em = np.zeros(len(m3), np.float32)
+        ab = np.zeros(len(m3), np.float32)
+        rc = self.lib.ffref_radiance(int(caster), len(faces), faces, len(m3), m3, len(opt), opt,
+                                     _f32(temperatures), int(n_rays), em, ab)
+        return rc, em, ab
+
+    def parallel_rays(self, faces, meshes, materials, n_rays, power, direction, caster=3):
+        """parallel_rays_cpu calculate() (distant source): (status, absorption)."""
+        faces = _f32(faces).reshape(-1, 9)
+        m3 = np.ascontiguousarray(np.asarray(meshes, np.int32).reshape(-1, 3))
+        opt = _f32(np.asarray(materials, np.float32).reshape(-1, 4))
+        ab = np.zeros(len(m3), np.float32)
+        rc = self.lib.ffref_parallel_rays(int(caster), len(faces), faces, len(m3), m3, len(opt), opt, int(n_rays),
+                                          float(power), _f32(direction), ab)
+        return rc, ab
+
+    def bsphere(self, faces):
+        faces = _f32(faces).reshape(-1, 9)
+        c = np.zeros(3, np.float32)
+        r = C.c_float()
+        self.lib.ffref_bsphere(len(faces), faces, c, C.byref(r))
+        return c, np.float32(r.value)
 
     def export_csv(self, filename, ff):
         """csv_export::export_csv of an n x n float matrix; returns the
