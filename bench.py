@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
+    ap.add_argument("--no-thermal", action="store_true", help="skip the radiance / distant-source section")
     ap.add_argument("--served-requests", type=int, default=16)
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     return ap.parse_args()
@@ -372,6 +373,62 @@ def csv_section(ctx, stream, counts, front, rear, n):
 
 
 # ---------------------------------------------------------------------------
+# ray-traced thermal equations on the same scene and grid
+# ---------------------------------------------------------------------------
+def thermal_section(ctx, faces, rays_per_face):
+    """One radiance-equation step (per-face meshes, temperature-weighted
+    Malley emission, absorbed power scattered to the hit meshes) and one
+    distant-source step (a disc of parallel rays) through the C ABI, against
+    the reference's radiance_cpu over its zgrid_cpu caster on a bounded ray
+    budget."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Reference
+    n = len(faces)
+    n_sphere = n - 1600  # the two 20 x 20 plates come last
+    meshes = [(f, 1, 0 if f < n_sphere else 1) for f in range(n)]
+    # sphere: inward emitter only, so that every ray starts inside the scene
+    materials = [(0.9, 0.0, 0.8, 0.8), (0.7, 0.6, 0.5, 0.4)]
+    temps = (300.0 + 100.0 * np.random.default_rng(5).random(n)).astype(np.float32)
+    n_rays = rays_per_face * n
+    ctx.radiance_step(faces, meshes, materials, temps, n_rays, seed=1, epoch=0)  # warm-up
+    reps = 3
+    t0 = time.perf_counter()
+    for e in range(reps):
+        em, ab = ctx.radiance_step(faces, meshes, materials, temps, n_rays, seed=1, epoch=1 + e)
+    rad_s = (time.perf_counter() - t0) / reps
+    rad_ms_kernel = ctx.stats().kernel_ms
+    sun_rays = 10_000_000
+    ctx.distant_source_step(faces, meshes, materials, sun_rays, 1361.0, [0.3, -0.4, -0.8], seed=2)
+    t0 = time.perf_counter()
+    for e in range(reps):
+        sun = ctx.distant_source_step(faces, meshes, materials, sun_rays, 1361.0, [0.3, -0.4, -0.8], seed=2,
+                                      epoch=1 + e)
+    sun_s = (time.perf_counter() - t0) / reps
+    sun_ms_kernel = ctx.stats().kernel_ms
+    ref = None
+    if Reference.available():
+        sample = 200_000
+        r = Reference()
+        m3 = np.array(meshes, np.int32)
+        t0 = time.perf_counter()
+        rc, _, _ = r.radiance(faces, m3, materials, temps, sample, caster=Reference.ZGRID_CPU)
+        ref_s = time.perf_counter() - t0
+        if rc == 0:
+            ref = {"rays_per_s": sample / ref_s, "cores": 1, "kind": "reference",
+                   "sample": "radiance_cpu + malley_cpu + zgrid_cpu (oracle/_ref), one calculate() of %d rays on "
+                             "the same scene and meshes (the reference's equation is single-threaded)" % sample}
+    return {
+        "workload": "enclosure, %d per-face meshes, two materials, temperatures 300-400 K" % n,
+        "radiance": {"rays": n_rays, "step_s": rad_s, "rays_per_s": n_rays / rad_s, "kernel_ms": rad_ms_kernel,
+                     "emitted_w": float(em.sum()), "absorbed_w": float(ab.sum()),
+                     "path": "host weights and powers -> fused emit/trace/fixed-point scatter -> host sums"},
+        "distant_source": {"rays": sun_rays, "step_s": sun_s, "rays_per_s": sun_rays / sun_s,
+                           "kernel_ms": sun_ms_kernel, "absorbed_w": float(sun.sum())},
+        "cpu_baseline": ref,
+    }
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def fp32_peak(device):
@@ -506,9 +563,11 @@ def ours(args):
     h2d = 16 * n_chunks
     d2h = 4 * n * n
 
-    batched = served = csv = None
+    batched = served = csv = thermal = None
     if rank == 0 and world == 1 and not args.no_csv:
         csv = csv_section(ctx, stream, counts, front, rear, n)
+    if rank == 0 and world == 1 and not args.no_thermal:
+        thermal = thermal_section(ctx, faces, args.rays_per_face)
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_section(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_served:
@@ -561,6 +620,8 @@ def ours(args):
             line["served"] = served
         if csv is not None:
             line["csv"] = csv
+        if thermal is not None:
+            line["thermal"] = thermal
         print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -67,6 +67,10 @@ struct ffb_server {
   std::vector<std::thread> workers;
   int running = 0;
   int peak_running = 0;
+  // Held around each request's trace: the fused kernel fills the whole GPU,
+  // so two traces at once only share it (and mix their grids in L2); the
+  // other slots meanwhile upload scenes and build grids.
+  std::mutex trace_mu;
 };
 
 namespace {
@@ -80,7 +84,7 @@ unsigned long long estimate_bytes(int n_faces)
   return 4ull * n * n + 1536ull * n + (8ull << 20);
 }
 
-int run_request(ffb_ctx* ctx, cudaStream_t stream, Request& r)
+int run_request(ffb_server* s, ffb_ctx* ctx, cudaStream_t stream, Request& r)
 {
   int rc = ffb_scene_set(ctx, r.faces.data(), r.n_faces);
   ffb_grid_params gp = {0, 0, 0, r.cells_per_face, 1};
@@ -96,6 +100,9 @@ int run_request(ffb_ctx* ctx, cudaStream_t stream, Request& r)
     return ffb_set_error(FFB_ERR_NO_MEMORY, "request matrix allocation failed");
   }
   std::vector<int32_t> front((size_t)r.n_faces, r.rays_per_face), rear((size_t)r.n_faces, 0);
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess)  // preparation done before taking the GPU
+    return ffb_set_error(FFB_ERR_CUDA, cudaGetErrorString(e));
+  std::lock_guard<std::mutex> trace(s->trace_mu);
   rc = ffb_form_factor_counts(ctx, front.data(), rear.data(), r.seed, 0, r.flags, nullptr, r.n_faces, r.counts);
   if (rc < 0)
     return rc;
@@ -140,7 +147,7 @@ void worker_main(ffb_server* s, int slot)
     int err = rc;
     if (err >= 0) {
       cudaEventRecord(e0, stream);
-      err = run_request(ctx, stream, *r);
+      err = run_request(s, ctx, stream, *r);
       cudaEventRecord(e1, stream);
       cudaEventSynchronize(e1);
       float ms = 0;

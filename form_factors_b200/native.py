@@ -67,17 +67,13 @@ class Optics(C.Structure):
 
 
 def _meshes(meshes):
-    arr = (Mesh * len(meshes))()
-    for i, (first, n, mat) in enumerate(meshes):
-        arr[i] = Mesh(int(first), int(n), int(mat))
-    return arr
+    """ffb_mesh array as a (n, 3) int32 numpy array (layout-identical)."""
+    return np.ascontiguousarray(np.asarray(meshes, np.int32).reshape(-1, 3))
 
 
 def _optics(materials):
-    arr = (Optics * len(materials))()
-    for i, m in enumerate(materials):
-        arr[i] = Optics(*[float(x) for x in m])
-    return arr
+    """ffb_optics array as a (n, 4) float32 numpy array (layout-identical)."""
+    return np.ascontiguousarray(np.asarray(materials, np.float32).reshape(-1, 4))
 
 
 def bounding_sphere(faces):
@@ -443,8 +439,9 @@ class Context:
         n_m = len(meshes)
         emission = np.zeros(n_m, np.float32) if emission is None else emission
         absorption = np.zeros(n_m, np.float32) if absorption is None else absorption
-        _check(self._lib.ffb_radiance_step(self._h, _ptr(faces), len(faces), _meshes(meshes), n_m,
-                                           _optics(materials), len(materials), _ptr(t), int(n_rays), int(seed),
+        m3, opt = _meshes(meshes), _optics(materials)
+        _check(self._lib.ffb_radiance_step(self._h, _ptr(faces), len(faces), _ptr(m3), n_m,
+                                           _ptr(opt), len(opt), _ptr(t), int(n_rays), int(seed),
                                            int(epoch), int(flags), _ptr(emission), _ptr(absorption)))
         return emission, absorption
 
@@ -456,8 +453,9 @@ class Context:
         d = np.ascontiguousarray(direction, np.float32)
         n_m = len(meshes)
         absorption = np.zeros(n_m, np.float32) if absorption is None else absorption
-        _check(self._lib.ffb_distant_source_step(self._h, _ptr(faces), len(faces), _meshes(meshes), n_m,
-                                                 _optics(materials), len(materials), int(n_rays), float(power),
+        m3, opt = _meshes(meshes), _optics(materials)
+        _check(self._lib.ffb_distant_source_step(self._h, _ptr(faces), len(faces), _ptr(m3), n_m,
+                                                 _ptr(opt), len(opt), int(n_rays), float(power),
                                                  _ptr(d), int(seed), int(epoch), _ptr(absorption)))
         return absorption
 

@@ -199,7 +199,7 @@ typedef struct {
   int n_faces;
   double queue_s;    /* submit -> admission */
   double latency_s;  /* submit -> result resident */
-  double gpu_ms;     /* device time of the request's work on its slot stream */
+  double gpu_ms;     /* time on the slot stream from the request's first to its last device operation (includes waiting for another request's trace) */
 } ffb_request_info;
 
 typedef struct {
