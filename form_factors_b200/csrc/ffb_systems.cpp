@@ -586,6 +586,527 @@ int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells
 }  // namespace b200_form_factors
 
 // ===========================================================================
+// Parallel-rays emission
+// ===========================================================================
+namespace b200_parallel_rays_emission {
+
+struct emitter_t : emission::system_t {
+  ray_caster::system_t* caster;
+  ray_caster::scene_t* scene;
+  ffb_ctx* ctx;
+  uint64_t seed;
+  uint32_t epoch;  // calls so far: every calculate draws fresh rays
+};
+
+static int init(emitter_t* s, ray_caster::system_t* caster)
+{
+  s->caster = caster;
+  s->scene = nullptr;
+  s->ctx = nullptr;
+  s->seed = 1;
+  s->epoch = 0;
+  return ffb_ctx_create(device_from_env(), &s->ctx);
+}
+
+static int shutdown(emitter_t* s)
+{
+  ffb_ctx_destroy(s->ctx);
+  s->ctx = nullptr;
+  s->scene = nullptr;
+  return EMISSION_OK;
+}
+
+// emission/parallel_rays_cpu.cpp:64-80
+static int set_scene(emitter_t* s, ray_caster::scene_t* scene)
+{
+  if (scene == 0 || scene->n_faces == 0)
+    return -EMISSION_ERROR;
+  s->scene = scene;
+  int r = 0;
+  if (s->caster) {
+    if ((r = s->caster->methods->set_scene(s->caster, scene)) < 0)
+      return r;
+    if ((r = s->caster->methods->prepare(s->caster)) < 0)
+      return r;
+  }
+  return EMISSION_OK;
+}
+
+// emission/parallel_rays_cpu.cpp:83-121
+static int calculate(emitter_t* s, emission::task_t* task)
+{
+  if (!s->ctx)
+    return -EMISSION_ERROR;
+  parallel_rays_emission_cpu::task_t* t = (parallel_rays_emission_cpu::task_t*)task;
+  if (task->rays) {
+    task_release(task->rays);
+    task->rays = 0;
+  }
+  if (t->n_rays <= 0)
+    return EMISSION_OK;
+  ffb_disc_source src;
+  const math::vec3 d = t->direction, c = t->center;
+  src.direction[0] = d.x;
+  src.direction[1] = d.y;
+  src.direction[2] = d.z;
+  src.center[0] = c.x;
+  src.center[1] = c.y;
+  src.center[2] = c.z;
+  src.distance = t->distance;
+  src.radius = t->radius;
+  ray_caster::task_t* rays = task_alloc(t->n_rays);
+  int r = ffb_emit_parallel(s->ctx, &src, t->n_rays, s->seed, s->epoch++, &rays->ray[0].origin.x);
+  if (r < 0) {
+    task_release(rays);
+    return r;
+  }
+  task->rays = rays;
+  if (s->caster && (r = s->caster->methods->cast(s->caster, rays)) < 0)
+    return r;
+  return EMISSION_OK;
+}
+
+const emission::system_methods_t methods = {
+    (int (*)(emission::system_t*, ray_caster::system_t*))&init,
+    (int (*)(emission::system_t*))&shutdown,
+    (int (*)(emission::system_t*, ray_caster::scene_t*))&set_scene,
+    (int (*)(emission::system_t*, emission::task_t*))&calculate,
+};
+
+emission::system_t* system_create()
+{
+  emitter_t* s = (emitter_t*)malloc(sizeof(emitter_t));
+  s->methods = &methods;
+  return s;
+}
+
+emission::system_t* create(ray_caster::system_t* caster)
+{
+  emission::system_t* s = system_create();
+  s->methods->init(s, caster);
+  return s;
+}
+
+void destroy(emission::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+int set_seed(emission::system_t* system, uint64_t seed)
+{
+  if (!system || system->methods != &methods)
+    return FFB_ERR_ARG;
+  emitter_t* s = (emitter_t*)system;
+  s->seed = seed;
+  s->epoch = 0;
+  return FFB_OK;
+}
+
+// seed and call number of a B200 parallel-rays emitter for the fused step
+bool draw_key(emission::system_t* system, uint64_t* seed, uint32_t* epoch)
+{
+  if (!system || system->methods != &methods)
+    return false;
+  emitter_t* s = (emitter_t*)system;
+  *seed = s->seed;
+  *epoch = s->epoch++;
+  return true;
+}
+
+}  // namespace b200_parallel_rays_emission
+
+// ===========================================================================
+// Ray-traced thermal equations (shared state)
+// ===========================================================================
+namespace {
+
+struct thermal_t : thermal_equation::system_t {
+  emission::system_t* emitter;
+  int n_rays;
+  int fused;
+  subject::scene_t* scene;
+  ray_caster::scene_t rc_scene;
+  ffb_ctx* ctx;
+  ffb_grid_params grid;
+  uint64_t seed;
+  uint32_t epoch;
+  // distant source
+  void* source_param;
+  parallel_rays_cpu::source_t (*source)(void* param);
+};
+
+void mesh_tables(const subject::scene_t* scene, std::vector<ffb_mesh>& meshes, std::vector<ffb_optics>& optics)
+{
+  meshes.resize((size_t)scene->n_meshes);
+  for (int m = 0; m < scene->n_meshes; ++m)
+    meshes[m] = ffb_mesh{scene->meshes[m].first_idx, scene->meshes[m].n_faces, scene->meshes[m].material_idx};
+  optics.resize((size_t)scene->n_materials);
+  for (int k = 0; k < scene->n_materials; ++k) {
+    const subject::material_t& mt = scene->materials[k];
+    optics[k] = ffb_optics{mt.front.emissivity, mt.rear.emissivity, mt.front.absorbance, mt.rear.absorbance};
+  }
+}
+
+// subject::build_face_to_mesh_index (subject/system.cpp:93-108)
+std::vector<int> face_mesh_index(const subject::scene_t* scene)
+{
+  std::vector<int> idx((size_t)scene->n_faces, 0);
+  for (int m = 0; m < scene->n_meshes; ++m)
+    for (int f = 0; f < scene->meshes[m].n_faces; ++f)
+      idx[(size_t)(scene->meshes[m].first_idx + f)] = m;
+  return idx;
+}
+
+const subject::material_t& mesh_material(const subject::scene_t* scene, int m)
+{
+  return scene->materials[scene->meshes[m].material_idx];
+}
+
+int thermal_init(thermal_t* s, emission::system_t* emitter, int n_rays, bool fused)
+{
+  s->emitter = emitter;
+  s->n_rays = n_rays;
+  s->fused = fused;
+  s->scene = 0;
+  s->rc_scene = ray_caster::scene_t{0, 0};
+  s->ctx = nullptr;
+  s->grid = ffb_grid_params{0, 0, 0, 32.f, 1};
+  s->seed = 1;
+  s->epoch = 0;
+  s->source_param = 0;
+  s->source = 0;
+  if (!fused)
+    return THERMAL_EQUATION_OK;
+  const int rc = ffb_ctx_create(device_from_env(), &s->ctx);
+  if (rc == FFB_OK)
+    ffb_ctx_set_stats(s->ctx, 0);
+  return rc;
+}
+
+int thermal_shutdown(thermal_t* s)
+{
+  s->scene = 0;
+  ffb_ctx_destroy(s->ctx);
+  s->ctx = nullptr;
+  return THERMAL_EQUATION_OK;
+}
+
+// radiance_cpu.cpp:78-94 / parallel_rays_cpu.cpp:66-78: the fused path keeps
+// the scene and grid resident; the other path sets the emitter's scene.
+int thermal_set_scene(thermal_t* s, subject::scene_t* scene)
+{
+  s->scene = scene;
+  s->rc_scene = ray_caster::scene_t{scene->n_faces, scene->faces};
+  if (!s->fused)
+    return s->emitter->methods->set_scene(s->emitter, &s->rc_scene);
+  if (scene->n_faces == 0)
+    return -EMISSION_ERROR;
+  if (!s->ctx)
+    return FFB_ERR_NO_DEVICE;
+  int r = ffb_scene_set(s->ctx, &scene->faces[0].points[0].x, scene->n_faces);
+  if (r < 0)
+    return r;
+  return ffb_grid_build(s->ctx, &s->grid);
+}
+
+thermal_t* as_thermal(thermal_equation::system_t* system, const thermal_equation::system_methods_t* m)
+{
+  return system && system->methods == m ? (thermal_t*)system : nullptr;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Radiance equation
+// ===========================================================================
+namespace b200_radiance_equation {
+
+static int init(thermal_t* s, radiance_equation::params_t* params)
+{
+  emission::system_t* e = params ? params->emitter : 0;
+  return thermal_init(s, e, params ? params->n_rays : 0, e == 0 || e->methods == &b200_emission::methods);
+}
+
+static int shutdown(thermal_t* s) { return thermal_shutdown(s); }
+
+static int set_scene(thermal_t* s, subject::scene_t* scene) { return thermal_set_scene(s, scene); }
+
+static int calculate_fused(thermal_t* s, thermal_equation::task_t* task)
+{
+  std::vector<ffb_mesh> meshes;
+  std::vector<ffb_optics> optics;
+  mesh_tables(s->scene, meshes, optics);
+  uint64_t seed = s->seed;
+  uint32_t epoch = 0;
+  int flags = 0;
+  if (!b200_emission::draw_key(s->emitter, &seed, &epoch, &flags))
+    epoch = s->epoch++;
+  return ffb_radiance_step(s->ctx, &s->scene->faces[0].points[0].x, s->scene->n_faces, meshes.data(),
+                           s->scene->n_meshes, optics.data(), s->scene->n_materials, task->temperatures, s->n_rays,
+                           seed, epoch, flags, task->emission, task->absorption);
+}
+
+// thermal_equation/radiance_cpu.cpp:96-190 over any Malley-style emitter
+static int calculate_generic(thermal_t* s, thermal_equation::task_t* task)
+{
+  const subject::scene_t* scene = s->scene;
+  const int n_faces = scene->n_faces;
+  std::vector<float> area((size_t)n_faces), w(2 * (size_t)n_faces, 0.f);
+  for (int f = 0; f < n_faces; ++f)
+    area[(size_t)f] = triangle_area(scene->faces[f]);
+  float total = 0;
+  for (int m = 0; m != scene->n_meshes; ++m) {
+    const subject::material_t& material = mesh_material(scene, m);
+    const float density = task->temperatures[m];
+    const float front_density = density * material.front.emissivity;
+    const float rear_density = density * material.rear.emissivity;
+    const subject::mesh_t& mesh = scene->meshes[m];
+    for (int f = mesh.first_idx; f != mesh.first_idx + mesh.n_faces; ++f) {
+      const float front = front_density * area[(size_t)f];
+      const float rear = rear_density * area[(size_t)f];
+      total += front + rear;
+      w[2 * (size_t)f] = front;
+      w[2 * (size_t)f + 1] = rear;
+    }
+  }
+  malley_emission::task_t et(s->n_rays, total, w.data());
+  int r = s->emitter->methods->calculate(s->emitter, &et);
+  if (r < 0) {
+    task_release(et.rays);
+    return r;
+  }
+  const ray_caster::task_t* rays = et.rays;
+  if (!rays)
+    return THERMAL_EQUATION_OK;
+  const std::vector<int> f2m = face_mesh_index(scene);
+  const float sigma = 5.670400e-8f;
+  int n_ray = 0;
+  for (int m = 0; m != scene->n_meshes; ++m) {
+    const subject::mesh_t& mesh = scene->meshes[m];
+    const subject::material_t& material = mesh_material(scene, m);
+    const float T = task->temperatures[m];
+    const float power_density = sigma * (T * T * T * T);
+    const float front_density = power_density * material.front.emissivity;
+    const float rear_density = power_density * material.rear.emissivity;
+    for (int f = mesh.first_idx; f != mesh.first_idx + mesh.n_faces; ++f) {
+      const float front_emission = front_density * area[(size_t)f];
+      const float rear_emission = rear_density * area[(size_t)f];
+      task->emission[m] += front_emission + rear_emission;
+      const int face_rays_front = emitted(s->n_rays, w[2 * (size_t)f], total);
+      const int face_rays_rear = emitted(s->n_rays, w[2 * (size_t)f + 1], total);
+      const int face_rays = face_rays_front + face_rays_rear;
+      for (int j = 0; j != face_rays && n_ray < rays->n_tasks; ++j, ++n_ray) {
+        if (rays->hit_face[n_ray]) {
+          const int hit_mesh = f2m[(size_t)(rays->hit_face[n_ray] - s->rc_scene.faces)];
+          const float ray_power =
+              j < face_rays_front ? (front_emission / face_rays_front) : (rear_emission / face_rays_rear);
+          task->absorption[hit_mesh] += ray_power;
+        }
+      }
+    }
+  }
+  task_release(et.rays);
+  return THERMAL_EQUATION_OK;
+}
+
+static int calculate(thermal_t* s, thermal_equation::task_t* task)
+{
+  if (!s->scene)
+    return -THERMAL_EQUATION_ERROR;
+  return s->fused ? calculate_fused(s, task) : calculate_generic(s, task);
+}
+
+static const thermal_equation::system_methods_t methods = {
+    (int (*)(thermal_equation::system_t*, void*))&init,
+    (int (*)(thermal_equation::system_t*))&shutdown,
+    (int (*)(thermal_equation::system_t*, subject::scene_t*))&set_scene,
+    (int (*)(thermal_equation::system_t*, thermal_equation::task_t*))&calculate,
+};
+
+thermal_equation::system_t* system_create()
+{
+  thermal_t* s = (thermal_t*)malloc(sizeof(thermal_t));
+  s->methods = &methods;
+  return s;
+}
+
+thermal_equation::system_t* create(radiance_equation::params_t* params)
+{
+  thermal_equation::system_t* s = system_create();
+  s->methods->init(s, params);
+  return s;
+}
+
+void destroy(thermal_equation::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+int set_seed(thermal_equation::system_t* system, uint64_t seed)
+{
+  thermal_t* s = as_thermal(system, &methods);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->seed = seed;
+  s->epoch = 0;
+  return FFB_OK;
+}
+
+int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float cells_per_face)
+{
+  thermal_t* s = as_thermal(system, &methods);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->grid = ffb_grid_params{nx, ny, nz, cells_per_face, 1};
+  return FFB_OK;
+}
+
+}  // namespace b200_radiance_equation
+
+// ===========================================================================
+// Distant source (parallel rays)
+// ===========================================================================
+namespace b200_distant_source {
+
+static int init(thermal_t* s, parallel_rays_cpu::params_t* params)
+{
+  emission::system_t* e = params ? params->emitter : 0;
+  const int rc = thermal_init(s, e, params ? params->n_rays : 0,
+                              e == 0 || e->methods == &b200_parallel_rays_emission::methods);
+  s->source_param = params ? params->source_param : 0;
+  s->source = params ? params->source : 0;
+  return rc;
+}
+
+static int shutdown(thermal_t* s) { return thermal_shutdown(s); }
+
+static int set_scene(thermal_t* s, subject::scene_t* scene) { return thermal_set_scene(s, scene); }
+
+static int calculate_fused(thermal_t* s, thermal_equation::task_t* task, const parallel_rays_cpu::source_t& src)
+{
+  std::vector<ffb_mesh> meshes;
+  std::vector<ffb_optics> optics;
+  mesh_tables(s->scene, meshes, optics);
+  uint64_t seed = s->seed;
+  uint32_t epoch = 0;
+  if (!b200_parallel_rays_emission::draw_key(s->emitter, &seed, &epoch))
+    epoch = s->epoch++;
+  const float dir[3] = {src.direction.x, src.direction.y, src.direction.z};
+  return ffb_distant_source_step(s->ctx, &s->scene->faces[0].points[0].x, s->scene->n_faces, meshes.data(),
+                                 s->scene->n_meshes, optics.data(), s->scene->n_materials, s->n_rays, src.power, dir,
+                                 seed, epoch, task->absorption);
+}
+
+// thermal_equation/parallel_rays_cpu.cpp:92-131 over any parallel-rays emitter
+static int calculate_generic(thermal_t* s, thermal_equation::task_t* task, const parallel_rays_cpu::source_t& src)
+{
+  const subject::scene_t* scene = s->scene;
+  float center[3], bradius;
+  int r = ffb_bounding_sphere(&scene->faces[0].points[0].x, scene->n_faces, center, &bradius);
+  if (r < 0)
+    return r;
+  const float radius = bradius * 1.1f;
+  parallel_rays_emission_cpu::task_t et(s->n_rays);
+  et.rays = 0;
+  et.center = math::vec3{center[0], center[1], center[2]};
+  et.distance = 1.1f + radius;
+  et.direction = src.direction;
+  et.radius = radius;
+  if ((r = s->emitter->methods->calculate(s->emitter, &et)) < 0) {
+    task_release(et.rays);
+    return r;
+  }
+  const ray_caster::task_t* rays = et.rays;
+  if (!rays)
+    return THERMAL_EQUATION_OK;
+  const std::vector<int> f2m = face_mesh_index(scene);
+  const float ray_power = src.power * (float(M_PI) * radius * radius) / s->n_rays;
+  for (int i = 0; i != rays->n_tasks; ++i) {
+    if (!rays->hit_face[i])
+      continue;
+    const math::triangle_t& t = *rays->hit_face[i];
+    // triangle_normal (math/triangle.cpp:114-119) and its side
+    const float vx = t.points[1].x - t.points[0].x, vy = t.points[1].y - t.points[0].y,
+                vz = t.points[1].z - t.points[0].z;
+    const float wx = t.points[2].x - t.points[0].x, wy = t.points[2].y - t.points[0].y,
+                wz = t.points[2].z - t.points[0].z;
+    const float nx = vy * wz - vz * wy, ny = vz * wx - vx * wz, nz = vx * wy - vy * wx;
+    const float side = nx * src.direction.x + ny * src.direction.y + nz * src.direction.z;
+    const int mesh = f2m[(size_t)(rays->hit_face[i] - s->rc_scene.faces)];
+    const subject::material_t& material = mesh_material(scene, mesh);
+    task->absorption[mesh] += (side < 0 ? material.front.absorbance : material.rear.absorbance) * ray_power;
+  }
+  task_release(et.rays);
+  return THERMAL_EQUATION_OK;
+}
+
+static int calculate(thermal_t* s, thermal_equation::task_t* task)
+{
+  if (!s->scene)
+    return -THERMAL_EQUATION_ERROR;
+  if (s->source == 0)  // parallel_rays_cpu.cpp:94-95
+    return THERMAL_EQUATION_OK;
+  const parallel_rays_cpu::source_t src = s->source(s->source_param);
+  return s->fused ? calculate_fused(s, task, src) : calculate_generic(s, task, src);
+}
+
+static const thermal_equation::system_methods_t methods = {
+    (int (*)(thermal_equation::system_t*, void*))&init,
+    (int (*)(thermal_equation::system_t*))&shutdown,
+    (int (*)(thermal_equation::system_t*, subject::scene_t*))&set_scene,
+    (int (*)(thermal_equation::system_t*, thermal_equation::task_t*))&calculate,
+};
+
+thermal_equation::system_t* system_create()
+{
+  thermal_t* s = (thermal_t*)malloc(sizeof(thermal_t));
+  s->methods = &methods;
+  return s;
+}
+
+thermal_equation::system_t* create(parallel_rays_cpu::params_t* params)
+{
+  thermal_equation::system_t* s = system_create();
+  s->methods->init(s, params);
+  return s;
+}
+
+void destroy(thermal_equation::system_t* s)
+{
+  if (!s)
+    return;
+  s->methods->shutdown(s);
+  free(s);
+}
+
+int set_seed(thermal_equation::system_t* system, uint64_t seed)
+{
+  thermal_t* s = as_thermal(system, &methods);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->seed = seed;
+  s->epoch = 0;
+  return FFB_OK;
+}
+
+int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float cells_per_face)
+{
+  thermal_t* s = as_thermal(system, &methods);
+  if (!s)
+    return FFB_ERR_ARG;
+  s->grid = ffb_grid_params{nx, ny, nz, cells_per_face, 1};
+  return FFB_OK;
+}
+
+}  // namespace b200_distant_source
+
+// ===========================================================================
 // CSV export
 // ===========================================================================
 namespace b200_csv_export {

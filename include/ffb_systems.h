@@ -28,6 +28,11 @@
 #include "emission/malley_emission.h"
 #include "form_factors/system.h"
 #include "import_export/csv_export.h"
+#include "subject/system.h"
+#include "thermal_equation/system.h"
+#include "thermal_equation/radiance_cpu.h"
+#include "thermal_equation/parallel_rays_cpu.h"
+#include "emission/parallel_rays_cpu.h"
 #else
 
 namespace math {
@@ -137,13 +142,100 @@ struct system_methods_t {
 #define CSV_EXPORT_OK 0
 #define CSV_EXPORT_FILE_ERROR 31
 
+/* emission/parallel_rays_cpu.h:25-33 */
+namespace parallel_rays_emission_cpu {
+struct task_t : emission::task_t {
+  task_t(int n) : emission::task_t(n) {}
+  math::vec3 direction;  // the reference does not normalise it
+  math::vec3 center;
+  float distance;
+  float radius;
+};
+}  // namespace parallel_rays_emission_cpu
+
+/* subject/system.h:28-86 */
+namespace subject {
+typedef math::triangle_t face_t;
+struct shell_properties_t {
+  float density, heat_capacity, thermal_conductivity, thickness;
+};
+struct optical_properties_t {
+  float specular_reflectance, diffuse_reflectance, absorbance, transmittance, emissivity;
+};
+struct material_t {
+  shell_properties_t shell;
+  optical_properties_t front;
+  optical_properties_t rear;
+  char name[128];
+};
+struct mesh_t {
+  int first_idx;
+  int n_faces;
+  int material_idx;
+};
+struct scene_t {
+  int n_faces;
+  face_t* faces;
+  int n_meshes;
+  mesh_t* meshes;
+  int n_materials;
+  material_t* materials;
+};
+}  // namespace subject
+
+/* thermal_equation/system.h:26-78 */
+namespace thermal_equation {
+struct task_t {
+  const float* temperatures;
+  float* emission;
+  float* absorption;
+};
+struct system_t {
+  const struct system_methods_t* methods;
+};
+#define THERMAL_EQUATION_OK 0
+#define THERMAL_EQUATION_ERROR 400
+struct system_methods_t {
+  int (*init)(system_t* system, void* params);
+  int (*shutdown)(system_t* system);
+  int (*set_scene)(system_t* system, subject::scene_t* scene);
+  int (*calculate)(system_t* system, task_t* task);
+};
+}  // namespace thermal_equation
+
+/* thermal_equation/radiance_cpu.h:29-33 */
+namespace radiance_equation {
+struct params_t {
+  emission::system_t* emitter;
+  int n_rays;
+};
+}  // namespace radiance_equation
+
+/* thermal_equation/parallel_rays_cpu.h:27-40 */
+namespace parallel_rays_cpu {
+struct source_t {
+  float power;  // W/m^2
+  math::vec3 direction;
+};
+struct params_t {
+  int n_rays;
+  emission::system_t* emitter;
+  void* source_param;
+  source_t (*source)(void* param);
+};
+}  // namespace parallel_rays_cpu
+
 #endif  // FFB_USE_REFERENCE_HEADERS
 
 /* Type IDs beside the reference's (ray_caster/system.h:106-109,
- * emission/system.h:92-93, form_factors/system.h:119). */
+ * emission/system.h:92-93, form_factors/system.h:119,
+ * thermal_equation/system.h:71-75). */
 #define RAY_CASTER_B200 5
 #define EMISSION_MALLEY_B200 3
+#define EMISSION_PARALLEL_RAYS_B200 4
 #define FORM_FACTORS_B200 2
+#define THERMAL_EQUATION_RADIANCE_B200 6
+#define THERMAL_EQUATION_DISTANT_SOURCE_B200 7
 
 namespace b200_ray_caster {
 /* Grid nearest-hit caster on the GPU.  set_scene keeps the pointer (the
@@ -193,6 +285,43 @@ int set_seed(form_factors::system_t* system, uint64_t seed);
 int set_flags(form_factors::system_t* system, int flags);
 int set_grid(form_factors::system_t* system, int nx, int ny, int nz, float cells_per_face);
 }  // namespace b200_form_factors
+
+namespace b200_parallel_rays_emission {
+/* Parallel rays from a disc (emission/parallel_rays_cpu.cpp): calculate reads
+ * a parallel_rays_emission_cpu::task_t, emits its n_rays on the GPU (Philox
+ * keyed by seed, call number and ray), copies them into task->rays (malloc'd,
+ * released by ray_caster::task_free) and casts them with the given caster.
+ * set_scene sets and prepares the caster as the reference does. */
+emission::system_t* system_create();
+emission::system_t* create(ray_caster::system_t* caster);
+void destroy(emission::system_t* system);
+int set_seed(emission::system_t* system, uint64_t seed);
+}  // namespace b200_parallel_rays_emission
+
+namespace b200_radiance_equation {
+/* The radiance equation (thermal_equation/radiance_cpu.cpp) for
+ * radiance_equation::params_t.  With a B200 Malley emitter or a NULL emitter
+ * the step runs fused on the GPU (ffb_radiance_step: the scene and grid stay
+ * resident from set_scene; needs meshes covering every face once); with any
+ * other emitter it runs the reference's algorithm over that emitter. */
+thermal_equation::system_t* system_create();
+thermal_equation::system_t* create(radiance_equation::params_t* params);
+void destroy(thermal_equation::system_t* system);
+int set_seed(thermal_equation::system_t* system, uint64_t seed);
+int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float cells_per_face);
+}  // namespace b200_radiance_equation
+
+namespace b200_distant_source {
+/* The distant source of parallel rays (thermal_equation/parallel_rays_cpu.cpp)
+ * for parallel_rays_cpu::params_t.  With a B200 parallel-rays emitter or a
+ * NULL emitter the step runs fused on the GPU (ffb_distant_source_step); with
+ * any other emitter it runs the reference's algorithm over that emitter. */
+thermal_equation::system_t* system_create();
+thermal_equation::system_t* create(parallel_rays_cpu::params_t* params);
+void destroy(thermal_equation::system_t* system);
+int set_seed(thermal_equation::system_t* system, uint64_t seed);
+int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float cells_per_face);
+}  // namespace b200_distant_source
 
 namespace b200_csv_export {
 /* csv_export::export_csv (import_export/csv_export.cpp:26-46) with the text

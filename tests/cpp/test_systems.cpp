@@ -17,6 +17,7 @@
 #include <cstring>
 #include <functional>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ffb_systems.h"
@@ -52,6 +53,17 @@ static math::ray_t ray_to(vec3 o, const math::triangle_t& t)
   vec3 h = sub(c, o);
   return math::ray_t{o, add(o, V(h.x / 2.f, h.y / 2.f, h.z / 2.f))};
 }
+// ray_caster::task_free for a task whose arrays were malloc'd by an emitter
+static void task_free_all(ray_caster::task_t* t)
+{
+  if (!t)
+    return;
+  free(t->ray);
+  free(t->hit_face);
+  free(t->hit_point);
+  free(t);
+}
+
 static bool near_enough(vec3 a, vec3 b)
 {
   vec3 d = sub(a, b);
@@ -392,6 +404,190 @@ static void emission_suite()
   b200_ray_caster::destroy(r);
 }
 
+// ---------------------------------------------------------------------------
+// Ray-traced thermal equations (thermal_equation/radiance_cpu.cpp,
+// thermal_equation/parallel_rays_cpu.cpp) and the parallel-rays emitter.
+// ---------------------------------------------------------------------------
+// The unit cube as 6 meshes of 2 triangles with inward normals.
+static std::vector<math::triangle_t> cube_inward()
+{
+  const vec3 c = V(0.5f, 0.5f, 0.5f);
+  const vec3 q[6][4] = {{V(0, 0, 0), V(1, 0, 0), V(1, 1, 0), V(0, 1, 0)}, {V(0, 0, 1), V(1, 0, 1), V(1, 1, 1), V(0, 1, 1)},
+                        {V(0, 0, 0), V(1, 0, 0), V(1, 0, 1), V(0, 0, 1)}, {V(0, 1, 0), V(1, 1, 0), V(1, 1, 1), V(0, 1, 1)},
+                        {V(0, 0, 0), V(0, 1, 0), V(0, 1, 1), V(0, 0, 1)}, {V(1, 0, 0), V(1, 1, 0), V(1, 1, 1), V(1, 0, 1)}};
+  std::vector<math::triangle_t> out;
+  for (int k = 0; k < 6; ++k) {
+    math::triangle_t t[2] = {T(q[k][0], q[k][1], q[k][2]), T(q[k][0], q[k][2], q[k][3])};
+    for (math::triangle_t& x : t) {
+      const vec3 u = sub(x.points[1], x.points[0]), w = sub(x.points[2], x.points[0]);
+      const vec3 n = V(u.y * w.z - u.z * w.y, u.z * w.x - u.x * w.z, u.x * w.y - u.y * w.x);
+      const vec3 in = sub(c, x.points[0]);
+      if (n.x * in.x + n.y * in.y + n.z * in.z < 0)
+        std::swap(x.points[1], x.points[2]);
+      out.push_back(x);
+    }
+  }
+  return out;
+}
+
+static subject::material_t optics_material(float emis_front, float emis_rear, float abs_front, float abs_rear)
+{
+  subject::material_t m;
+  std::memset(&m, 0, sizeof m);
+  m.front.emissivity = emis_front;
+  m.rear.emissivity = emis_rear;
+  m.front.absorbance = abs_front;
+  m.rear.absorbance = abs_rear;
+  return m;
+}
+
+static bool within(float a, float b, float rel) { return std::fabs(a - b) <= rel * std::fabs(b); }
+
+static parallel_rays_cpu::source_t sun_from_above(void*)
+{
+  parallel_rays_cpu::source_t s;
+  s.power = 1000.f;
+  s.direction = V(0, 0, -1);
+  return s;
+}
+
+static void thermal_suite()
+{
+  std::vector<math::triangle_t> faces = cube_inward();
+  subject::mesh_t meshes[6];
+  for (int m = 0; m < 6; ++m)
+    meshes[m] = subject::mesh_t{2 * m, 2, m % 2};
+  subject::material_t materials[2] = {optics_material(0.9f, 0.f, 0.8f, 0.6f), optics_material(0.5f, 0.f, 0.7f, 0.3f)};
+  subject::scene_t scene = {12, faces.data(), 6, meshes, 2, materials};
+  const float temps[6] = {300, 320, 340, 360, 380, 400};
+  const int n_rays = 200000;
+
+  g_case = "B200 radiance (fused): energy";
+  float em[6] = {0}, ab[6] = {0};
+  {
+    radiance_equation::params_t params = {0, n_rays};
+    thermal_equation::system_t* eq = b200_radiance_equation::create(&params);
+    CHECK(eq->methods->set_scene(eq, &scene) == THERMAL_EQUATION_OK);
+    thermal_equation::task_t task = {temps, em, ab};
+    CHECK(eq->methods->calculate(eq, &task) == THERMAL_EQUATION_OK);
+    float se = 0, sa = 0;
+    for (int m = 0; m < 6; ++m) {
+      se += em[m];
+      sa += ab[m];
+    }
+    // inward emitters only: every ray lands but for the few float rounding
+    // lets through the seams between walls
+    CHECK(se > 0 && sa <= se * 1.0001f && sa > se * 0.998f);
+    b200_radiance_equation::destroy(eq);
+  }
+
+  g_case = "B200 distant source (fused): projected area";
+  {
+    parallel_rays_cpu::params_t params = {n_rays, 0, 0, &sun_from_above};
+    thermal_equation::system_t* eq = b200_distant_source::create(&params);
+    CHECK(eq->methods->set_scene(eq, &scene) == THERMAL_EQUATION_OK);
+    float a[6] = {0}, e[6] = {0};
+    thermal_equation::task_t task = {temps, e, a};
+    CHECK(eq->methods->calculate(eq, &task) == THERMAL_EQUATION_OK);
+    // straight down: only the top (mesh 1, material 1) is hit, from outside,
+    // i.e. on its rear side: 1 m^2 of 1000 W/m^2 at rear absorbance 0.3
+    CHECK(within(a[1], 300.f, 0.02f));
+    CHECK(a[0] == 0 && a[2] == 0 && a[3] == 0 && a[4] == 0 && a[5] == 0);
+    b200_distant_source::destroy(eq);
+  }
+
+  g_case = "B200 parallel-rays emitter";
+  {
+    ray_caster::system_t* r = b200_ray_caster::create();
+    emission::system_t* e = b200_parallel_rays_emission::create(r);
+    ray_caster::scene_t rs = {12, faces.data()};
+    CHECK(e->methods->set_scene(e, &rs) == EMISSION_OK);
+    // the reference's task type has no constructor: it lives in malloc'd
+    // memory (thermal_equation/parallel_rays_cpu.cpp:27-38)
+    alignas(parallel_rays_emission_cpu::task_t) unsigned char storage[sizeof(parallel_rays_emission_cpu::task_t)];
+    parallel_rays_emission_cpu::task_t& task = *reinterpret_cast<parallel_rays_emission_cpu::task_t*>(storage);
+    task.n_rays = 1000;
+    task.rays = 0;
+    task.direction = V(0, 0, -1);
+    task.center = V(0.5f, 0.5f, 0.5f);
+    task.distance = 3.f;
+    task.radius = 0.5f;
+    CHECK(e->methods->calculate(e, &task) == EMISSION_OK);
+    CHECK(task.rays && task.rays->n_tasks == 1000);
+    if (task.rays) {
+      int hits = 0;
+      for (int i = 0; i < 1000; ++i) {
+        const math::ray_t ray = task.rays->ray[i];
+        CHECK(std::fabs(ray.origin.z - 3.5f) < 1e-5f && std::fabs(ray.direction.z - 3.4f) < 1e-5f);
+        hits += task.rays->hit_face[i] == &faces[2] || task.rays->hit_face[i] == &faces[3];
+      }
+      CHECK(hits == 1000);  // a disc of radius 0.5 about the centre lands on the top
+      task_free_all(task.rays);
+    }
+    b200_parallel_rays_emission::destroy(e);
+    b200_ray_caster::destroy(r);
+  }
+
+#ifdef FFB_WITH_REFERENCE
+  g_case = "B200 radiance vs reference radiance_cpu";
+  {
+    ray_caster::system_t* rc = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
+    emission::system_t* me = emission::system_create(EMISSION_MALLEY_CPU, rc);
+    radiance_equation::params_t rp = {me, n_rays};
+    thermal_equation::system_t* ref = radiance_equation::system_create();
+    thermal_equation::system_init(ref, &rp);
+    CHECK(thermal_equation::system_set_scene(ref, &scene) == THERMAL_EQUATION_OK);
+    float rem[6] = {0}, rab[6] = {0};
+    thermal_equation::task_t rt = {temps, rem, rab};
+    CHECK(thermal_equation::system_calculate(ref, &rt) == THERMAL_EQUATION_OK);
+    for (int m = 0; m < 6; ++m) {
+      CHECK(em[m] == rem[m]);
+      CHECK(within(ab[m], rab[m], 0.03f));
+    }
+    // the B200 equation over the reference's emitter (the non-fused path)
+    radiance_equation::params_t gp = {me, n_rays};
+    thermal_equation::system_t* mixed = b200_radiance_equation::create(&gp);
+    CHECK(mixed->methods->set_scene(mixed, &scene) == THERMAL_EQUATION_OK);
+    float gem[6] = {0}, gab[6] = {0};
+    thermal_equation::task_t gt = {temps, gem, gab};
+    CHECK(mixed->methods->calculate(mixed, &gt) == THERMAL_EQUATION_OK);
+    for (int m = 0; m < 6; ++m) {
+      CHECK(gem[m] == rem[m]);
+      CHECK(within(gab[m], rab[m], 0.03f));
+    }
+    b200_radiance_equation::destroy(mixed);
+    thermal_equation::system_free(ref);
+    emission::system_free(me);
+    ray_caster::system_free(rc);
+  }
+
+  g_case = "B200 distant source vs reference parallel_rays_cpu";
+  {
+    ray_caster::system_t* rc = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
+    emission::system_t* pe = emission::system_create(EMISSION_PARALLEL_RAYS_CPU, rc);
+    parallel_rays_cpu::params_t rp = {n_rays, pe, 0, &sun_from_above};
+    thermal_equation::system_t* ref = parallel_rays_cpu::system_create();
+    thermal_equation::system_init(ref, &rp);
+    CHECK(thermal_equation::system_set_scene(ref, &scene) == THERMAL_EQUATION_OK);
+    float ra[6] = {0}, re[6] = {0};
+    thermal_equation::task_t rt = {temps, re, ra};
+    CHECK(thermal_equation::system_calculate(ref, &rt) == THERMAL_EQUATION_OK);
+    CHECK(within(ra[1], 300.f, 0.02f));
+    // the B200 equation over the reference's emitter
+    thermal_equation::system_t* mixed = b200_distant_source::create(&rp);
+    CHECK(mixed->methods->set_scene(mixed, &scene) == THERMAL_EQUATION_OK);
+    float ga[6] = {0}, ge[6] = {0};
+    thermal_equation::task_t gt = {temps, ge, ga};
+    CHECK(mixed->methods->calculate(mixed, &gt) == THERMAL_EQUATION_OK);
+    CHECK(within(ga[1], ra[1], 0.03f));
+    b200_distant_source::destroy(mixed);
+    thermal_equation::system_free(ref);
+    emission::system_free(pe);
+    ray_caster::system_free(rc);
+  }
+#endif
+}
+
 // CSV export (import_export/csv_export.cpp:26-46): the B200 export writes
 // the reference's bytes; with the reference built in, the two files are
 // compared whole.
@@ -437,6 +633,7 @@ static void csv_suite()
 int main()
 {
   csv_suite();
+  thermal_suite();
   for (const Caster& c : casters())
     ray_caster_suite(c);
   emission_suite();
