@@ -14,10 +14,13 @@
 #include <string>
 #include <vector>
 
+#include <map>
+
 #include <cuda_runtime.h>
 
 #include "ffb.h"
 #include "ffb_csv.cuh"
+#include "ffb_obj.cuh"
 #include "ffb_trace.cuh"
 
 using namespace ffb;
@@ -103,6 +106,12 @@ struct ffb_ctx {
   DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
   DevBuf power_tab, absorb;                     // radiance sink
+  // OBJ import: the text and its line tables, the parsed geometry
+  DevBuf obj_text, obj_chunk, obj_chunk_off, obj_starts, obj_flags, obj_ords, obj_vertices, obj_face_idx,
+      obj_face_line, obj_special, obj_ranges, obj_faces, obj_err;
+  std::vector<ffb_mesh> obj_meshes;
+  std::vector<ffb_material> obj_materials;
+  long long obj_n_faces = -1;  // faces of the last successful parse
   void* csv_pinned[2] = {nullptr, nullptr};     // double-buffered text on its way to a file
   size_t csv_pinned_cap[2] = {0, 0};
   void* pinned = nullptr;
@@ -566,7 +575,9 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
                     &c->scan_sums, &c->chunks,      &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
                     &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
-                    &c->power_tab, &c->absorb};
+                    &c->power_tab, &c->absorb, &c->obj_text, &c->obj_chunk, &c->obj_chunk_off,
+                    &c->obj_starts, &c->obj_flags, &c->obj_ords, &c->obj_vertices, &c->obj_face_idx,
+                    &c->obj_face_line, &c->obj_special, &c->obj_ranges, &c->obj_faces, &c->obj_err};
   for (DevBuf* b : bufs)
     release(c, *b);
   cudaStreamSynchronize(c->stream);
@@ -1083,6 +1094,348 @@ extern "C" int ffb_parallel_rays(ffb_ctx* c, const ffb_disc_source* src, long lo
     FFB_CUDA(cudaStreamSynchronize(c->stream));
   }
   return FFB_OK;
+}
+
+// ===========================================================================
+// Wavefront OBJ import (import_export/obj_import.cpp:44-340)
+// ===========================================================================
+namespace {
+
+constexpr int kObjFileError = 21, kObjFormatError = 22, kObjMaterialNotDefined = 23,
+              kObjMaterialNotEnough = 24, kObjMaterialInvalidValue = 25;
+
+// subject::black_body (subject/objects.cpp:157-188)
+ffb_material black_body()
+{
+  ffb_material m;
+  memset(&m, 0, sizeof m);
+  m.shell_density = m.shell_heat_capacity = m.shell_thermal_conductivity = m.shell_thickness = 1.f;
+  m.front_absorbance = m.front_emissivity = 1.f;
+  m.rear_absorbance = m.rear_emissivity = 1.f;
+  strcpy(m.name, "black_body");
+  return m;
+}
+
+bool getline_str(FILE* f, std::string& out)
+{
+  out.clear();
+  int ch;
+  bool any = false;
+  while ((ch = fgetc(f)) != EOF) {
+    any = true;
+    if (ch == '\n')
+      return true;
+    out.push_back((char)ch);
+  }
+  return any;
+}
+
+// obj_import::material_lib (obj_import.cpp:44-164), host side: a material
+// library is a handful of lines.  Returns 0 or the reference's negative code.
+int material_lib(const char* filename, std::vector<ffb_material>& materials, std::map<std::string, int>& library)
+{
+  FILE* file = fopen(filename, "rb");
+  if (!file)
+    return -kObjFileError;
+  static const char* kNames[14] = {"shell.density", "shell.heat_capacity", "shell.thermal_conductivity",
+                                   "shell.thickness", "front.specular_reflectance", "front.diffuse_reflectance",
+                                   "front.absorbance", "front.transmittance", "front.emissivity",
+                                   "rear.specular_reflectance", "rear.diffuse_reflectance", "rear.absorbance",
+                                   "rear.transmittance", "rear.emissivity"};
+  std::string str;
+  int rc = 0;
+  while (rc == 0 && getline_str(file, str)) {
+    if (str.empty() || str[0] == '#')
+      continue;
+    if (str[0] != 'n')
+      continue;
+    if (strncmp("newmtl", str.c_str(), 6) != 0) {
+      rc = -kObjFormatError;
+      break;
+    }
+    const std::string name = str.size() > 7 ? str.substr(7) : std::string();
+    ffb_material m;
+    memset(&m, 0, sizeof m);
+    if (name.length() >= sizeof(m.name)) {
+      rc = -kObjFormatError;
+      break;
+    }
+    memcpy(m.name, name.c_str(), name.length());
+    float* fields[14] = {&m.shell_density, &m.shell_heat_capacity, &m.shell_thermal_conductivity,
+                         &m.shell_thickness, &m.front_specular_reflectance, &m.front_diffuse_reflectance,
+                         &m.front_absorbance, &m.front_transmittance, &m.front_emissivity,
+                         &m.rear_specular_reflectance, &m.rear_diffuse_reflectance, &m.rear_absorbance,
+                         &m.rear_transmittance, &m.rear_emissivity};
+    bool parsed[14] = {false};
+    int n_parsed = 0;
+    // as the reference: getline first, then the count test (the line after
+    // the fourteenth property is consumed)
+    while (getline_str(file, str) && n_parsed != 14) {
+      if (str.empty())
+        break;
+      if (str[0] == '#')
+        continue;
+      const std::string::size_type pos = str.find_first_of(" \t");
+      if (pos == std::string::npos || pos + 1 >= str.length()) {
+        rc = -kObjFormatError;
+        break;
+      }
+      const std::string prop = str.substr(0, pos), value = str.substr(pos + 1);
+      int k = 0;
+      while (k < 14 && prop != kNames[k])
+        ++k;
+      if (k == 14)
+        continue;  // unknown property: skipped
+      if (sscanf(value.c_str(), "%f", fields[k]) != 1) {
+        rc = -kObjMaterialInvalidValue;
+        break;
+      }
+      if (!parsed[k]) {
+        parsed[k] = true;
+        ++n_parsed;
+      }
+    }
+    if (rc)
+      break;
+    if (n_parsed != 14) {
+      rc = -kObjMaterialNotEnough;
+      break;
+    }
+    materials.push_back(m);
+    library[name] = (int)materials.size() - 1;
+  }
+  fclose(file);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int ffb_obj_parse(ffb_ctx* c, const char* text, unsigned long long n_bytes, const char* filename,
+                             ffb_obj_info* info)
+{
+  FFB_TRY(check_ctx(c));
+  if (!info || (n_bytes && !text))
+    return fail(FFB_ERR_ARG, "bad OBJ arguments");
+  if (n_bytes >= 0xFFFFFFF0ull)
+    return fail(FFB_ERR_TOO_LARGE, "OBJ text of %llu bytes; at most 4 GiB", n_bytes);
+  memset(info, 0, sizeof *info);
+  c->obj_n_faces = -1;
+  c->obj_meshes.clear();
+  c->obj_materials.clear();
+  const uint32_t n = (uint32_t)n_bytes;
+  // the text, and its newlines per chunk
+  FFB_TRY(upload(c, c->obj_text, text, n));
+  const uint32_t chunks = (n + obj::kObjChunk - 1) / obj::kObjChunk;
+  FFB_TRY(ensure(c, c->obj_chunk, sizeof(uint32_t) * (size_t)std::max(chunks, 1u)));
+  FFB_TRY(ensure(c, c->obj_chunk_off, sizeof(uint32_t) * (size_t)(chunks + 1)));
+  uint32_t n_nl = 0;
+  if (chunks) {
+    obj::k_obj_nl_count<<<chunks, obj::kObjThreads, 0, c->stream>>>(dptr<char>(c->obj_text), n,
+                                                                      dptr<uint32_t>(c->obj_chunk));
+    FFB_CUDA(cudaGetLastError());
+    FFB_TRY(scan(c, dptr<uint32_t>(c->obj_chunk), (int)chunks, dptr<uint32_t>(c->obj_chunk_off)));
+    FFB_CUDA(cudaMemcpyAsync(&n_nl, dptr<uint32_t>(c->obj_chunk_off) + chunks, sizeof n_nl,
+                             cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  const uint32_t n_lines = n_nl + ((n > 0 && text[n - 1] != '\n') ? 1u : 0u);
+  FFB_TRY(ensure(c, c->obj_starts, sizeof(uint32_t) * ((size_t)n_nl + 2)));
+  if (chunks) {
+    obj::k_obj_line_starts<<<chunks, obj::kObjThreads, 0, c->stream>>>(
+        dptr<char>(c->obj_text), n, dptr<uint32_t>(c->obj_chunk_off), dptr<uint32_t>(c->obj_starts));
+    FFB_CUDA(cudaGetLastError());
+  }
+  const uint32_t sentinel = n + 1;  // the last line ends at n
+  FFB_CUDA(cudaMemcpyAsync(dptr<uint32_t>(c->obj_starts) + n_nl + 1, &sentinel, sizeof sentinel,
+                           cudaMemcpyHostToDevice, c->stream));
+  // classes and ordinals
+  const size_t L = std::max<size_t>(n_lines, 1);
+  FFB_TRY(ensure(c, c->obj_flags, sizeof(uint32_t) * 3 * L));
+  FFB_TRY(ensure(c, c->obj_ords, sizeof(uint32_t) * 3 * (L + 1)));
+  uint32_t* is_v = dptr<uint32_t>(c->obj_flags);
+  uint32_t* is_f = is_v + L;
+  uint32_t* is_s = is_f + L;
+  uint32_t* vord = dptr<uint32_t>(c->obj_ords);
+  uint32_t* ford = vord + (L + 1);
+  uint32_t* sord = ford + (L + 1);
+  uint32_t counts[3] = {0, 0, 0};
+  if (n_lines) {
+    obj::k_obj_classify<<<grid_blocks(n_lines, 256, c->n_sm * 16), 256, 0, c->stream>>>(
+        dptr<char>(c->obj_text), dptr<uint32_t>(c->obj_starts), n_lines, is_v, is_f, is_s);
+    FFB_CUDA(cudaGetLastError());
+    FFB_TRY(scan(c, is_v, (int)n_lines, vord));
+    FFB_TRY(scan(c, is_f, (int)n_lines, ford));
+    FFB_TRY(scan(c, is_s, (int)n_lines, sord));
+    FFB_CUDA(cudaMemcpyAsync(&counts[0], vord + n_lines, 4, cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaMemcpyAsync(&counts[1], ford + n_lines, 4, cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaMemcpyAsync(&counts[2], sord + n_lines, 4, cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  const uint32_t n_vertices = counts[0], n_faces = counts[1], n_special = counts[2];
+  // parse
+  FFB_TRY(ensure(c, c->obj_vertices, sizeof(float) * 3 * std::max<size_t>(n_vertices, 1)));
+  FFB_TRY(ensure(c, c->obj_face_idx, sizeof(int32_t) * 3 * std::max<size_t>(n_faces, 1)));
+  FFB_TRY(ensure(c, c->obj_face_line, sizeof(uint32_t) * std::max<size_t>(n_faces, 1)));
+  FFB_TRY(ensure(c, c->obj_special, sizeof(uint32_t) * 2 * std::max<size_t>(n_special, 1)));
+  FFB_TRY(ensure(c, c->obj_ranges, sizeof(uint32_t) * 2 * std::max<size_t>(n_special, 1)));
+  FFB_TRY(ensure(c, c->obj_faces, sizeof(float) * 9 * std::max<size_t>(n_faces, 1)));
+  FFB_TRY(ensure(c, c->obj_err, sizeof(unsigned long long)));
+  FFB_CUDA(cudaMemsetAsync(c->obj_err.ptr, 0xFF, sizeof(unsigned long long), c->stream));
+  uint32_t* sp_line = dptr<uint32_t>(c->obj_special);
+  uint32_t* sp_faces = sp_line + std::max<uint32_t>(n_special, 1);
+  if (n_lines) {
+    obj::k_obj_parse<<<grid_blocks(n_lines, 256, c->n_sm * 16), 256, 0, c->stream>>>(
+        dptr<char>(c->obj_text), dptr<uint32_t>(c->obj_starts), n_lines, is_v, vord, is_f, ford, is_s, sord,
+        dptr<float>(c->obj_vertices), dptr<int32_t>(c->obj_face_idx), dptr<uint32_t>(c->obj_face_line), sp_line,
+        sp_faces, dptr<unsigned long long>(c->obj_err));
+    FFB_CUDA(cudaGetLastError());
+  }
+  if (n_faces) {
+    obj::k_obj_gather<<<grid_blocks(n_faces, 256, c->n_sm * 16), 256, 0, c->stream>>>(
+        dptr<float>(c->obj_vertices), n_vertices, dptr<int32_t>(c->obj_face_idx), dptr<uint32_t>(c->obj_face_line),
+        n_faces, dptr<float>(c->obj_faces), dptr<unsigned long long>(c->obj_err));
+    FFB_CUDA(cudaGetLastError());
+  }
+  std::vector<uint32_t> ranges(2 * (size_t)n_special), sp_count((size_t)n_special), sp_lines((size_t)n_special);
+  if (n_special) {
+    obj::k_obj_special_ranges<<<grid_blocks(n_special, 256, c->n_sm * 4), 256, 0, c->stream>>>(
+        dptr<uint32_t>(c->obj_starts), sp_line, n_special, dptr<uint32_t>(c->obj_ranges));
+    FFB_CUDA(cudaGetLastError());
+    FFB_CUDA(cudaMemcpyAsync(ranges.data(), c->obj_ranges.ptr, sizeof(uint32_t) * ranges.size(),
+                             cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaMemcpyAsync(sp_count.data(), sp_faces, sizeof(uint32_t) * n_special, cudaMemcpyDeviceToHost,
+                             c->stream));
+    FFB_CUDA(cudaMemcpyAsync(sp_lines.data(), sp_line, sizeof(uint32_t) * n_special, cudaMemcpyDeviceToHost,
+                             c->stream));
+  }
+  unsigned long long dev_err = 0;
+  FFB_CUDA(cudaMemcpyAsync(&dev_err, c->obj_err.ptr, sizeof dev_err, cudaMemcpyDeviceToHost, c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  // special lines in file order (obj_import.cpp:228-300), stopping at the
+  // first error; a geometry error on an earlier line wins
+  const unsigned long long dev_line = dev_err >> 8;
+  int status = 0;
+  unsigned long long err_line = ~0ull;
+  std::vector<ffb_mesh> meshes;
+  std::vector<ffb_material> materials;
+  std::map<std::string, int> library;
+  for (uint32_t i = 0; i < n_special && status == 0; ++i) {
+    if (sp_lines[i] > dev_line)
+      break;
+    const std::string str(text + ranges[2 * i], text + ranges[2 * i + 1]);
+    int r = 0;
+    switch (str[0]) {
+    case 'o':
+    case 'g': {
+      ffb_mesh m = {(int)sp_count[i], 0, 0};
+      if (!meshes.empty())
+        meshes.back().n_faces = (int)sp_count[i] - meshes.back().first_idx;
+      meshes.push_back(m);
+    } break;
+    case 'u': {
+      const std::string::size_type pos = str.find_first_of(" \t");
+      if (pos == std::string::npos || str.substr(0, pos) != "usemtl") {
+        r = -kObjFormatError;
+        break;
+      }
+      const auto found = library.find(str.substr(pos + 1));
+      if (found == library.end())
+        r = -kObjMaterialNotDefined;
+      else if (meshes.empty())
+        r = -kObjFormatError;  // usemtl before any object (undefined in the reference)
+      else
+        meshes.back().material_idx = found->second;
+    } break;
+    case 'm': {
+      if (strncmp("mtllib", str.c_str(), 6) != 0) {
+        r = -kObjFormatError;
+        break;
+      }
+      // the library path as obj_import.cpp:263-277 builds it
+      const std::string library_name = str.size() > 7 ? str.substr(7) : std::string();
+      std::string library_path = library_name;
+      if (library_name.find("/\\") > library_name.length()) {
+        std::string base_name(filename ? filename : "");
+        const size_t dir_pos = base_name.find_last_of("/\\");
+        base_name = dir_pos < base_name.length() ? base_name.substr(0, dir_pos + 1) : std::string();
+        library_path = base_name + library_name;
+      }
+      r = material_lib(library_path.c_str(), materials, library);
+    } break;
+    }
+    if (r < 0) {
+      status = r;
+      err_line = sp_lines[i];
+    }
+  }
+  if (dev_err != ~0ull && dev_line < err_line) {
+    status = -(int)(dev_err & 0xFF);
+    err_line = dev_line;
+  }
+  info->n_vertices = (int)n_vertices;
+  info->n_faces = (int)n_faces;
+  info->status = status;
+  info->error_line = status ? (int)(err_line + 1) : 0;
+  if (status)
+    return fail(FFB_ERR_FORMAT, "OBJ import failed with status %d at line %d", status, info->error_line);
+  // meshes and materials as obj_import.cpp:320-340 finish them
+  if (meshes.empty())
+    meshes.push_back(ffb_mesh{0, (int)n_faces, 0});
+  else
+    meshes.back().n_faces = (int)n_faces - meshes.back().first_idx;
+  if (materials.empty())
+    materials.push_back(black_body());
+  info->n_meshes = (int)meshes.size();
+  info->n_materials = (int)materials.size();
+  c->obj_meshes = meshes;
+  c->obj_materials = materials;
+  c->obj_n_faces = n_faces;
+  return FFB_OK;
+}
+
+extern "C" int ffb_obj_load(ffb_ctx* c, const char* filename, ffb_obj_info* info)
+{
+  FFB_TRY(check_ctx(c));
+  if (!filename || !info)
+    return fail(FFB_ERR_ARG, "bad OBJ arguments");
+  memset(info, 0, sizeof *info);
+  FILE* f = fopen(filename, "rb");
+  if (!f) {
+    info->status = -kObjFileError;
+    return fail(FFB_ERR_FILE, "cannot open %s", filename);
+  }
+  std::vector<char> text;
+  char buf[1 << 16];
+  size_t k;
+  while ((k = fread(buf, 1, sizeof buf, f)) > 0)
+    text.insert(text.end(), buf, buf + k);
+  fclose(f);
+  return ffb_obj_parse(c, text.data(), text.size(), filename, info);
+}
+
+extern "C" int ffb_obj_result(ffb_ctx* c, float* faces9, ffb_mesh* meshes, ffb_material* materials)
+{
+  FFB_TRY(check_ctx(c));
+  if (c->obj_n_faces < 0)
+    return fail(FFB_ERR_NO_SCENE, "no parsed OBJ scene");
+  if (faces9 && c->obj_n_faces) {
+    FFB_CUDA(cudaMemcpyAsync(faces9, c->obj_faces.ptr, sizeof(float) * 9 * (size_t)c->obj_n_faces, cudaMemcpyDefault,
+                             c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (meshes)
+    memcpy(meshes, c->obj_meshes.data(), sizeof(ffb_mesh) * c->obj_meshes.size());
+  if (materials)
+    memcpy(materials, c->obj_materials.data(), sizeof(ffb_material) * c->obj_materials.size());
+  return FFB_OK;
+}
+
+extern "C" int ffb_obj_scene_set(ffb_ctx* c)
+{
+  FFB_TRY(check_ctx(c));
+  if (c->obj_n_faces < 0)
+    return fail(FFB_ERR_NO_SCENE, "no parsed OBJ scene");
+  return ffb_scene_set(c, dptr<float>(c->obj_faces), (int)c->obj_n_faces);
 }
 
 // ===========================================================================

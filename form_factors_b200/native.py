@@ -18,10 +18,12 @@ HEADER = os.path.join(ROOT, "include", "ffb.h")
 
 FFB_OK = 0
 FFB_EMIT_REF_NORMAL = 1
+FFB_ERR_FILE = -309
+FFB_ERR_FORMAT = -310
 ERRORS = {
     -301: "FFB_ERR_ARG", -302: "FFB_ERR_CUDA", -303: "FFB_ERR_NO_SCENE", -304: "FFB_ERR_NO_GRID",
     -305: "FFB_ERR_NO_MEMORY", -306: "FFB_ERR_TOO_LARGE", -307: "FFB_ERR_NO_DEVICE", -308: "FFB_ERR_TIMEOUT",
-    -309: "FFB_ERR_FILE",
+    -309: "FFB_ERR_FILE", -310: "FFB_ERR_FORMAT",
 }
 
 
@@ -55,6 +57,15 @@ class DiscSource(C.Structure):
     @classmethod
     def make(cls, direction, center, distance, radius):
         return cls((C.c_float * 3)(*direction), (C.c_float * 3)(*center), float(distance), float(radius))
+
+
+class ObjInfo(C.Structure):
+    _fields_ = [("n_vertices", C.c_int), ("n_faces", C.c_int), ("n_meshes", C.c_int), ("n_materials", C.c_int),
+                ("status", C.c_int), ("error_line", C.c_int)]
+
+
+# subject::material_t / ffb_material: 14 floats (shell, front, rear) and a name
+MATERIAL_DTYPE = np.dtype([("props", "<f4", (14,)), ("name", "S128")])
 
 
 class Mesh(C.Structure):
@@ -138,6 +149,10 @@ def load(path=LIB_PATH):
         "ffb_csv_export_counts": (i32, [vp, C.c_char_p, vp, vp, i32]),
         "ffb_stats_get": (i32, [vp, C.POINTER(Stats)]),
         "ffb_radiance_absorption": (i32, [vp, vp, vp, vp, vp, vp, i32, u64, u32, i32, vp]),
+        "ffb_obj_parse": (i32, [vp, C.c_char_p, C.c_ulonglong, C.c_char_p, C.POINTER(ObjInfo)]),
+        "ffb_obj_load": (i32, [vp, C.c_char_p, C.POINTER(ObjInfo)]),
+        "ffb_obj_result": (i32, [vp, vp, vp, vp]),
+        "ffb_obj_scene_set": (i32, [vp]),
         "ffb_emit_parallel": (i32, [vp, C.POINTER(DiscSource), i64, u64, u32, vp]),
         "ffb_parallel_rays": (i32, [vp, C.POINTER(DiscSource), i64, u64, u32, vp]),
         "ffb_bounding_sphere": (i32, [vp, i32, vp, C.POINTER(C.c_float)]),
@@ -400,6 +415,39 @@ class Context:
             _check(self._lib.ffb_csv_export(self._h, name, _ptr(ff), n))
         else:
             _check(self._lib.ffb_csv_export_counts(self._h, name, _ptr(counts), _ptr(outgoing), n))
+
+    def _obj_info(self, rc, info):
+        d = {k: getattr(info, k) for k, _ in ObjInfo._fields_}
+        if rc < 0 and rc not in (FFB_ERR_FORMAT, FFB_ERR_FILE):
+            _check(rc)
+        return d
+
+    def obj_parse(self, text, filename=None):
+        """obj_import::scene on OBJ text (bytes) with the geometry parsed on
+        the GPU; `filename` locates mtllib files.  Returns the info dict
+        (status: the reference's return code, error_line)."""
+        info = ObjInfo()
+        rc = self._lib.ffb_obj_parse(self._h, text, len(text), os.fsencode(filename) if filename else None,
+                                     C.byref(info))
+        return self._obj_info(rc, info)
+
+    def obj_load(self, filename):
+        info = ObjInfo()
+        rc = self._lib.ffb_obj_load(self._h, os.fsencode(filename), C.byref(info))
+        return self._obj_info(rc, info)
+
+    def obj_result(self, info):
+        """(faces (n, 9) float32, meshes (m, 3) int32, materials) of the last parse."""
+        faces = np.empty((info["n_faces"], 9), np.float32)
+        meshes = np.empty((info["n_meshes"], 3), np.int32)
+        materials = np.zeros(info["n_materials"], MATERIAL_DTYPE)
+        _check(self._lib.ffb_obj_result(self._h, _ptr(faces), _ptr(meshes), materials.ctypes.data))
+        return faces, meshes, materials
+
+    def obj_scene_set(self, n_faces):
+        """The parsed faces become this context's scene (device to device)."""
+        _check(self._lib.ffb_obj_scene_set(self._h))
+        self.n_faces = int(n_faces)
 
     def radiance_absorption(self, front, rear, power_front, power_rear, face_to_mesh, n_meshes, seed, epoch=0,
                             flags=0):

@@ -39,6 +39,7 @@ extern "C" {
 #define FFB_ERR_NO_DEVICE (-307) /* no CUDA device / not an sm_100 device */
 #define FFB_ERR_TIMEOUT (-308)   /* a wait ended before the work finished */
 #define FFB_ERR_FILE (-309)      /* a file could not be opened or written */
+#define FFB_ERR_FORMAT (-310)    /* malformed input file (see the call's status) */
 
 /* Emission flag: rotate +z towards the raw cross-product normal, as the
  * reference's emission/malley_cpu.cpp:125-129 does.  Without it the normal is
@@ -291,6 +292,43 @@ int ffb_radiance_step(ffb_ctx* ctx, const float* faces9, int n_faces, const ffb_
 int ffb_distant_source_step(ffb_ctx* ctx, const float* faces9, int n_faces, const ffb_mesh* meshes, int n_meshes,
                             const ffb_optics* materials, int n_materials, int n_rays, float power,
                             const float* direction3, uint64_t seed, uint32_t epoch, float* absorption);
+
+/* subject::material_t (subject/system.h:31-59), layout-identical. */
+typedef struct {
+  float shell_density, shell_heat_capacity, shell_thermal_conductivity, shell_thickness;
+  float front_specular_reflectance, front_diffuse_reflectance, front_absorbance, front_transmittance, front_emissivity;
+  float rear_specular_reflectance, rear_diffuse_reflectance, rear_absorbance, rear_transmittance, rear_emissivity;
+  char name[128];
+} ffb_material;
+
+typedef struct {
+  int n_vertices, n_faces, n_meshes, n_materials;
+  int status;     /* what obj_import::scene returns: 0 or -OBJ_IMPORT_* (-21 file, -22 format, -23..-25 material) */
+  int error_line; /* 1-based line of the first error, 0 when none */
+} ffb_obj_info;
+
+/* obj_import::scene (import_export/obj_import.cpp:167-340) with the geometry
+ * parsed on the GPU: the text goes to the device once; lines, vertex ("v x y
+ * z", sscanf "%f" = correctly rounded strtof) and face lines ("f" in the
+ * reference's three formats) are split, converted and gathered into
+ * triangles by kernels; the few object, usemtl and mtllib lines (and the
+ * material library itself) are handled on the host in file order.  The
+ * result is the reference's: faces, meshes (o/g), materials (or the black
+ * body).  ffb_obj_parse takes the text in memory (filename: where mtllib
+ * paths are resolved from, may be NULL); ffb_obj_load reads the file.
+ * FFB_ERR_FORMAT / FFB_ERR_FILE on failure with info->status the reference's
+ * code and info->error_line the line where the reference would stop.  A face
+ * index outside the vertex list (undefined in the reference) and usemtl
+ * before any object are format errors here. */
+int ffb_obj_parse(ffb_ctx* ctx, const char* text, unsigned long long n_bytes, const char* filename,
+                  ffb_obj_info* info);
+int ffb_obj_load(ffb_ctx* ctx, const char* filename, ffb_obj_info* info);
+/* The parsed scene: faces9 (host or device, 9 * n_faces floats), meshes
+ * (n_meshes), materials (n_materials); any may be NULL. */
+int ffb_obj_result(ffb_ctx* ctx, float* faces9, ffb_mesh* meshes, ffb_material* materials);
+/* Makes the parsed faces the context's scene without a copy through the host
+ * (then ffb_grid_build). */
+int ffb_obj_scene_set(ffb_ctx* ctx);
 
 /* CSV text of an n x n form-factor matrix, byte for byte the file of
  * csv_export::export_csv (import_export/csv_export.cpp:26-46): row i is the n

@@ -18,6 +18,7 @@
 //   parallel_rays_cpu::system_create / calculate              thermal_equation/parallel_rays_cpu.cpp:66-131
 //   parallel_rays_emission_cpu::system_create                 emission/parallel_rays_cpu.cpp:88-138
 //   math::triangles_bsphere                                   math/triangle.cpp:361-384
+//   obj_import::scene                                         import_export/obj_import.cpp:167-340
 #include "ray_caster/system.h"
 #include "import_export/csv_export.h"
 #include "subject/system.h"
@@ -25,6 +26,7 @@
 #include "thermal_equation/radiance_cpu.h"
 #include "thermal_equation/parallel_rays_cpu.h"
 #include "emission/parallel_rays_cpu.h"
+#include "import_export/obj_import.h"
 #include "emission/system.h"
 #include "emission/malley_emission.h"
 #include "form_factors/system.h"
@@ -382,6 +384,31 @@ int ffref_parallel_rays(int type, int n_faces, const float* faces9, int n_meshes
   ray_caster::system_free(caster);
   return r;
 }
+
+// obj_import::scene: status, and on success the scene (release with
+// ffref_obj_free); counts3 = faces, meshes, materials.
+int ffref_obj_load(const char* filename, void** scene_out, int* counts3)
+{
+  subject::scene_t* scene = 0;
+  const int r = obj_import::scene(filename, &scene);
+  *scene_out = scene;
+  if (r == 0 && scene) {
+    counts3[0] = scene->n_faces;
+    counts3[1] = scene->n_meshes;
+    counts3[2] = scene->n_materials;
+  }
+  return r;
+}
+
+void ffref_obj_copy(void* handle, float* faces9, int* meshes3, void* materials)
+{
+  subject::scene_t* s = (subject::scene_t*)handle;
+  std::memcpy(faces9, s->faces, sizeof(subject::face_t) * (size_t)s->n_faces);
+  std::memcpy(meshes3, s->meshes, sizeof(subject::mesh_t) * (size_t)s->n_meshes);
+  std::memcpy(materials, s->materials, sizeof(subject::material_t) * (size_t)s->n_materials);
+}
+
+void ffref_obj_free(void* handle) { subject::scene_free((subject::scene_t*)handle); }
 
 void ffref_bsphere(int n_faces, const float* faces9, float* center3, float* radius)
 {

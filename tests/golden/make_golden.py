@@ -22,7 +22,10 @@ Fixtures (compressed .npz, all seeded):
                   digit, count / outgoing ratios, random magnitudes) and the
                   bytes csv_export::export_csv writes for it
 
-`python tests/golden/make_golden.py csv` writes csv_ref.npz only.
+  obj_ref.npz     a generated OBJ scene (mixed number and face styles, objects,
+                  a material library) and what obj_import::scene returns for it
+
+`python tests/golden/make_golden.py csv` (or `obj`) writes that fixture only.
 """
 import os
 import sys
@@ -102,7 +105,29 @@ def csv_fixture(ref, rng):
     np.savez_compressed(os.path.join(HERE, "csv_ref.npz"), ff=ff, text=np.frombuffer(text, np.uint8))
 
 
+def obj_fixture(ref):
+    import tempfile
+    import obj_text as O
+    faces = scenes.clutter(60, 0.1, seed=12, enclosure_cells=2)
+    meshes = [(0, 20), (20, 30), (50, len(faces) - 50)]
+    rng = np.random.default_rng(77)
+    mtl = O.mtl_text(["alpha", "beta"], rng).encode()
+    obj = O.obj_text(faces, meshes, ["alpha", "beta"], mtllib="golden.mtl", seed=78)
+    with tempfile.TemporaryDirectory() as d:
+        open(os.path.join(d, "golden.mtl"), "wb").write(mtl)
+        path = os.path.join(d, "golden.obj")
+        open(path, "wb").write(obj)
+        rc, f, m, mats = ref.obj_scene(path)
+    assert rc == 0, rc
+    np.savez_compressed(os.path.join(HERE, "obj_ref.npz"), obj=np.frombuffer(obj, np.uint8),
+                        mtl=np.frombuffer(mtl, np.uint8), faces=f, meshes=m, materials=mats)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "obj":
+        obj_fixture(Reference())
+        print("obj_ref.npz written to", HERE)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "csv":
         csv_fixture(Reference(), np.random.default_rng(20261204))
         print("csv_ref.npz written to", HERE)
@@ -194,6 +219,7 @@ def main():
     ff["box_ff"] = mat
     np.savez_compressed(os.path.join(HERE, "ff_ref.npz"), **ff)
     csv_fixture(ref, np.random.default_rng(20261204))
+    obj_fixture(ref)
     print("fixtures written to", HERE)
 
 

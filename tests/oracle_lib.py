@@ -193,7 +193,26 @@ class Reference:
                                             C.c_float, _f32p, _f32p]
         lib.ffref_parallel_rays.restype = C.c_int
         lib.ffref_bsphere.argtypes = [C.c_int, _f32p, _f32p, C.POINTER(C.c_float)]
+        lib.ffref_obj_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), _i32p]
+        lib.ffref_obj_load.restype = C.c_int
+        lib.ffref_obj_copy.argtypes = [C.c_void_p, _f32p, _i32p, C.c_void_p]
+        lib.ffref_obj_free.argtypes = [C.c_void_p]
         self.lib = lib
+
+    def obj_scene(self, filename):
+        """obj_import::scene: (status, faces (n, 9), meshes (m, 3), materials
+        as raw 184-byte records)."""
+        h = C.c_void_p()
+        counts = np.zeros(3, np.int32)
+        rc = self.lib.ffref_obj_load(os.fsencode(filename), C.byref(h), counts)
+        if rc != 0 or not h.value:
+            return rc, None, None, None
+        faces = np.zeros((counts[0], 9), np.float32)
+        meshes = np.zeros((counts[1], 3), np.int32)
+        materials = np.zeros(counts[2] * 184, np.uint8)
+        self.lib.ffref_obj_copy(h, faces, meshes, materials.ctypes.data)
+        self.lib.ffref_obj_free(h)
+        return rc, faces, meshes, materials
 
     def radiance(self, faces, meshes, materials, temperatures, n_rays, caster=3):
         """radiance_equation calculate() with malley_cpu over caster `caster`:
