@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
     ap.add_argument("--no-thermal", action="store_true", help="skip the radiance / distant-source section")
+    ap.add_argument("--no-obj", action="store_true", help="skip the OBJ-import section")
     ap.add_argument("--served-requests", type=int, default=16)
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     return ap.parse_args()
@@ -429,6 +430,64 @@ def thermal_section(ctx, faces, rays_per_face):
 
 
 # ---------------------------------------------------------------------------
+# OBJ scene import, then the scene and grid rebuilt on the device
+# ---------------------------------------------------------------------------
+def obj_section(device):
+    """A 250 000-face scene written as OBJ text (%.9g coordinates, one object
+    per 1 000 faces), imported through the C ABI (file read, upload, GPU
+    parse and gather), set as the scene from the device and gridded; the
+    reference's obj_import::scene timed on the same file."""
+    import io
+    import shutil
+    from form_factors_b200 import native, scenes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Reference
+    faces = scenes.clutter(240000, 0.004, seed=3, enclosure_cells=65)[:250000]
+    n = len(faces)
+    buf = io.StringIO()
+    v = faces.reshape(-1, 3)
+    for k in range(0, n, 1000):
+        buf.write("o part_%d\n" % (k // 1000))
+        np.savetxt(buf, v[3 * k:3 * min(n, k + 1000)], fmt="v %.9g %.9g %.9g")
+        idx = np.arange(3 * k + 1, 3 * min(n, k + 1000) + 1).reshape(-1, 3)
+        np.savetxt(buf, idx, fmt="f %d %d %d")
+    text = buf.getvalue().encode()
+    shm = "/dev/shm"
+    where = shm if os.path.isdir(shm) and shutil.disk_usage(shm).free > 4 * len(text) else tempfile.gettempdir()
+    path = os.path.join(where, "ffb_bench_%d.obj" % os.getpid())
+    with open(path, "wb") as f:
+        f.write(text)
+    ctx = native.Context(device)
+    ctx.obj_load(path)  # warm-up
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        info = ctx.obj_load(path)
+        times.append(time.perf_counter() - t0)
+    load_s = statistics.median(times)
+    t0 = time.perf_counter()
+    ctx.obj_scene_set(info["n_faces"])
+    ctx.grid_build()
+    ctx.synchronize()
+    rebuild_s = time.perf_counter() - t0
+    ctx.close()
+    ref = None
+    if Reference.available():
+        t0 = time.perf_counter()
+        rc, _, _, _ = Reference().obj_scene(path)
+        ref_s = time.perf_counter() - t0
+        if rc == 0:
+            ref = {"s": ref_s, "mb_per_s": len(text) / ref_s / 1e6, "cores": 1, "kind": "reference",
+                   "sample": "obj_import::scene (oracle/_ref) on the same file"}
+    os.remove(path)
+    return {"workload": "%d faces, %d objects, %.1f MB of OBJ text" % (n, (n + 999) // 1000, len(text) / 1e6),
+            "status": info["status"], "load_s": load_s, "mb_per_s": len(text) / load_s / 1e6,
+            "faces_per_s": n / load_s, "scene_and_grid_rebuild_s": rebuild_s,
+            "path": "file read -> one upload -> GPU line split, parse, gather -> host object/material lines",
+            "cpu_baseline": ref}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def fp32_peak(device):
@@ -568,6 +627,9 @@ def ours(args):
         csv = csv_section(ctx, stream, counts, front, rear, n)
     if rank == 0 and world == 1 and not args.no_thermal:
         thermal = thermal_section(ctx, faces, args.rays_per_face)
+    obj = None
+    if rank == 0 and world == 1 and not args.no_obj:
+        obj = obj_section(local)
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_section(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_served:
@@ -622,6 +684,8 @@ def ours(args):
             line["csv"] = csv
         if thermal is not None:
             line["thermal"] = thermal
+        if obj is not None:
+            line["obj"] = obj
         print(json.dumps(line))
     ctx.close()
     if world > 1:

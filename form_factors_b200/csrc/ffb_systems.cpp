@@ -1107,6 +1107,54 @@ int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float c
 }  // namespace b200_distant_source
 
 // ===========================================================================
+// OBJ import
+// ===========================================================================
+namespace b200_obj_import {
+
+int scene(const char* filename, subject::scene_t** out)
+{
+  if (!filename || !out)
+    return FFB_ERR_ARG;
+  ffb_ctx* ctx = nullptr;
+  int rc = ffb_ctx_create(device_from_env(), &ctx);
+  if (rc < 0)
+    return rc;
+  ffb_obj_info info;
+  rc = ffb_obj_load(ctx, filename, &info);
+  if (rc == FFB_ERR_FILE || rc == FFB_ERR_FORMAT) {
+    ffb_ctx_destroy(ctx);
+    return info.status;
+  }
+  if (rc < 0) {
+    ffb_ctx_destroy(ctx);
+    return rc;
+  }
+  // subject::scene_create layout; arrays malloc'd for subject::scene_free
+  subject::scene_t* s = (subject::scene_t*)malloc(sizeof(subject::scene_t));
+  s->n_faces = info.n_faces;
+  s->faces = (subject::face_t*)malloc(sizeof(subject::face_t) * (size_t)std::max(info.n_faces, 1));
+  s->n_meshes = info.n_meshes;
+  s->meshes = (subject::mesh_t*)malloc(sizeof(subject::mesh_t) * (size_t)info.n_meshes);
+  s->n_materials = info.n_materials;
+  s->materials = (subject::material_t*)malloc(sizeof(subject::material_t) * (size_t)info.n_materials);
+  static_assert(sizeof(subject::mesh_t) == sizeof(ffb_mesh), "mesh layout");
+  static_assert(sizeof(subject::material_t) == sizeof(ffb_material), "material layout");
+  rc = ffb_obj_result(ctx, &s->faces[0].points[0].x, (ffb_mesh*)s->meshes, (ffb_material*)s->materials);
+  ffb_ctx_destroy(ctx);
+  if (rc < 0) {
+    free(s->faces);
+    free(s->meshes);
+    free(s->materials);
+    free(s);
+    return rc;
+  }
+  *out = s;
+  return OBJ_IMPORT_OK;
+}
+
+}  // namespace b200_obj_import
+
+// ===========================================================================
 // CSV export
 // ===========================================================================
 namespace b200_csv_export {

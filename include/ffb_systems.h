@@ -33,6 +33,7 @@
 #include "thermal_equation/radiance_cpu.h"
 #include "thermal_equation/parallel_rays_cpu.h"
 #include "emission/parallel_rays_cpu.h"
+#include "import_export/obj_import.h"
 #else
 
 namespace math {
@@ -183,6 +184,14 @@ struct scene_t {
 };
 }  // namespace subject
 
+/* import_export/obj_import.h:31-36 */
+#define OBJ_IMPORT_OK 0
+#define OBJ_IMPORT_FILE_ERROR 21
+#define OBJ_IMPORT_FORMAT_ERROR 22
+#define OBJ_IMPORT_MATERIAL_NOT_DEFINED 23
+#define OBJ_IMPORT_MATERIAL_NOT_ENOUGH_PARAMETERS 24
+#define OBJ_IMPORT_MATERIAL_INVALID_PARAMETER_VALUE 25
+
 /* thermal_equation/system.h:26-78 */
 namespace thermal_equation {
 struct task_t {
@@ -322,6 +331,15 @@ void destroy(thermal_equation::system_t* system);
 int set_seed(thermal_equation::system_t* system, uint64_t seed);
 int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float cells_per_face);
 }  // namespace b200_distant_source
+
+namespace b200_obj_import {
+/* obj_import::scene (import_export/obj_import.cpp:167-340) with the geometry
+ * parsed on the GPU (ffb_obj_load): the same faces, meshes and materials, and
+ * the same return codes (OBJ_IMPORT_OK or -OBJ_IMPORT_*).  On success *scene is
+ * malloc'd as subject::scene_create does, for subject::scene_free.  Each call
+ * uses its own context on device FFB_DEVICE (default 0). */
+int scene(const char* filename, subject::scene_t** scene);
+}  // namespace b200_obj_import
 
 namespace b200_csv_export {
 /* csv_export::export_csv (import_export/csv_export.cpp:26-46) with the text

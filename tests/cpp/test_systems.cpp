@@ -630,9 +630,45 @@ static void csv_suite()
   std::remove(path);
 }
 
+// OBJ import (import_export/obj_import.cpp:167-340)
+static void obj_suite()
+{
+  g_case = "B200 obj import";
+  const char* path = "test_systems_scene.obj";
+  FILE* f = std::fopen(path, "wb");
+  std::fputs("# two objects\no first\nv 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0.5e0\nf 1 2 3\n"
+             "g second\nvn 0 0 1\nf 2//1 4//1 3//1\nf 1/1/1 2/2/2 4/4/4\n", f);
+  std::fclose(f);
+  subject::scene_t* s = 0;
+  CHECK(b200_obj_import::scene(path, &s) == OBJ_IMPORT_OK);
+  if (s) {
+    CHECK(s->n_faces == 3 && s->n_meshes == 2 && s->n_materials == 1);
+    CHECK(s->meshes[0].first_idx == 0 && s->meshes[0].n_faces == 1 && s->meshes[1].n_faces == 2);
+    CHECK(s->faces[1].points[1].z == 0.5f && std::strcmp(s->materials[0].name, "black_body") == 0);
+#ifdef FFB_WITH_REFERENCE
+    subject::scene_t* r = 0;
+    CHECK(obj_import::scene(path, &r) == OBJ_IMPORT_OK);
+    if (r) {
+      CHECK(r->n_faces == s->n_faces && r->n_meshes == s->n_meshes && r->n_materials == s->n_materials);
+      CHECK(std::memcmp(r->faces, s->faces, sizeof(subject::face_t) * s->n_faces) == 0);
+      CHECK(std::memcmp(r->meshes, s->meshes, sizeof(subject::mesh_t) * s->n_meshes) == 0);
+      CHECK(std::memcmp(r->materials, s->materials, sizeof(subject::material_t) * s->n_materials) == 0);
+      subject::scene_free(r);
+    }
+#endif
+    free(s->faces);
+    free(s->meshes);
+    free(s->materials);
+    free(s);
+  }
+  CHECK(b200_obj_import::scene("no_such_file.obj", &s) == -OBJ_IMPORT_FILE_ERROR);
+  std::remove(path);
+}
+
 int main()
 {
   csv_suite();
+  obj_suite();
   thermal_suite();
   for (const Caster& c : casters())
     ray_caster_suite(c);
