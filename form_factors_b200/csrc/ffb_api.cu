@@ -63,6 +63,17 @@ struct DevBuf {
 
 constexpr int kChunkRays = 256;  // rays per work chunk of the fused kernel
 constexpr int kMaxRows = 65535;  // matrix index row * n + col stays below 0xFFFFFFFF
+constexpr int kMaxPipeBlocks = 16;  // row blocks of a pipelined host output
+
+// Host outputs of the count matrix of at least FFB_PIPELINE_MIN_BYTES are
+// traced in row blocks of about FFB_PIPELINE_BLOCK_BYTES (2 to
+// kMaxPipeBlocks) whose copies overlap the next block's trace.
+#ifndef FFB_PIPELINE_MIN_BYTES
+#define FFB_PIPELINE_MIN_BYTES (64ull << 20)
+#endif
+#ifndef FFB_PIPELINE_BLOCK_BYTES
+#define FFB_PIPELINE_BLOCK_BYTES (160ull << 20)
+#endif
 
 // One resident scene: faces, triangle records and its grid.
 struct SceneData {
@@ -119,6 +130,11 @@ struct ffb_ctx {
   cudaEvent_t pinned_free = nullptr;  // recorded after the last copy out of `pinned`
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;
+  // pipelined host output of the count matrix: a copy stream fed by one
+  // event per row block (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t block_done[kMaxPipeBlocks] = {};
+  cudaEvent_t copies_done = nullptr;
 };
 
 namespace {
@@ -277,6 +293,20 @@ int scan(ffb_ctx* c, const uint32_t* in, int n, uint32_t* out)
   k_scan_sums<<<1, kScanBlock, 0, c->stream>>>(sums, nb);
   k_scan_apply<<<nb, kScanBlock, 0, c->stream>>>(in, n, sums, out);
   FFB_CUDA(cudaGetLastError());
+  return FFB_OK;
+}
+
+int ensure_pipeline(ffb_ctx* c)
+{
+  if (c->copy_stream)
+    return FFB_OK;
+  cudaError_t e = cudaEventCreateWithFlags(&c->copies_done, cudaEventDisableTiming);
+  for (int b = 0; b < kMaxPipeBlocks && e == cudaSuccess; ++b)
+    e = cudaEventCreateWithFlags(&c->block_done[b], cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess)
+    return fail(FFB_ERR_CUDA, "copy stream/event creation: %s", cudaGetErrorString(e));
   return FFB_OK;
 }
 
@@ -586,6 +616,10 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   for (void* p : c->csv_pinned)
     if (p)
       cudaFreeHost(p);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->copies_done) cudaEventDestroy(c->copies_done);
+  for (cudaEvent_t e : c->block_done)
+    if (e) cudaEventDestroy(e);
   if (c->pinned_free) cudaEventDestroy(c->pinned_free);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -825,61 +859,111 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
         return fail(FFB_ERR_ARG, "face_to_row[%d] = %d outside [0, %d)", f, face_to_row[f], n_rows);
   }
   FFB_TRY(ensure_frames(c, flags));
-  // only the faces of rows [row_begin, row_end) emit
-  std::vector<int32_t> fr(front, front + s.n_faces), re(rear, rear + s.n_faces);
-  if (row_begin > 0 || row_end < n_rows) {
-    for (int f = 0; f < s.n_faces; ++f) {
-      const int row = face_to_row ? face_to_row[f] : f;
-      if (row < row_begin || row >= row_end)
-        fr[f] = re[f] = 0;
-    }
-  }
-  std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
-  add_chunks(chunks, fr.data(), re.data(), s.n_faces, 0);
   const size_t words = (size_t)(row_end - row_begin) * n_rows;
   void* d_counts;
   bool host_out;
   FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * words, c->tmp_out, &d_counts, &host_out));
-  FFB_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * words, c->stream));
+  // Row blocks: one launch each.  A host output of FFB_PIPELINE_MIN_BYTES or
+  // more is split so that each finished block goes to the host on the copy
+  // stream while the next block traces.
+  const int span = row_end - row_begin;
+  int n_blocks = 1;
+  if (host_out && sizeof(uint32_t) * words >= FFB_PIPELINE_MIN_BYTES) {
+    const size_t want = (sizeof(uint32_t) * words + FFB_PIPELINE_BLOCK_BYTES - 1) / FFB_PIPELINE_BLOCK_BYTES;
+    n_blocks = (int)std::min<size_t>(std::max<size_t>(want, 2), (size_t)std::min(kMaxPipeBlocks, span));
+  }
+  std::vector<int> bounds(n_blocks + 1);
+  for (int b = 0; b <= n_blocks; ++b)
+    bounds[b] = row_begin + (int)((long long)span * b / n_blocks);
+  // the chunks of each block, block after block; faces outside
+  // [row_begin, row_end) do not emit
+  std::vector<int> face_block(s.n_faces, -1);
+  for (int f = 0; f < s.n_faces; ++f) {
+    const int row = face_to_row ? face_to_row[f] : f;
+    if (row >= row_begin && row < row_end)
+      face_block[f] = (int)(std::upper_bound(bounds.begin(), bounds.end(), row) - bounds.begin()) - 1;
+  }
+  std::vector<Chunk> chunks;
+  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
+  std::vector<int> first(n_blocks + 1, 0);
+  for (int b = 0; b < n_blocks; ++b) {
+    first[b] = (int)chunks.size();
+    for (int f = 0; f < s.n_faces; ++f) {
+      if (face_block[f] != b)
+        continue;
+      const int nf = front[f] + rear[f];
+      for (int j0 = 0; j0 < nf; j0 += kChunkRays)
+        chunks.push_back(Chunk{f, j0, (int16_t)std::min(kChunkRays, nf - j0), 0, front[f]});
+    }
+  }
+  first[n_blocks] = (int)chunks.size();
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
   if (!chunks.empty()) {
     FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
     if (face_to_row)
       FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)s.n_faces));
-    FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
-    FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
-    TraceParams<1> p;
-    p.frames = dptr<float>(c->frames);
-    p.chunks = dptr<Chunk>(c->chunks);
-    p.n_chunks = (int)chunks.size();
-    p.key0 = (uint32_t)seed;
-    p.key1 = (uint32_t)(seed >> 32);
-    p.epoch = epoch;
-    p.epoch_ptr = nullptr;
-    p.scene_keys = nullptr;
-    p.chunk_cursor = dptr<uint32_t>(c->cursor);
-    p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
-    p.power = nullptr;
-    p.absorb = nullptr;
-    p.scenes[0].g = make_view(s);
-    // the kernel adds at row * n_rows + col; the block holds rows from
-    // row_begin, so its base is moved back by row_begin rows (only rows of
-    // the block are ever written)
-    p.scenes[0].counts = (uint32_t*)((uintptr_t)d_counts - sizeof(uint32_t) * (size_t)row_begin * n_rows);
-    p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
-    p.scenes[0].face_base = 0;
-    p.scenes[0].n_cols = n_rows;
-    if (s.info.skip_empty)
-      FFB_TRY((launch_fused<true, 1>(c, p, 1, true)));
-    else
-      FFB_TRY((launch_fused<false, 1>(c, p, 1, true)));
   }
-  if (host_out) {
+  FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * kMaxPipeBlocks));
+  if (n_blocks > 1)
+    FFB_TRY(ensure_pipeline(c));
+  TraceParams<1> p;
+  p.frames = dptr<float>(c->frames);
+  p.key0 = (uint32_t)seed;
+  p.key1 = (uint32_t)(seed >> 32);
+  p.epoch = epoch;
+  p.epoch_ptr = nullptr;
+  p.scene_keys = nullptr;
+  p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
+  p.power = nullptr;
+  p.absorb = nullptr;
+  p.scenes[0].g = make_view(s);
+  // the kernel adds at row * n_rows + col; the output holds rows from
+  // row_begin, so its base is moved back by row_begin rows (only rows of the
+  // range are ever written)
+  p.scenes[0].counts = (uint32_t*)((uintptr_t)d_counts - sizeof(uint32_t) * (size_t)row_begin * n_rows);
+  p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
+  p.scenes[0].face_base = 0;
+  p.scenes[0].n_cols = n_rows;
+  FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t) * n_blocks, c->stream));
+  timing_begin(c);
+  for (int b = 0; b < n_blocks; ++b) {
+    const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
+    const size_t n_words = (size_t)(bounds[b + 1] - bounds[b]) * n_rows;
+    FFB_CUDA(cudaMemsetAsync((uint32_t*)d_counts + off, 0, sizeof(uint32_t) * n_words, c->stream));
+    if (first[b + 1] > first[b]) {
+      p.chunks = dptr<Chunk>(c->chunks) + first[b];
+      p.n_chunks = first[b + 1] - first[b];
+      p.chunk_cursor = dptr<uint32_t>(c->cursor) + b;
+      if (s.info.skip_empty)
+        FFB_TRY((launch_fused<true, 1>(c, p, 1, false)));
+      else
+        FFB_TRY((launch_fused<false, 1>(c, p, 1, false)));
+    }
+    if (n_blocks > 1)
+      FFB_CUDA(cudaEventRecord(c->block_done[b], c->stream));
+  }
+  timing_end(c);
+  if (!host_out)
+    return FFB_OK;
+  if (n_blocks == 1) {
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
-    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  } else {
+    // all launches are queued before the first copy: a copy to pageable
+    // memory holds the host until it ends
+    for (int b = 0; b < n_blocks; ++b) {
+      const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
+      const size_t n_words = (size_t)(bounds[b + 1] - bounds[b]) * n_rows;
+      FFB_CUDA(cudaStreamWaitEvent(c->copy_stream, c->block_done[b], 0));
+      FFB_CUDA(cudaMemcpyAsync(counts + off, (const uint32_t*)d_counts + off, sizeof(uint32_t) * n_words,
+                               cudaMemcpyDeviceToHost, c->copy_stream));
+    }
+    // later work on the context stream (a reuse of the device output) waits
+    // for the copies
+    FFB_CUDA(cudaEventRecord(c->copies_done, c->copy_stream));
+    FFB_CUDA(cudaStreamWaitEvent(c->stream, c->copies_done, 0));
   }
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
   return FFB_OK;
 }
 

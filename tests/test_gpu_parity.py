@@ -137,3 +137,37 @@ def test_row_blocks_concatenate_to_full_matrix(ctx):
         blocks = [ctx.form_factor_counts_rows(front, rear, 12, b, e, epoch=3)
                   for b, e in shard.row_ranges(shard.rays_per_row(front, rear), world)]
         assert np.array_equal(np.concatenate(blocks), full)
+
+
+def test_pipelined_host_output_matches_device_output(ctx):
+    """Host outputs of 64 MB and more are traced in row blocks whose copies to
+    the host overlap the next block: pageable and pinned host outputs, a row
+    sub-range and a permuted face-to-row map give the device output bit for
+    bit."""
+    import torch
+    faces = scenes.icosphere(4, 1.0, inward=True)  # 5120 faces
+    faces = np.concatenate([faces, scenes.transform(faces, shift=(0.5, 0, 0))])  # 10240 faces
+    n = len(faces)
+    rng = np.random.default_rng(8)
+    front = rng.integers(0, 40, n).astype(np.int32)
+    front[rng.choice(n, 300, replace=False)] = 0
+    rear = rng.integers(0, 3, n).astype(np.int32)
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=16)
+    dev = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    ctx.form_factor_counts(front, rear, seed=31, epoch=2, out=dev)
+    ctx.synchronize()
+    want = dev.cpu().numpy().view(np.uint32)
+    assert want.sum() > 0
+    pageable = ctx.form_factor_counts(front, rear, seed=31, epoch=2)
+    assert np.array_equal(pageable, want)
+    pinned = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+    ctx.form_factor_counts(front, rear, seed=31, epoch=2, out=pinned)
+    assert np.array_equal(pinned.numpy().view(np.uint32), want)
+    part = ctx.form_factor_counts_rows(front, rear, 31, 1234, 9876, epoch=2)
+    assert np.array_equal(part, want[1234:9876])
+    perm = rng.permutation(n).astype(np.int32)
+    permuted = ctx.form_factor_counts(front, rear, seed=31, epoch=2, face_to_row=perm)
+    expect = np.zeros_like(want)
+    expect[perm[:, None], perm[None, :]] = want
+    assert np.array_equal(permuted, expect)
