@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--no-obj", action="store_true", help="skip the OBJ-import section")
     ap.add_argument("--served-requests", type=int, default=16)
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--served-sub-rate", type=float, default=0.5,
+                    help="arrival rate of the sub-saturation run, requests/s (0: skip it)")
+    ap.add_argument("--served-sub-requests", type=int, default=8)
     return ap.parse_args()
 
 
@@ -275,7 +278,7 @@ def served_section(args):
     gaps = rng.exponential(1.0 / args.served_rate, n)
     rays = sum(len(f) * r for f, r, _ in reqs)
 
-    def run(slots, arrivals):
+    def run(slots, arrivals, reqs=reqs):
         server = native.Server(0, budget_bytes=int(80e9), slots=slots)
         t0 = time.perf_counter()
         ids = []
@@ -296,6 +299,21 @@ def served_section(args):
 
     served_wall, lat, peak = run(4, np.cumsum(gaps))
     plain_wall, plain_lat, _ = run(1, np.zeros(n))
+    sub = None
+    if args.served_sub_rate > 0:
+        # the same kind of requests at a rate the server keeps up with:
+        # latency is then service time, not queueing
+        m = args.served_sub_requests
+        sub_reqs = [(scenes.family_scene(fams[i % 3], sizes[i % n], rng), int(rng.integers(1000, 100001)), 500 + i)
+                    for i in range(m)]
+        sub_gaps = rng.exponential(1.0 / args.served_sub_rate, m)
+        sub_wall, sub_lat, sub_peak = run(4, np.cumsum(sub_gaps), sub_reqs)
+        sub_rays = sum(len(f) * r for f, r, _ in sub_reqs)
+        sub = {"rate_per_s": args.served_sub_rate, "requests": m, "rays": int(sub_rays),
+               "offered_rays_per_s": sub_rays / max(float(np.sum(sub_gaps)), 1e-9),
+               "p50_latency_s": float(np.percentile(sub_lat, 50)),
+               "p99_latency_s": float(np.percentile(sub_lat, 99)),
+               "max_latency_s": float(sub_lat.max()), "wall_s": sub_wall, "peak_concurrent": int(sub_peak)}
     return {"workload": "%d requests, faces log-uniform 500-50000 (plates/UV spheres/clutter), 1k-100k front "
                         "rays/face, Poisson %.0f req/s, 80 GB budget, 4 slots" % (n, args.served_rate),
             "rays": int(rays), "served_scenes_per_s": n / served_wall, "plain_scenes_per_s": n / plain_wall,
@@ -303,7 +321,8 @@ def served_section(args):
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "plain_p50_latency_s": float(np.percentile(plain_lat, 50)),
             "offered_rays_per_s": rays / max(float(np.sum(gaps)), 1e-9), "peak_concurrent": int(peak),
-            "note": "offered load far above capacity: latency is queueing under saturation"}
+            "note": "offered load far above capacity: latency is queueing under saturation",
+            "sub_saturation": sub}
 
 
 # ---------------------------------------------------------------------------

@@ -458,17 +458,19 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
       dptr<int32_t>(s.ref_tri), total, dptr<TriRec>(s.tri), dptr<TriRec>(s.ref_rec));
   FFB_CUDA(cudaGetLastError());
   if (I.skip_empty) {
-    FFB_TRY(ensure(c, s.empty_dist, (size_t)n_cells));
+    // one byte per cell and octant; passes along x, y, z double the octants
+    FFB_TRY(ensure(c, s.empty_dist, (size_t)kOctants * n_cells));
     uint8_t* d = dptr<uint8_t>(s.empty_dist);
     k_empty_init<<<grid_blocks(n_cells, 256), 256, 0, c->stream>>>(dptr<uint32_t>(s.cell_start), (int)n_cells, d);
-    k_empty_pass<<<grid_blocks((long long)I.ny * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 0);
-    k_empty_pass<<<grid_blocks((long long)I.nx * I.nz, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 1);
-    k_empty_pass<<<grid_blocks((long long)I.nx * I.ny, 128), 128, 0, c->stream>>>(d, I.nx, I.ny, I.nz, 2);
+    const long long lines[3] = {(long long)I.ny * I.nz, (long long)I.nx * I.nz, (long long)I.nx * I.ny};
+    for (int axis = 0; axis < 3; ++axis)
+      k_empty_pass<<<dim3(grid_blocks(lines[axis], 128), 1u << axis), 128, 0, c->stream>>>(d, n_cells, I.nx, I.ny,
+                                                                                         I.nz, axis);
     FFB_CUDA(cudaGetLastError());
   }
   FFB_TRY(ensure(c, s.cell_rec, sizeof(uint2) * (size_t)n_cells));
   k_cell_rec<<<grid_blocks(n_cells, 256, c->n_sm * 8), 256, 0, c->stream>>>(
-      dptr<uint32_t>(s.cell_start), I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr, (int)n_cells,
+      dptr<uint32_t>(s.cell_start), I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr, n_cells,
       dptr<uint2>(s.cell_rec));
   FFB_CUDA(cudaGetLastError());
   // live faces: those with a non-empty binning box

@@ -188,14 +188,53 @@ __device__ __forceinline__ void for_each_cell(const BinGeom& g, const float* __r
   float3 h = mul3(g.cs, 0.5f);
   float reach = fabsf(n.x) * h.x + fabsf(n.y) * h.y + fabsf(n.z) * h.z + m * 1.5f;
   bool flat = (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1) <= 2;
+  // Edge axes of the separating-axis test: edge x unit axis, for the three
+  // edges.  Each axis is an exact float vector (a permutation of an edge's
+  // components), so only the projections round.  The cell grown by the
+  // margin on every axis, as the box range above grows it, reaches
+  // r = sum (h_a + m) |A_a| along axis A; a further 0.5 m per axis covers
+  // the rounding of the projections (coordinates relative to p0).  An axis
+  // that separates the triangle from the grown cell proves that no hit point
+  // computed on the triangle can land in the cell.
+  const float3 ed[3] = {sub3(f3(p[3], p[4], p[5]), p0), sub3(f3(p[6], p[7], p[8]), f3(p[3], p[4], p[5])),
+                        sub3(p0, f3(p[6], p[7], p[8]))};
+  const float3 q1 = ed[0], q2 = sub3(f3(p[6], p[7], p[8]), p0);  // vertices relative to p0 (q0 = 0)
+  const float3 hm = f3(h.x + 1.5f * m, h.y + 1.5f * m, h.z + 1.5f * m);
+  float ax_lo[9], ax_hi[9], ax_r[9];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float3 A = a == 0 ? f3(0.f, ed[e].z, -ed[e].y) : (a == 1 ? f3(-ed[e].z, 0.f, ed[e].x)
+                                                                     : f3(ed[e].y, -ed[e].x, 0.f));
+      const float v1 = dot3(q1, A), v2 = dot3(q2, A);
+      ax_lo[3 * e + a] = fminf(0.f, fminf(v1, v2));
+      ax_hi[3 * e + a] = fmaxf(0.f, fmaxf(v1, v2));
+      ax_r[3 * e + a] = fabsf(A.x) * hm.x + fabsf(A.y) * hm.y + fabsf(A.z) * hm.z;
+    }
+  }
   for (int k = k0; k <= k1; ++k)
     for (int j = j0; j <= j1; ++j)
       for (int i = i0; i <= i1; ++i) {
         if (!flat) {
           float3 c = f3(g.lo.x + ((float)i + 0.5f) * g.cs.x, g.lo.y + ((float)j + 0.5f) * g.cs.y,
                         g.lo.z + ((float)k + 0.5f) * g.cs.z);
-          float d = fabsf(dot3(n, sub3(c, p0)));
+          const float3 dc = sub3(c, p0);
+          float d = fabsf(dot3(n, dc));
           if (d > reach)
+            continue;
+          bool sep = false;
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const float3 A = a == 0 ? f3(0.f, ed[e].z, -ed[e].y) : (a == 1 ? f3(-ed[e].z, 0.f, ed[e].x)
+                                                                             : f3(ed[e].y, -ed[e].x, 0.f));
+              const float pc = dot3(dc, A);
+              sep |= (ax_lo[3 * e + a] > pc + ax_r[3 * e + a]) | (ax_hi[3 * e + a] < pc - ax_r[3 * e + a]);
+            }
+          }
+          if (sep)
             continue;
         }
         fn((k * g.ny + j) * g.nx + i);
@@ -350,13 +389,25 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ in, int n, const uint3
 }
 
 // ---------------------------------------------------------------------------
-// Empty-space distance: for each cell, the Chebyshev distance (in cells) to
-// the nearest occupied cell, saturated at kEmptyCap.  The L-infinity distance
-// transform is separable: pass a computes new[i] = min_j max(|i-j|, old[j])
-// along axis a, starting from 0 (occupied) / kEmptyCap (empty).  A saturated
-// value under-states the distance, which only shortens a jump.
+// Empty-space distance per octant.  For each empty cell and each of the 8
+// octants of ray directions, the largest k such that the cube of k x k x k
+// cells with the cell at its corner, extending from it in the octant's
+// directions, holds no reference: the L-infinity distance to the nearest
+// occupied cell lying in that octant of the cell.  A ray whose direction
+// lies in the octant leaves the cube only through its far faces, so it jumps
+// to them (tracer_advance); occupied cells behind the ray do not shorten the
+// jump.  The transform is separable: pass a computes, along axis a and in
+// each direction, new[i] = min_{r >= 0} max(r, old[i + r*s]), starting from
+// 0 (occupied) / kEmptyCap (empty).  Octant o has bit a set when it points
+// down axis a.  A saturated value under-states the distance, which only
+// shortens a jump.
 // ---------------------------------------------------------------------------
-constexpr int kEmptyCap = 32;
+#ifndef FFB_EMPTY_CAP
+#define FFB_EMPTY_CAP 127
+#endif
+constexpr int kEmptyCap = FFB_EMPTY_CAP;  // at most 127: 7 bits per octant in the cell record
+static_assert(kEmptyCap >= 1 && kEmptyCap <= 127, "octant distances are 7-bit fields");
+constexpr int kOctants = 8;
 constexpr int kMaxDim = 256;
 
 __global__ void k_empty_init(const uint32_t* __restrict__ cell_start, int n_cells, uint8_t* __restrict__ d)
@@ -366,7 +417,11 @@ __global__ void k_empty_init(const uint32_t* __restrict__ cell_start, int n_cell
     d[c] = cell_start[c + 1] > cell_start[c] ? 0 : kEmptyCap;
 }
 
-__global__ void k_empty_pass(uint8_t* __restrict__ d, int nx, int ny, int nz, int axis)
+// One pass along `axis`: octant slot blockIdx.y (< 2^axis, the octants of
+// the axes before) holds the input; the positive direction is written back
+// in place and the negative one to slot blockIdx.y | 2^axis.  One thread per
+// line of cells; slots are n_cells bytes apart.
+__global__ void k_empty_pass(uint8_t* __restrict__ d, long long n_cells, int nx, int ny, int nz, int axis)
 {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n_len, stride, base;
@@ -381,27 +436,43 @@ __global__ void k_empty_pass(uint8_t* __restrict__ d, int nx, int ny, int nz, in
     if (t >= nx * ny) return;
     n_len = nz; stride = nx * ny; base = t;
   }
+  uint8_t* in = d + (size_t)blockIdx.y * n_cells;
+  uint8_t* neg = d + (size_t)(blockIdx.y | (1u << axis)) * n_cells;
   uint8_t buf[kMaxDim];
   for (int i = 0; i < n_len; ++i)
-    buf[i] = d[base + i * stride];
+    buf[i] = in[base + i * stride];
   for (int i = 0; i < n_len; ++i) {
-    int best = buf[i];
-    for (int r = 1; r < best; ++r) {
-      int v = kEmptyCap;
-      if (i - r >= 0) v = min(v, (int)buf[i - r]);
-      if (i + r < n_len) v = min(v, (int)buf[i + r]);
-      best = min(best, max(r, v));
-    }
-    d[base + i * stride] = (uint8_t)best;
+    int bp = buf[i], bn = buf[i];
+    for (int r = 1; r < bp && i + r < n_len; ++r)
+      bp = min(bp, max(r, (int)buf[i + r]));
+    for (int r = 1; r < bn && i - r >= 0; ++r)
+      bn = min(bn, max(r, (int)buf[i - r]));
+    in[base + i * stride] = (uint8_t)bp;
+    neg[base + i * stride] = (uint8_t)bn;
   }
 }
 
-__global__ void k_cell_rec(const uint32_t* __restrict__ cell_start, const uint8_t* __restrict__ empty_dist, int n_cells,
-                           uint2* __restrict__ rec)
+// Packs the cell records: occupied {start, end}; empty {octants 0-3, flag |
+// octants 4-7}, one byte per octant (octant o in byte o & 3).  Without a
+// distance map every octant distance is 1 (single DDA steps).
+__global__ void k_cell_rec(const uint32_t* __restrict__ cell_start, const uint8_t* __restrict__ empty_dist,
+                           long long n_cells, uint2* __restrict__ rec)
 {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n_cells;
+       c += (long long)gridDim.x * blockDim.x) {
     const uint32_t b = cell_start[c], e = cell_start[c + 1];
-    rec[c] = e > b ? make_uint2(b, e) : make_uint2(0u, kCellEmpty | (empty_dist ? (uint32_t)empty_dist[c] : 1u));
+    if (e > b) {
+      rec[c] = make_uint2(b, e);
+      continue;
+    }
+    uint32_t w[2] = {0x01010101u, 0x01010101u};
+    if (empty_dist) {
+      w[0] = w[1] = 0;
+#pragma unroll
+      for (int o = 0; o < kOctants; ++o)
+        w[o >> 2] |= (uint32_t)empty_dist[(size_t)o * n_cells + c] << (8 * (o & 3));
+    }
+    rec[c] = make_uint2(w[0], kCellEmpty | w[1]);
   }
 }
 
@@ -445,7 +516,7 @@ __device__ __forceinline__ float next_t(int s, int c, float lo, float cs, float 
 }
 
 // Landing cell on one axis after a jump to parameter tj: never against the
-// ray, never beyond the empty cube of half-width `jump`.
+// ray, never beyond the far face of the empty cube of `jump` cells per side.
 __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, float tj, float lo, float ics)
 {
   if (s == 0)
@@ -485,7 +556,14 @@ __device__ __forceinline__ void tracer_enter(Tracer& T, const GridView& g)
   const int cell = (T.cz * g.ny + T.cy) * g.nx + T.cx;
   const uint2 r = __ldg(g.cell_rec + cell);
   const bool empty = (r.y & kCellEmpty) != 0;
-  T.jump = kSkip && empty ? (int)(r.y & 0xFFu) : 0;
+  if (kSkip) {
+    // the distance of the octant of the ray's direction
+    const uint32_t w = T.dir.z < 0.f ? r.y : r.x;
+    const int sh = (T.dir.x < 0.f ? 8 : 0) + (T.dir.y < 0.f ? 16 : 0);
+    T.jump = empty ? (int)((w >> sh) & 0x7Fu) : 0;
+  } else {
+    T.jump = 0;
+  }
   T.i = r.x;
   T.en = empty ? 0u : r.y;
 }
@@ -564,10 +642,11 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
     return false;
   const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
   if (kSkip) {
-    // Every move leaves the empty cube of half-width jump-1 around the cell
-    // (the cell itself when jump <= 1, where the exit parameter is the DDA's
-    // next boundary) and lands in the cell where the ray crosses the cube's
-    // boundary.  A diagonal landing skips only cells that the ray touches
+    // Every move leaves the empty cube of jump cells per side that extends
+    // from the cell in the octant of the ray's direction (the cell itself
+    // when jump <= 1, where the exit parameter is the DDA's next boundary).
+    // The ray starts inside it and moves monotonically, so it leaves through
+    // a far face; it lands in the cell where it crosses that face.  A diagonal landing skips only cells that the ray touches
     // within rounding of the landing cell, whose triangles the binning margin
     // puts into the landing cell as well.  Lanes that step and lanes that
     // jump run the same instructions.
