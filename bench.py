@@ -52,8 +52,8 @@ def parse():
     ap.add_argument("--cpu-sample-every", type=int, default=0, help="reference sample: every k-th source face")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="", help="grid dims nx,ny,nz (default: automatic)")
-    ap.add_argument("--cells-per-face", type=float, default=128.0,
-                    help="automatic grid sizing target (128 measured fastest on this workload; the library default is 32)")
+    ap.add_argument("--cells-per-face", type=float, default=192.0,
+                    help="automatic grid sizing target (192-256 measured fastest on this workload; the library default is 32)")
     ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")

@@ -695,6 +695,22 @@ extern "C" int ffb_grid_info_get(ffb_ctx* c, ffb_grid_info* out)
   return FFB_OK;
 }
 
+extern "C" int ffb_grid_export(ffb_ctx* c, uint32_t* cell_rec, int32_t* ref_tri)
+{
+  FFB_TRY(check_ctx(c));
+  SceneData& s = c->main;
+  if (!s.grid_ok)
+    return fail(FFB_ERR_NO_GRID, "no grid built");
+  const size_t n_cells = (size_t)s.info.nx * s.info.ny * s.info.nz;
+  if (cell_rec)
+    FFB_CUDA(cudaMemcpyAsync(cell_rec, s.cell_rec.ptr, sizeof(uint2) * n_cells, cudaMemcpyDefault, c->stream));
+  if (ref_tri && s.info.n_refs > 0)
+    FFB_CUDA(cudaMemcpyAsync(ref_tri, s.ref_tri.ptr, sizeof(int32_t) * (size_t)s.info.n_refs, cudaMemcpyDefault,
+                             c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  return FFB_OK;
+}
+
 // ===========================================================================
 // Casts
 // ===========================================================================

@@ -138,6 +138,7 @@ def load(path=LIB_PATH):
         "ffb_scene_set": (i32, [vp, vp, i32]),
         "ffb_grid_build": (i32, [vp, C.POINTER(GridParams)]),
         "ffb_grid_info_get": (i32, [vp, C.POINTER(GridInfo)]),
+        "ffb_grid_export": (i32, [vp, vp, vp]),
         "ffb_cast": (i32, [vp, vp, i64, vp, vp]),
         "ffb_cast_bruteforce": (i32, [vp, vp, i64, vp, vp]),
         "ffb_emit": (i32, [vp, vp, vp, u64, u32, i32, vp]),
@@ -305,6 +306,16 @@ class Context:
         info = GridInfo()
         _check(self._lib.ffb_grid_info_get(self._h, C.byref(info)))
         return info
+
+    def grid_export(self):
+        """The current grid: cell records (nz, ny, nx, 2) uint32 and the
+        references (face index per reference, each cell's in ascending
+        order), as ffb_grid_export lays them out."""
+        info = self.grid_info()
+        rec = np.empty((info.nz, info.ny, info.nx, 2), np.uint32)
+        refs = np.empty(max(int(info.n_refs), 1), np.int32)
+        _check(self._lib.ffb_grid_export(self._h, _ptr(rec), _ptr(refs)))
+        return rec, refs[:int(info.n_refs)]
 
     def cast(self, rays, hit=None, points=None, want_points=True, brute=False):
         """rays: (n, 6) float32 host array or device tensor.  Returns (hit, points)."""

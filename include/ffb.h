@@ -106,6 +106,20 @@ int ffb_scene_set(ffb_ctx* ctx, const float* faces9, int n_faces);
 int ffb_grid_build(ffb_ctx* ctx, const ffb_grid_params* params);
 int ffb_grid_info_get(ffb_ctx* ctx, ffb_grid_info* out);
 
+/* Copies the grid of the current scene to host or device buffers (either
+ * may be NULL):
+ *  cell_rec: 2 uint32 per cell, x fastest.  An occupied cell holds {first
+ *    reference, end}.  An empty one holds {octant distances 0-3,
+ *    0x80000000 | octant distances 4-7}, one byte per octant (octant o in
+ *    byte o & 3).  Octant o points down axis a when bit a of o is set; its
+ *    distance is the side of the largest cube of empty cells that extends
+ *    from the cell in those directions (capped at 127; 1 for every octant
+ *    when the grid skips no empty space).
+ *  ref_tri: n_refs face indices, each cell's references in ascending order.
+ * No reference counterpart (zgrid_cpu keeps its 2-D cells internal,
+ * math/grid.h:36-49): an inspection hook for tests and tools. */
+int ffb_grid_export(ffb_ctx* ctx, uint32_t* cell_rec, int32_t* ref_tri);
+
 /* Nearest hit per ray through the grid.  rays6: host or device; hit_face:
  * host or device, face index or -1; hit_point: host, device or NULL, the
  * reference's hit point for hits and NaN for misses.  Equal bit for bit to
