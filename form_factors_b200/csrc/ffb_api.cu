@@ -112,6 +112,11 @@ struct ffb_ctx {
   DevBuf batch_frames, batch_chunks, batch_keys, batch_epoch;
   int batch_frames_mode = -1;
   int batch_n_chunks = 0;
+  std::vector<int> batch_chunk_first;  // first chunk of each scene (scene-major), plus the total
+  // side streams of the batched launch: one launch per scene, spread over
+  // them so that a scene's launch tail overlaps the next scenes
+  cudaStream_t batch_streams[4] = {};
+  cudaEvent_t batch_fork = nullptr, batch_join[4] = {};
 
   // per-call scratch
   DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
@@ -307,6 +312,24 @@ int ensure_pipeline(ffb_ctx* c)
     e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess)
     return fail(FFB_ERR_CUDA, "copy stream/event creation: %s", cudaGetErrorString(e));
+  return FFB_OK;
+}
+
+int ensure_batch_streams(ffb_ctx* c)
+{
+  if (c->batch_fork)
+    return FFB_OK;
+  cudaError_t e = cudaSuccess;
+  for (cudaStream_t& st : c->batch_streams)
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  for (cudaEvent_t& ev : c->batch_join)
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&c->batch_fork, cudaEventDisableTiming);
+  if (e != cudaSuccess)
+    return fail(FFB_ERR_CUDA, "batch stream/event creation: %s", cudaGetErrorString(e));
   return FFB_OK;
 }
 
@@ -522,22 +545,20 @@ int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long lo
 #endif
 
 // Occupancy-sized persistent launch of the fused kernel for p.n_chunks chunks.
-template <bool kSkip, int kScenes>
-int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, int n_scenes, bool timed)
+template <bool kSkip>
+int launch_fused(ffb_ctx* c, const TraceParams& p, bool timed, cudaStream_t stream = nullptr)
 {
-  bool hash = false;
-  for (int s = 0; s < n_scenes; ++s)
-    hash |= (unsigned long long)p.scenes[s].n_cols * (unsigned long long)p.scenes[s].n_cols < FFB_DIRECT_MIN_WORDS;
-  void (*kern)(TraceParams<kScenes>);
+  if (!stream)
+    stream = c->stream;
+  bool hash = (unsigned long long)p.scene.n_cols * (unsigned long long)p.scene.n_cols < FFB_DIRECT_MIN_WORDS;
+  void (*kern)(TraceParams);
   if (p.stats)
-    kern = hash ? k_form_factors<kSkip, kScenes, true, true> : k_form_factors<kSkip, kScenes, true, false>;
+    kern = hash ? k_form_factors<kSkip, true, true> : k_form_factors<kSkip, true, false>;
   else
-    kern = hash ? k_form_factors<kSkip, kScenes, false, true> : k_form_factors<kSkip, kScenes, false, false>;
-  if constexpr (kScenes == 1) {
-    if (p.power) {  // radiance sink: no matrix, no histogram
-      kern = p.stats ? k_form_factors<kSkip, 1, true, false, true> : k_form_factors<kSkip, 1, false, false, true>;
-      hash = false;
-    }
+    kern = hash ? k_form_factors<kSkip, false, true> : k_form_factors<kSkip, false, false>;
+  if (p.power) {  // radiance sink: no matrix, no histogram
+    kern = p.stats ? k_form_factors<kSkip, true, false, true> : k_form_factors<kSkip, false, false, true>;
+    hash = false;
   }
   const size_t smem = hash ? kHashSmem : 0;
   int per_sm = 0;
@@ -548,7 +569,7 @@ int launch_fused(ffb_ctx* c, const TraceParams<kScenes>& p, int n_scenes, bool t
   const int blocks = (int)std::max<long long>(1, std::min(wave, by_work));
   if (timed)
     timing_begin(c);
-  kern<<<blocks, kTraceThreads, smem, c->stream>>>(p);
+  kern<<<blocks, kTraceThreads, smem, stream>>>(p);
   if (timed)
     timing_end(c);
   FFB_CUDA(cudaGetLastError());
@@ -618,6 +639,11 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   for (void* p : c->csv_pinned)
     if (p)
       cudaFreeHost(p);
+  for (cudaStream_t st : c->batch_streams)
+    if (st) cudaStreamDestroy(st);
+  for (cudaEvent_t e : c->batch_join)
+    if (e) cudaEventDestroy(e);
+  if (c->batch_fork) cudaEventDestroy(c->batch_fork);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->copies_done) cudaEventDestroy(c->copies_done);
   for (cudaEvent_t e : c->block_done)
@@ -925,7 +951,7 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * kMaxPipeBlocks));
   if (n_blocks > 1)
     FFB_TRY(ensure_pipeline(c));
-  TraceParams<1> p;
+  TraceParams p;
   p.frames = dptr<float>(c->frames);
   p.key0 = (uint32_t)seed;
   p.key1 = (uint32_t)(seed >> 32);
@@ -935,14 +961,14 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
   p.power = nullptr;
   p.absorb = nullptr;
-  p.scenes[0].g = make_view(s);
+  p.scene.g = make_view(s);
   // the kernel adds at row * n_rows + col; the output holds rows from
   // row_begin, so its base is moved back by row_begin rows (only rows of the
   // range are ever written)
-  p.scenes[0].counts = (uint32_t*)((uintptr_t)d_counts - sizeof(uint32_t) * (size_t)row_begin * n_rows);
-  p.scenes[0].face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
-  p.scenes[0].face_base = 0;
-  p.scenes[0].n_cols = n_rows;
+  p.scene.counts = (uint32_t*)((uintptr_t)d_counts - sizeof(uint32_t) * (size_t)row_begin * n_rows);
+  p.scene.face_to_row = face_to_row ? dptr<int32_t>(c->rows) : nullptr;
+  p.scene.face_base = 0;
+  p.scene.n_cols = n_rows;
   FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t) * n_blocks, c->stream));
   timing_begin(c);
   for (int b = 0; b < n_blocks; ++b) {
@@ -954,9 +980,9 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
       p.n_chunks = first[b + 1] - first[b];
       p.chunk_cursor = dptr<uint32_t>(c->cursor) + b;
       if (s.info.skip_empty)
-        FFB_TRY((launch_fused<true, 1>(c, p, 1, false)));
+        FFB_TRY((launch_fused<true>(c, p, false)));
       else
-        FFB_TRY((launch_fused<false, 1>(c, p, 1, false)));
+        FFB_TRY((launch_fused<false>(c, p, false)));
     }
     if (n_blocks > 1)
       FFB_CUDA(cudaEventRecord(c->block_done[b], c->stream));
@@ -1079,7 +1105,7 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
     FFB_TRY(upload(c, c->rows, face_to_mesh, sizeof(int32_t) * (size_t)s.n_faces));
     FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
     FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
-    TraceParams<1> p;
+    TraceParams p;
     p.frames = dptr<float>(c->frames);
     p.chunks = dptr<Chunk>(c->chunks);
     p.n_chunks = (int)chunks.size();
@@ -1092,15 +1118,15 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
     p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
     p.power = dptr<unsigned long long>(c->power_tab);
     p.absorb = dptr<unsigned long long>(c->absorb);
-    p.scenes[0].g = make_view(s);
-    p.scenes[0].counts = nullptr;
-    p.scenes[0].face_to_row = dptr<int32_t>(c->rows);
-    p.scenes[0].face_base = 0;
-    p.scenes[0].n_cols = n_meshes;
+    p.scene.g = make_view(s);
+    p.scene.counts = nullptr;
+    p.scene.face_to_row = dptr<int32_t>(c->rows);
+    p.scene.face_base = 0;
+    p.scene.n_cols = n_meshes;
     if (s.info.skip_empty)
-      FFB_TRY((launch_fused<true, 1>(c, p, 1, true)));
+      FFB_TRY((launch_fused<true>(c, p, true)));
     else
-      FFB_TRY((launch_fused<false, 1>(c, p, 1, true)));
+      FFB_TRY((launch_fused<false>(c, p, true)));
   }
   std::vector<long long> sums((size_t)n_meshes);
   FFB_CUDA(cudaMemcpyAsync(sums.data(), c->absorb.ptr, sizeof(long long) * sums.size(), cudaMemcpyDeviceToHost,
@@ -1774,10 +1800,13 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
   FFB_TRY(check_counts((int)n_all, front, rear, &total));
   std::vector<Chunk> chunks;
   chunks.reserve((size_t)(total / kChunkRays + n_all));
+  c->batch_chunk_first.assign(n_scenes + 1, 0);
   for (int s = 0; s < n_scenes; ++s) {
     const long long f0 = c->batch_offsets[s];
+    c->batch_chunk_first[s] = (int)chunks.size();
     add_chunks(chunks, front + f0, rear + f0, c->batch[s].n_faces, s);
   }
+  c->batch_chunk_first[n_scenes] = (int)chunks.size();
   c->batch_n_chunks = (int)chunks.size();
   if (!chunks.empty())
     FFB_TRY(upload(c, c->batch_chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
@@ -1795,7 +1824,7 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
                            dptr<float>(c->batch_frames) + 20 * c->batch_offsets[s]));
     c->batch_frames_mode = mode;
   }
-  FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
+  FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * (size_t)std::max(n_scenes, kMaxPipeBlocks)));
   FFB_TRY(ensure(c, c->batch_epoch, sizeof(uint32_t)));
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->batch_epoch.ptr, 0, sizeof(uint32_t), c->stream));
@@ -1823,43 +1852,56 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     return fail(FFB_ERR_ARG, "batched counts must be device memory");
   FFB_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * counts_words, c->stream));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
-  FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t), c->stream));
+  FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t) * (size_t)n_scenes, c->stream));
   if (advance_epoch) {
     k_epoch_bump<<<1, 32, 0, c->stream>>>(dptr<uint32_t>(c->batch_epoch));
     FFB_CUDA(cudaGetLastError());
   }
   if (c->batch_n_chunks == 0)
     return FFB_OK;
-  TraceParams<kMaxBatchScenes> p;
-  p.frames = dptr<float>(c->batch_frames);
-  p.chunks = dptr<Chunk>(c->batch_chunks);
-  p.n_chunks = c->batch_n_chunks;
-  p.key0 = p.key1 = p.epoch = 0;
-  p.epoch_ptr = dptr<uint32_t>(c->batch_epoch);
-  p.scene_keys = dptr<uint2>(c->batch_keys);
-  p.chunk_cursor = dptr<uint32_t>(c->cursor);
-  p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
-  p.power = nullptr;
-  p.absorb = nullptr;
-  // all scenes share one kernel variant: empty-space jumps need every
-  // scene's distance map
-  bool skip = true;
-  for (int s = 0; s < kMaxBatchScenes; ++s) {
-    SceneSlot& slot = p.scenes[s];
-    memset(&slot, 0, sizeof slot);
-    if (s >= n_scenes)
+  FFB_TRY(ensure_batch_streams(c));
+  constexpr int kSide = (int)(sizeof(c->batch_streams) / sizeof(c->batch_streams[0]));
+  FFB_CUDA(cudaEventRecord(c->batch_fork, c->stream));
+  for (int k = 0; k < kSide; ++k)
+    FFB_CUDA(cudaStreamWaitEvent(c->batch_streams[k], c->batch_fork, 0));
+  // largest scenes first, dealt round-robin over the side streams
+  std::vector<int> order(n_scenes);
+  for (int s = 0; s < n_scenes; ++s)
+    order[s] = s;
+  const std::vector<int>& first = c->batch_chunk_first;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return first[a + 1] - first[a] > first[b + 1] - first[b]; });
+  int k = 0;
+  for (int s : order) {
+    if (first[s + 1] == first[s])
       continue;
+    TraceParams p;
+    p.frames = dptr<float>(c->batch_frames);
+    p.chunks = dptr<Chunk>(c->batch_chunks) + first[s];
+    p.n_chunks = first[s + 1] - first[s];
+    p.key0 = p.key1 = p.epoch = 0;
+    p.epoch_ptr = dptr<uint32_t>(c->batch_epoch);
+    p.scene_keys = dptr<uint2>(c->batch_keys) + s;
+    p.chunk_cursor = dptr<uint32_t>(c->cursor) + s;
+    p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
+    p.power = nullptr;
+    p.absorb = nullptr;
+    SceneSlot& slot = p.scene;
     slot.g = make_view(c->batch[s]);
     slot.counts = counts + counts_offsets[s];
     slot.face_to_row = nullptr;
     slot.face_base = (int)c->batch_offsets[s];
     slot.n_cols = c->batch[s].n_faces;
-    skip = skip && c->batch[s].info.skip_empty;
+    cudaStream_t st = c->batch_streams[k++ % kSide];
+    if (c->batch[s].info.skip_empty)
+      FFB_TRY((launch_fused<true>(c, p, false, st)));
+    else
+      FFB_TRY((launch_fused<false>(c, p, false, st)));
   }
-  if (skip)
-    FFB_TRY((launch_fused<true, kMaxBatchScenes>(c, p, n_scenes, false)));
-  else
-    FFB_TRY((launch_fused<false, kMaxBatchScenes>(c, p, n_scenes, false)));
+  for (int j = 0; j < kSide; ++j) {
+    FFB_CUDA(cudaEventRecord(c->batch_join[j], c->batch_streams[j]));
+    FFB_CUDA(cudaStreamWaitEvent(c->stream, c->batch_join[j], 0));
+  }
   return FFB_OK;
 }
 

@@ -398,7 +398,7 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ in, int n, const uint3
 // to them (tracer_advance); occupied cells behind the ray do not shorten the
 // jump.  The transform is separable: pass a computes, along axis a and in
 // each direction, new[i] = min_{r >= 0} max(r, old[i + r*s]), starting from
-// 0 (occupied) / kEmptyCap (empty).  Octant o has bit a set when it points
+// 0 (occupied) / kEmptyCap (empty), in one linear scan per line.  Octant o has bit a set when it points
 // down axis a.  A saturated value under-states the distance, which only
 // shortens a jump.
 // ---------------------------------------------------------------------------
@@ -441,14 +441,27 @@ __global__ void k_empty_pass(uint8_t* __restrict__ d, long long n_cells, int nx,
   uint8_t buf[kMaxDim];
   for (int i = 0; i < n_len; ++i)
     buf[i] = in[base + i * stride];
-  for (int i = 0; i < n_len; ++i) {
-    int bp = buf[i], bn = buf[i];
-    for (int r = 1; r < bp && i + r < n_len; ++r)
-      bp = min(bp, max(r, (int)buf[i + r]));
-    for (int r = 1; r < bn && i - r >= 0; ++r)
-      bn = min(bn, max(r, (int)buf[i - r]));
-    in[base + i * stride] = (uint8_t)bp;
-    neg[base + i * stride] = (uint8_t)bn;
+  // Linear scan against the direction.  With G the value one step ahead,
+  // the new value is min(w, G) when a position within G steps ahead holds
+  // G, else min(w, G + 1): the positions within G steps all hold at least
+  // G.  last[v] is the scan index of the nearest position seen holding v.
+  int16_t last[kEmptyCap + 1];
+  for (int dir = 0; dir < 2; ++dir) {  // 0: positive direction (in place), 1: negative
+    uint8_t* out = dir ? neg : in;
+    for (int v = 0; v <= kEmptyCap; ++v)
+      last[v] = -32768;
+    int G = kEmptyCap;
+    for (int k = 0; k < n_len; ++k) {
+      const int i = dir ? k : n_len - 1 - k;
+      const int w = buf[i];
+      int h = kEmptyCap;
+      if (k > 0)
+        h = (G < kEmptyCap && k - last[G] <= G) ? G : min(G + 1, kEmptyCap);
+      const int g = min(w, h);
+      out[base + i * stride] = (uint8_t)g;
+      last[w] = (int16_t)k;
+      G = g;
+    }
   }
 }
 

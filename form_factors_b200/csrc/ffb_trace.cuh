@@ -14,15 +14,15 @@ struct Chunk {
   int32_t face;
   int32_t j0;
   int16_t count;
-  int16_t scene;
+  int16_t scene;  // scene of a batched work list (informational: each scene has its own launch)
   int32_t front;
 };
 
 // Statistics slots (uint64 each), accumulated once per warp.
 enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatJumps = 4, kStatSlots = 5 };
 
-// One scene of a fused launch: its grid, its count matrix and where its faces
-// start in the launch's frame table.
+// The scene of a fused launch: its grid, its count matrix and where its
+// faces start in the launch's frame table.
 struct SceneSlot {
   GridView g;
   uint32_t* __restrict__ counts;              // n_cols * n_cols
@@ -31,17 +31,16 @@ struct SceneSlot {
   int n_cols;                                 // matrix side
 };
 
-// Up to 256 scenes ride in the kernel parameter space (32 KB on sm_100).
-constexpr int kMaxBatchScenes = 256;
+// Scenes of one batch (ffb_batch_set); each is traced by its own launch.
+constexpr int kMaxBatchScenes = 4096;
 
-template <int kScenes>
 struct TraceParams {
   const float* __restrict__ frames;          // 20 floats per face, scenes concatenated
   const Chunk* __restrict__ chunks;
   int n_chunks;
   uint32_t key0, key1, epoch;
   const uint32_t* __restrict__ epoch_ptr;    // when set, the epoch is read from device memory
-  const uint2* __restrict__ scene_keys;      // per-scene Philox key, or null for (key0, key1)
+  const uint2* __restrict__ scene_keys;      // device Philox key of the scene, or null for (key0, key1)
   uint32_t* __restrict__ chunk_cursor;        // work counter, zero before the launch
   unsigned long long* __restrict__ stats;     // kStatSlots, or null
   // radiance sink (kPower): per-ray power of each (face, side) as 64-bit
@@ -49,7 +48,7 @@ struct TraceParams {
   // scene's face_to_row of the hit face)
   const unsigned long long* __restrict__ power;
   unsigned long long* __restrict__ absorb;
-  SceneSlot scenes[kScenes];
+  SceneSlot scene;
 };
 
 constexpr int kTraceThreads = 128;
@@ -165,8 +164,8 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 #define FFB_TEST_PER_ITER 2
 #endif
 
-template <bool kSkip, int kScenes, bool kStats, bool kHash, bool kPower = false>
-__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams<kScenes> p)
+template <bool kSkip, bool kStats, bool kHash, bool kPower = false>
+__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams p)
 {
   extern __shared__ uint32_t s_hash[];  // kWarpsPerBlock x (keys, values) when kHash
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -182,16 +181,15 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
   const uint32_t epoch = p.epoch_ptr ? *p.epoch_ptr : p.epoch;
   const unsigned lane_below = (1u << lane) - 1u;
   int fill = 0;  // occupied slots (warp-uniform)
-  // current chunk and scene (warp-uniform)
+  // current chunk (warp-uniform)
   int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0;
-  int scene = 0;
+  const SceneSlot& S = p.scene;
   uint32_t key0 = p.key0, key1 = p.key1;
   if (p.scene_keys) {
     const uint2 k = p.scene_keys[0];
     key0 = k.x;
     key1 = k.y;
   }
-  int pending = -1;  // a fetched chunk of another scene, waiting for the warp to drain
   bool exhausted = false;
   // lane state
   Tracer T;
@@ -204,41 +202,21 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
       need = 0;
     while (need && !exhausted) {
       if (c_left == 0) {
-        int k = pending;
-        if (k < 0) {
-          if (lane == 0)
-            k = (int)atomicAdd(p.chunk_cursor, 1u);
-          k = __shfl_sync(kFull, k, 0);
-          if (k >= p.n_chunks) {
-            exhausted = true;
-            break;
-          }
+        int k = 0;
+        if (lane == 0)
+          k = (int)atomicAdd(p.chunk_cursor, 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= p.n_chunks) {
+          exhausted = true;
+          break;
         }
         const Chunk ch = p.chunks[k];
-        if (kScenes > 1 && ch.scene != scene) {
-          if (__any_sync(kFull, active)) {  // drain before switching scene
-            pending = k;
-            break;
-          }
-          if (kHash)
-            warp_hash_flush(keys, vals, p.scenes[scene].counts, lane);
-          fill = 0;
-          scene = ch.scene;
-          if (p.scene_keys) {
-            const uint2 sk = p.scene_keys[scene];
-            key0 = sk.x;
-            key1 = sk.y;
-          }
-        }
-        pending = -1;
-        const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
         c_face = ch.face;
         c_j = ch.j0;
         c_left = ch.count;
         c_front = ch.front;
         c_row = S.face_to_row ? __ldg(S.face_to_row + ch.face) : ch.face;
       }
-      const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
       const int take = min(__popc(need), c_left);
       const int rank = __popc(need & lane_below);
       const bool mine = ((need >> lane) & 1u) && rank < take;
@@ -256,7 +234,6 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     }
     if (exhausted && !__any_sync(kFull, active))
       break;
-    const SceneSlot& S = p.scenes[kScenes > 1 ? scene : 0];
     int hit = -1;
     if (active) {
       bool live = true;
@@ -297,7 +274,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     }
   }
   if (kHash)
-    warp_hash_flush(keys, vals, p.scenes[kScenes > 1 ? scene : 0].counts, lane);
+    warp_hash_flush(keys, vals, S.counts, lane);
   if (kStats)
     warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits, n_jumps);
 }

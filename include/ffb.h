@@ -168,9 +168,8 @@ int ffb_normalise(ffb_ctx* ctx, const uint32_t* counts, const int32_t* outgoing,
 int ffb_form_factors(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch,
                      int flags, const int32_t* face_to_row, int n_rows, const int32_t* outgoing, float* ff);
 
-/* Batched scenes: up to 256 independent scenes traced by ONE persistent
- * launch (BASELINE config "batched"), each with its own resident grid and
- * count matrix.  Scene s is faces [face_offsets[s], face_offsets[s+1]) of
+/* Batched scenes: up to 4096 independent scenes, each with its own resident
+ * grid and count matrix (BASELINE config "batched").  Scene s is faces [face_offsets[s], face_offsets[s+1]) of
  * faces9 (host or device); params: one ffb_grid_params per scene, or NULL
  * (automatic).  The batch is separate from the scene of the single-scene
  * calls above, which keep working. */
@@ -182,12 +181,14 @@ int ffb_batch_grid_info(ffb_ctx* ctx, int scene, ffb_grid_info* out);
  * per scene (host, or NULL for 1), emission flags.  Resets the device epoch
  * to 0 and synchronises. */
 int ffb_batch_prepare(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, const uint64_t* seeds, int flags);
-/* One fused launch over every prepared scene: zeroes `counts` (device,
- * counts_words uint32) and adds scene s's per-face counts into the N_s x N_s
- * matrix at counts + counts_offsets[s] (host offsets).  With advance_epoch the
- * device epoch is incremented first, so that successive launches -- or the
- * replays of a CUDA graph that captured this call -- draw fresh rays.  Only
- * enqueues work on the context stream (capturable). */
+/* Traces every prepared scene: zeroes `counts` (device, counts_words
+ * uint32) and adds scene s's per-face counts into the N_s x N_s matrix at
+ * counts + counts_offsets[s] (host offsets).  One fused launch per scene,
+ * largest first, dealt over four side streams forked from and joined back
+ * to the context stream, so that one scene's launch tail overlaps the next
+ * scenes.  With advance_epoch the device epoch is incremented first, so that
+ * successive calls -- or the replays of a CUDA graph that captured this
+ * call -- draw fresh rays.  Only enqueues work (capturable as one graph). */
 int ffb_batch_launch(ffb_ctx* ctx, uint32_t* counts, const unsigned long long* counts_offsets,
                      unsigned long long counts_words, int advance_epoch);
 
