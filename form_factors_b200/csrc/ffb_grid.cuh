@@ -13,8 +13,9 @@
 //  2. Hits are merged as a lexicographic minimum of (squared distance, index),
 //     which equals a strict '<' scan in index order.
 //  3. Traversal stops only when the best squared distance is below the squared
-//     distance at which the ray leaves the current cell, reduced by twice the
-//     margin; nothing in an unvisited cell can then compute a smaller one.
+//     distance at which the ray leaves the current cell (or the empty cube
+//     it jumps across), reduced by twice the margin; nothing in an unvisited
+//     cell can then compute a smaller one.
 #pragma once
 
 #include "ffb_device.cuh"
@@ -547,14 +548,14 @@ __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, fl
 // (persistent refill).
 //
 // Stopping rule: after a cell, stop when the best squared distance is below
-// the squared distance at which the ray leaves that cell, reduced by twice
-// the binning margin; any triangle not yet tested lies in unvisited cells and
-// cannot compute a smaller distance.
+// the squared distance at which the ray leaves that cell (or the empty cube
+// it is about to cross), reduced by twice the binning margin; any triangle
+// not yet tested lies in unvisited cells and cannot compute a smaller
+// distance.
 // ---------------------------------------------------------------------------
 struct Tracer {
   float3 o, dir, inv;
   float t1, dlen, best;
-  float tnx, tny, tnz;
   float3 best_pt;
   int cx, cy, cz;
   int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
@@ -595,9 +596,6 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.cx = cell_of(o.x + t0 * T.dir.x, g.lo.x, g.inv_cs.x, g.nx);
   T.cy = cell_of(o.y + t0 * T.dir.y, g.lo.y, g.inv_cs.y, g.ny);
   T.cz = cell_of(o.z + t0 * T.dir.z, g.lo.z, g.inv_cs.z, g.nz);
-  T.tnx = next_t(sgn(T.dir.x), T.cx, g.lo.x, g.cs.x, o.x, T.inv.x);
-  T.tny = next_t(sgn(T.dir.y), T.cy, g.lo.y, g.cs.y, o.y, T.inv.y);
-  T.tnz = next_t(sgn(T.dir.z), T.cz, g.lo.z, g.cs.z, o.z, T.inv.z);
   T.dlen = sqrtf(dot3(T.dir, T.dir));
   T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
   T.best_ref = -1;
@@ -642,76 +640,60 @@ __device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
 
 // The current cell is exhausted: stop, or move to the next cell.  Returns
 // false when the ray is finished.
+//
+// Every move leaves the empty cube of `jump` cells per side that extends
+// from the cell in the octant of the ray's direction (the cell itself when
+// jump <= 1: an occupied cell, or a plain DDA step).  The ray starts inside
+// the cube and moves monotonically, so it leaves through a far face, at tj,
+// and lands in the cell where it crosses that face.  A diagonal landing skips
+// only cells that the ray touches within rounding of the landing cell, whose
+// triangles the binning margin puts into the landing cell as well.  Lanes
+// that step and lanes that jump run the same instructions.
+//
+// Stopping rule, checked before the move: every reference whose computed
+// hit lies before tj, less twice the margin, is in a visited cell (the cube
+// holds none), so a best hit closer than that is final.
 template <bool kSkip>
 __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells, uint32_t& n_jumps)
 {
-  const float tx = fminf(fminf(T.tnx, T.tny), T.tnz);
+  const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
+  const int jump = max(T.jump, 1);
+  float ex = sx ? boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x) : INFINITY;
+  float ey = sy ? boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y) : INFINITY;
+  float ez = sz ? boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z) : INFINITY;
+  const float tj = fminf(fminf(ex, ey), ez);
   if (T.best_ref >= 0) {
-    const float L = fminf(tx, T.t1) * T.dlen - g.slack;
+    const float L = fminf(tj, T.t1) * T.dlen - g.slack;
     if (L > 0.f && T.best < L * L)
       return false;
   }
-  if (!(tx < T.t1) || --T.iters <= 0)
+  if (!(tj < T.t1) || --T.iters <= 0)
     return false;
-  const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
-  if (kSkip) {
-    // Every move leaves the empty cube of jump cells per side that extends
-    // from the cell in the octant of the ray's direction (the cell itself
-    // when jump <= 1, where the exit parameter is the DDA's next boundary).
-    // The ray starts inside it and moves monotonically, so it leaves through
-    // a far face; it lands in the cell where it crosses that face.  A diagonal landing skips only cells that the ray touches
-    // within rounding of the landing cell, whose triangles the binning margin
-    // puts into the landing cell as well.  Lanes that step and lanes that
-    // jump run the same instructions.
-    const int jump = max(T.jump, 1);
-    const float bx = boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x);
-    const float by = boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y);
-    const float bz = boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z);
-    const float tj = fminf(fminf(sx ? bx : INFINITY, sy ? by : INFINITY), sz ? bz : INFINITY);
-    if (!(tj < T.t1))
-      return false;
-    int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
-    int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
-    int nz = land(sz, T.cz, jump, T.o.z, T.dir.z, tj, g.lo.z, g.inv_cs.z);
-    if (nx == T.cx && ny == T.cy && nz == T.cz) {
-      // the landing point rounded back into the cell: one DDA step along the
-      // axis whose boundary comes first
-      const bool ax = T.tnx <= T.tny && T.tnx <= T.tnz;
-      const bool ay = !ax && T.tny <= T.tnz;
-      nx += ax ? sx : 0;
-      ny += ay ? sy : 0;
-      nz += (ax || ay) ? 0 : sz;
+  int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
+  int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
+  int nz = land(sz, T.cz, jump, T.o.z, T.dir.z, tj, g.lo.z, g.inv_cs.z);
+  if (nx == T.cx && ny == T.cy && nz == T.cz) {
+    // The landing point rounded back into the cell: one DDA step along the
+    // axis whose cell boundary the ray reaches first.  With jump 1 the cube
+    // exits are those boundaries; a longer jump lands in another cell unless
+    // rounding exceeds a cell, and then the cell's own boundaries decide.
+    if (jump > 1) {
+      ex = next_t(sx, T.cx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
+      ey = next_t(sy, T.cy, g.lo.y, g.cs.y, T.o.y, T.inv.y);
+      ez = next_t(sz, T.cz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
     }
-    if ((unsigned)nx >= (unsigned)g.nx || (unsigned)ny >= (unsigned)g.ny || (unsigned)nz >= (unsigned)g.nz)
-      return false;
-    n_jumps += jump >= 2;
-    T.cx = nx;
-    T.cy = ny;
-    T.cz = nz;
-    T.tnx = next_t(sx, nx, g.lo.x, g.cs.x, T.o.x, T.inv.x);
-    T.tny = next_t(sy, ny, g.lo.y, g.cs.y, T.o.y, T.inv.y);
-    T.tnz = next_t(sz, nz, g.lo.z, g.cs.z, T.o.z, T.inv.z);
-    ++n_cells;
-    tracer_enter<kSkip>(T, g);
-    return true;
+    const bool ax = ex <= ey && ex <= ez;
+    const bool ay = !ax && ey <= ez;
+    nx += ax ? sx : 0;
+    ny += ay ? sy : 0;
+    nz += (ax || ay) ? 0 : sz;
   }
-  // one DDA step along the axis whose boundary comes first, the axis chosen
-  // with selects so that lanes stepping along different axes run the same
-  // instructions
-  const bool ax = T.tnx <= T.tny && T.tnx <= T.tnz;
-  const bool ay = !ax && T.tny <= T.tnz;
-  const int s = ax ? sx : (ay ? sy : sz);
-  const int c = (ax ? T.cx : (ay ? T.cy : T.cz)) + s;
-  if ((unsigned)c >= (unsigned)(ax ? g.nx : (ay ? g.ny : g.nz)))
+  if ((unsigned)nx >= (unsigned)g.nx || (unsigned)ny >= (unsigned)g.ny || (unsigned)nz >= (unsigned)g.nz)
     return false;
-  const float tn = next_t(s, c, ax ? g.lo.x : (ay ? g.lo.y : g.lo.z), ax ? g.cs.x : (ay ? g.cs.y : g.cs.z),
-                          ax ? T.o.x : (ay ? T.o.y : T.o.z), ax ? T.inv.x : (ay ? T.inv.y : T.inv.z));
-  T.cx = ax ? c : T.cx;
-  T.cy = ay ? c : T.cy;
-  T.cz = (ax || ay) ? T.cz : c;
-  T.tnx = ax ? tn : T.tnx;
-  T.tny = ay ? tn : T.tny;
-  T.tnz = (ax || ay) ? T.tnz : tn;
+  n_jumps += jump >= 2;
+  T.cx = nx;
+  T.cy = ny;
+  T.cz = nz;
   ++n_cells;
   tracer_enter<kSkip>(T, g);
   return true;
