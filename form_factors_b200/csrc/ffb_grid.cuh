@@ -561,7 +561,7 @@ struct Tracer {
   int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
   int jump;          // empty-space distance of the current cell
   uint32_t i, en;    // pending references of the current cell
-  int iters;         // cells left before the hard stop
+  int sx, sy, sz;    // signs of the direction
 };
 
 template <bool kSkip>
@@ -590,6 +590,9 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.dir = sub3(e, o);
   float t0 = 0.f;
   T.t1 = INFINITY;
+  T.sx = sgn(T.dir.x);
+  T.sy = sgn(T.dir.y);
+  T.sz = sgn(T.dir.z);
   if (!slab(T.dir.x, o.x, g.lo.x, g.hi.x, T.inv.x, t0, T.t1) || !slab(T.dir.y, o.y, g.lo.y, g.hi.y, T.inv.y, t0, T.t1) ||
       !slab(T.dir.z, o.z, g.lo.z, g.hi.z, T.inv.z, t0, T.t1) || !(t0 <= T.t1))
     return false;
@@ -599,7 +602,6 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.dlen = sqrtf(dot3(T.dir, T.dir));
   T.best = 3.40282347e+38f;  // FLT_MAX, the reference's starting distance
   T.best_ref = -1;
-  T.iters = g.nx + g.ny + g.nz + 3;
   ++n_cells;
   tracer_enter<kSkip>(T, g);
   return true;
@@ -648,7 +650,10 @@ __device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
 // and lands in the cell where it crosses that face.  A diagonal landing skips
 // only cells that the ray touches within rounding of the landing cell, whose
 // triangles the binning margin puts into the landing cell as well.  Lanes
-// that step and lanes that jump run the same instructions.
+// that step and lanes that jump run the same instructions.  Every move
+// advances at least one cell coordinate in the ray's direction (landings are
+// clamped monotone, and a landing that rounds back becomes a step), so a ray
+// leaves the grid after at most nx + ny + nz moves.
 //
 // Stopping rule, checked before the move: every reference whose computed
 // hit lies before tj, less twice the margin, is in a visited cell (the cube
@@ -656,7 +661,7 @@ __device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
 template <bool kSkip>
 __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells, uint32_t& n_jumps)
 {
-  const int sx = sgn(T.dir.x), sy = sgn(T.dir.y), sz = sgn(T.dir.z);
+  const int sx = T.sx, sy = T.sy, sz = T.sz;
   const int jump = max(T.jump, 1);
   float ex = sx ? boundary_t(g.lo.x, sx > 0 ? T.cx + jump : T.cx - jump + 1, g.cs.x, T.o.x, T.inv.x) : INFINITY;
   float ey = sy ? boundary_t(g.lo.y, sy > 0 ? T.cy + jump : T.cy - jump + 1, g.cs.y, T.o.y, T.inv.y) : INFINITY;
@@ -667,7 +672,7 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
     if (L > 0.f && T.best < L * L)
       return false;
   }
-  if (!(tj < T.t1) || --T.iters <= 0)
+  if (!(tj < T.t1))
     return false;
   int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
   int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
