@@ -106,8 +106,8 @@ __device__ __forceinline__ bool tri_hit_regs(const float4 q0, const float4 q1, c
   const float uu = q0.w, uv = q1.w, vv = q2.w, D = q3.w;
   const float ns = uv * wv - vv * wu;
   const float nt = uv * wu - uu * wv;
-  const bool out = (fabsf(b) < FFB_EPS_ABOVE_1E8) | surely_negative(a, b) | (r < 0.f) | surely_negative(ns, D) |
-                   surely_above_one(ns, D) | surely_negative(nt, D);
+  const bool out = (fabsf(b) < FFB_EPS_ABOVE_1E8) | (r < 0.f) | surely_negative(ns, D) | surely_above_one(ns, D) |
+                   surely_negative(nt, D);
   if (out)
     return false;
   float s = ns / D;

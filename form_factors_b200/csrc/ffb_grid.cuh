@@ -555,7 +555,7 @@ __device__ __forceinline__ int land(int s, int c, int jump, float o, float d, fl
 // ---------------------------------------------------------------------------
 struct Tracer {
   float3 o, dir, inv;
-  float t1, dlen, best;
+  float dlen, best;
   float3 best_pt;
   int cx, cy, cz;
   int best_ref;      // reference (position in ref_tri) of the best hit, -1 if none
@@ -589,12 +589,12 @@ __device__ __forceinline__ bool tracer_begin(Tracer& T, const GridView& g, float
   T.o = o;
   T.dir = sub3(e, o);
   float t0 = 0.f;
-  T.t1 = INFINITY;
+  float t1 = INFINITY;
   T.sx = sgn(T.dir.x);
   T.sy = sgn(T.dir.y);
   T.sz = sgn(T.dir.z);
-  if (!slab(T.dir.x, o.x, g.lo.x, g.hi.x, T.inv.x, t0, T.t1) || !slab(T.dir.y, o.y, g.lo.y, g.hi.y, T.inv.y, t0, T.t1) ||
-      !slab(T.dir.z, o.z, g.lo.z, g.hi.z, T.inv.z, t0, T.t1) || !(t0 <= T.t1))
+  if (!slab(T.dir.x, o.x, g.lo.x, g.hi.x, T.inv.x, t0, t1) || !slab(T.dir.y, o.y, g.lo.y, g.hi.y, T.inv.y, t0, t1) ||
+      !slab(T.dir.z, o.z, g.lo.z, g.hi.z, T.inv.z, t0, t1) || !(t0 <= t1))
     return false;
   T.cx = cell_of(o.x + t0 * T.dir.x, g.lo.x, g.inv_cs.x, g.nx);
   T.cy = cell_of(o.y + t0 * T.dir.y, g.lo.y, g.inv_cs.y, g.ny);
@@ -657,7 +657,9 @@ __device__ __forceinline__ int tracer_result(const Tracer& T, const GridView& g)
 //
 // Stopping rule, checked before the move: every reference whose computed
 // hit lies before tj, less twice the margin, is in a visited cell (the cube
-// holds none), so a best hit closer than that is final.
+// holds none, and nothing lies outside the grid), so a best hit closer than
+// that is final.  A ray that leaves the grid lands outside it and stops at
+// the bounds check.
 template <bool kSkip>
 __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uint32_t& n_cells, uint32_t& n_jumps)
 {
@@ -668,11 +670,11 @@ __device__ __forceinline__ bool tracer_advance(Tracer& T, const GridView& g, uin
   float ez = sz ? boundary_t(g.lo.z, sz > 0 ? T.cz + jump : T.cz - jump + 1, g.cs.z, T.o.z, T.inv.z) : INFINITY;
   const float tj = fminf(fminf(ex, ey), ez);
   if (T.best_ref >= 0) {
-    const float L = fminf(tj, T.t1) * T.dlen - g.slack;
+    const float L = tj * T.dlen - g.slack;
     if (L > 0.f && T.best < L * L)
       return false;
   }
-  if (!(tj < T.t1))
+  if (!(tj < INFINITY))
     return false;
   int nx = land(sx, T.cx, jump, T.o.x, T.dir.x, tj, g.lo.x, g.inv_cs.x);
   int ny = land(sy, T.cy, jump, T.o.y, T.dir.y, tj, g.lo.y, g.inv_cs.y);
