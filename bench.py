@@ -384,7 +384,8 @@ def csv_section(ctx, stream, counts, front, rear, n):
         "workload": "CSV text of the %dx%d matrix of this step (csv_export::export_csv format)" % (n, n),
         "entries": entries, "text_bytes": int(n_text),
         "format_ms": fmt_s * 1e3, "format_entries_per_s": entries / fmt_s,
-        "roofline": {"bound": "hbm", "achieved": alg_bytes / fmt_s / 1e9, "peak": measured_hbm_gbs(), "unit": "GB/s",
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / fmt_s / 1e9, "peak": measured_hbm_gbs(),
+                     "peak_source": hbm_peak()[1], "unit": "GB/s",
                      "frac": alg_bytes / fmt_s / 1e9 / measured_hbm_gbs(),
                      "work": "4 B count read + text bytes written per entry (algorithmic)"},
         "export_s": exp_s, "export_entries_per_s": entries / exp_s, "export_bytes": size, "export_dir": where,
@@ -531,10 +532,16 @@ def fp32_peak(device):
 
 def measured_hbm_gbs():
     """Copy bandwidth of this pool's B200s, measured by the driver (GB/s)."""
+    return hbm_peak()[0]
+
+
+def hbm_peak():
+    """(GB/s, source): MEASURED_PEAKS.json's copy bandwidth, else the
+    fallback measured earlier on this pool."""
     try:
-        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
     except (OSError, ValueError, KeyError):
-        return 6650.0  # earlier measurement on this pool
+        return 6650.0, "fallback"
 
 
 def traffic_per_launch():
@@ -694,7 +701,8 @@ def ours(args):
                          "hbm": {"achieved_gbs": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9,
                                  "peak_gbs": measured_hbm_gbs(),
                                  "frac": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
-                                 "note": "DRAM bytes per launch (ncu) / kernel time, of measured copy bandwidth"}},
+                                 "peak_source": hbm_peak()[1],
+                                 "note": "DRAM bytes per launch (ncu) / kernel time, of the copy bandwidth"}},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,
             "hit_fraction": hits / rays_per_step,

@@ -1573,13 +1573,13 @@ namespace {
 
 constexpr int kCsvSegmentTiles = 4096;  // tiles per staged segment (16.8 M entries, <= 218 MB of text)
 
-// Formats the n x n matrix of `src`.  One length pass and one scan cover the
-// whole matrix; then the text goes to a device buffer in one launch, or, for
-// a host buffer or a file, segment by segment through a device staging
-// buffer (a file gets pinned double buffers: the host writes one segment
-// while the GPU formats the next).  Exactly one sink is used: text (device
-// or host, cap bytes), file, or neither (length only).  *total gets the
-// text length.
+// Formats the n x n matrix of `src`.  A device buffer gets the text from one
+// single-pass launch (k_csv_fused).  Otherwise one length pass and one scan
+// cover the whole matrix; then the text goes, for a host buffer or a file,
+// segment by segment through a device staging buffer (a file gets pinned
+// double buffers: the host writes one segment while the GPU formats the
+// next).  Exactly one sink is used: text (device or host, cap bytes), file,
+// or neither (length only).  *total gets the text length.
 int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FILE* file, unsigned long long* total)
 {
   // per device (the attribute belongs to the current device); cheap to repeat
@@ -1591,6 +1591,35 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
   FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (size_t)(n_tiles + 2)));
   auto* tile_len = dptr<unsigned long long>(c->csv_tile_len);
   auto* tile_off = dptr<unsigned long long>(c->csv_tile_off);
+  if (text && is_device_ptr(text)) {
+    // one pass: the tile-length buffer holds the look-back status words; the
+    // first two words of the offset buffer the ticket and error bits, then
+    // the total
+    FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)csv::kFusedSmem));
+    FFB_CUDA(cudaMemsetAsync(tile_len, 0, sizeof(unsigned long long) * (size_t)n_tiles, c->stream));
+    FFB_CUDA(cudaMemsetAsync(tile_off, 0, 2 * sizeof(unsigned long long), c->stream));
+    csv::FusedSink sink;
+    sink.text = text;
+    sink.cap = cap;
+    sink.status = tile_len;
+    sink.ticket = reinterpret_cast<unsigned int*>(tile_off);
+    sink.err = reinterpret_cast<unsigned int*>(tile_off) + 1;
+    sink.total = tile_off + 1;
+    sink.n_tiles = n_tiles;
+    csv::k_csv_fused<<<(unsigned)n_tiles, csv::kThreads, csv::kFusedSmem, c->stream>>>(src, sink);
+    FFB_CUDA(cudaGetLastError());
+    unsigned long long aux[2] = {0, 0};  // {ticket | err << 32, total}
+    FFB_CUDA(cudaMemcpyAsync(aux, tile_off, sizeof aux, cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+    *total = aux[1];
+    const unsigned err = (unsigned)(aux[0] >> 32);
+    if (err & csv::kFusedTimeout)
+      return fail(FFB_ERR_TIMEOUT, "CSV formatting: a tile's offset never arrived");
+    if (err & csv::kFusedOverflow)
+      return fail(FFB_ERR_ARG, "CSV text of %llu bytes does not fit the %llu-byte buffer", aux[1], cap);
+    return FFB_OK;
+  }
   csv::k_csv_len<<<(unsigned)n_tiles, csv::kThreads, 0, c->stream>>>(src, tile_len);
   csv::k_csv_scan<<<1, csv::kScanThreads, 0, c->stream>>>(tile_len, (int)n_tiles, tile_off);
   FFB_CUDA(cudaGetLastError());
@@ -1606,12 +1635,6 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
     return FFB_OK;
   if (text && all > cap)
     return fail(FFB_ERR_ARG, "CSV text of %llu bytes does not fit the %llu-byte buffer", all, cap);
-  if (text && is_device_ptr(text)) {
-    csv::k_csv_write<<<(unsigned)n_tiles, csv::kThreads, smem, c->stream>>>(src, tile_off, 0, 0, region, text);
-    FFB_CUDA(cudaGetLastError());
-    FFB_CUDA(cudaStreamSynchronize(c->stream));
-    return FFB_OK;
-  }
   // staged: segment byte ranges from the tile offsets
   std::vector<unsigned long long> off((size_t)n_tiles + 1);
   FFB_CUDA(cudaMemcpy(off.data(), tile_off, sizeof(unsigned long long) * off.size(), cudaMemcpyDeviceToHost));

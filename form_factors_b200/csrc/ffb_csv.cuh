@@ -315,7 +315,8 @@ __host__ __device__ inline int format_g6_len(float f)
 #ifdef __CUDACC__
 // ---------------------------------------------------------------------------
 // Kernels.  The matrix (row-major entries) is cut into tiles of kTile
-// entries, one block each.
+// entries, one block each.  A device buffer gets its text from k_csv_fused
+// (one pass, below); lengths, host buffers and files use:
 //  1. k_csv_len: the text length of every tile.
 //  2. k_csv_scan: exclusive prefix sums of the tile lengths (64-bit) and the
 //     total.
@@ -615,6 +616,240 @@ __global__ void __launch_bounds__(kThreads, 4) k_csv_write(Source s, const unsig
     dv[i] = sv[i];
   for (uint32_t i = head + 16u * body + threadIdx.x; i < L; i += kThreads)
     dst[i] = (char)sbuf[shift + i];
+}
+
+// ---------------------------------------------------------------------------
+// Single pass into a device buffer (decoupled look-back).  Each block takes
+// the next tile by ticket, so every tile it waits for already runs and waits
+// only for earlier tiles.  Thread t holds entries [16t, 16t + 16) of its
+// tile, so its text is one contiguous run whose offset comes from a block
+// scan of 16-entry sums; +0 entries ("0" and the separator) are written by
+// their thread, the others formatted densely through the block queue (once
+// for the length, once for the text).  The tile publishes its length and
+// lays its text out in shared memory; then it sums the lengths and prefixes
+// the preceding tiles published (bounded polls), publishes its inclusive
+// prefix and stores its text with 16-byte writes.  A tile whose text would
+// pass the end of the buffer writes nothing and sets kFusedOverflow; the
+// last tile writes the text length.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kTileAgg = 1ull << 62;     // status: the tile's own length
+constexpr unsigned long long kTilePrefix = 2ull << 62;  // status: the inclusive prefix
+constexpr unsigned long long kTileValue = (1ull << 62) - 1;
+constexpr unsigned kLookbackPolls = 1u << 22;           // polls of one status word before giving up
+enum : unsigned { kFusedTimeout = 1u, kFusedOverflow = 2u };
+constexpr int kRun = 16;                                 // consecutive entries per thread
+static_assert(kRun * kThreads == kTile, "a tile is one run per thread");
+constexpr int kFusedText = kTile * (kMaxEntry - 3) + 16;  // staged text of a tile at most, + one word read past it
+static_assert(kFusedText % 16 == 0, "the length bytes start 16-byte aligned");
+constexpr size_t kFusedSmem = kFusedText + kTile * (sizeof(uint8_t) + sizeof(uint16_t)) + kThreads * sizeof(uint32_t);
+
+struct FusedSink {
+  char* text;
+  unsigned long long cap;
+  unsigned long long* status;  // one word per tile, zero before the launch
+  unsigned int* ticket;        // zero before the launch
+  unsigned int* err;           // kFused* bits, zero before the launch
+  unsigned long long* total;   // the text length, written by the last tile
+  long long n_tiles;
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p)
+{
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v)
+{
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive prefix of `tile` from the status words of the tiles before it;
+// run by one full warp after the tile's own length was published.
+__device__ __forceinline__ unsigned long long look_back(const FusedSink& out, long long tile, int lane)
+{
+  unsigned long long excl = 0;
+  for (long long j = tile - 1;; j -= 32) {
+    const long long idx = j - lane;
+    unsigned long long w = kTilePrefix;  // before the first tile: prefix 0
+    if (idx >= 0) {
+      unsigned polls = 0;
+      do {
+        w = ld_relaxed(out.status + idx);
+      } while ((w >> 62) == 0 && ++polls < kLookbackPolls);
+    }
+    if (__any_sync(0xFFFFFFFFu, (w >> 62) == 0)) {  // a tile never published: give up
+      if (lane == 0)
+        atomicOr(out.err, kFusedTimeout);
+      return excl;
+    }
+    // lane 0 is the nearest tile; stop at the nearest one with a prefix
+    const unsigned pm = __ballot_sync(0xFFFFFFFFu, (w >> 62) == 2);
+    unsigned long long v = w & kTileValue;
+    if (pm && lane > __ffs(pm) - 1)
+      v = 0;
+    for (int d = 16; d > 0; d >>= 1)
+      v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
+    excl += v;
+    if (pm)
+      return excl;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink out)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* sbuf = smem;                                         // staged text
+  uint8_t* len = smem + kFusedText;                                   // entry lengths, run by run
+  uint16_t* queue = reinterpret_cast<uint16_t*>(len + kTile);         // nonzero entries
+  uint32_t* toff = reinterpret_cast<uint32_t*>(queue + kTile);       // staged offset of each run
+  __shared__ uint32_t qn;
+  __shared__ long long s_tile;
+  __shared__ unsigned long long s_prefix;
+  __shared__ uint32_t warp_sum[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    qn = 0;
+    s_tile = (long long)atomicAdd(out.ticket, 1u);
+  }
+  __syncthreads();
+  const long long tile = s_tile;
+  // 1. the run's entries, their +0 / row-end flags and the +0 lengths
+  const int o0 = kRun * (int)threadIdx.x;
+  const long long e0 = tile * kTile + o0;
+  const uint32_t* words = s.ff ? reinterpret_cast<const uint32_t*>(s.ff) : s.counts;
+  uint32_t raw[kRun];
+  if (e0 + kRun <= s.n_entries && ((uintptr_t)(words + e0) & 15u) == 0) {
+    const uint4* p = reinterpret_cast<const uint4*>(words + e0);
+#pragma unroll
+    for (int j = 0; j < kRun / 4; ++j) {
+      const uint4 w = __ldg(p + j);
+      raw[4 * j] = w.x;
+      raw[4 * j + 1] = w.y;
+      raw[4 * j + 2] = w.z;
+      raw[4 * j + 3] = w.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kRun; ++k)
+      raw[k] = e0 + k < s.n_entries ? __ldg(words + e0 + k) : 0u;
+  }
+  int row = (int)(e0 / s.n), col = (int)(e0 - (long long)row * s.n);
+  float ratio = (!s.ff && row < s.n) ? row_ratio(s, row) : 1.f;
+  uint32_t zero_mask = 0, end_mask = 0, lens[kRun / 4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int k = 0; k < kRun; ++k) {
+    const bool valid = e0 + k < s.n_entries;
+    const float v = s.ff ? __uint_as_float(raw[k]) : (float)raw[k] * ratio;
+    const bool zero = valid && __float_as_uint(v) == 0u;
+    zero_mask |= zero ? 1u << k : 0u;
+    end_mask |= col == s.n - 1 ? 1u << k : 0u;
+    lens[k >> 2] |= zero ? 2u << (8 * (k & 3)) : 0u;
+    enqueue(queue, &qn, valid && !zero, o0 + k);
+    if (++col == s.n) {
+      col = 0;
+      ++row;
+      if (!s.ff && row < s.n)
+        ratio = row_ratio(s, row);
+    }
+  }
+  *reinterpret_cast<uint4*>(len + o0) = make_uint4(lens[0], lens[1], lens[2], lens[3]);
+  __syncthreads();
+  const uint32_t n_q = qn;
+  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+    const int o = queue[q];
+    int c;
+    len[o] = (uint8_t)(format_g6_len(tile_value(s, tile, o, &c)) + 1);
+  }
+  __syncthreads();
+  // 2. run lengths, the tile's length and each run's offset in the tile
+  const uint4 lw = *reinterpret_cast<const uint4*>(len + o0);
+  const uint32_t run_len[4] = {lw.x, lw.y, lw.z, lw.w};  // four entry lengths per word
+  const uint32_t mine = __dp4a(lw.x, 0x01010101u, __dp4a(lw.y, 0x01010101u, __dp4a(lw.z, 0x01010101u,
+                                                                                  __dp4a(lw.w, 0x01010101u, 0u))));
+  uint32_t incl = mine;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= d)
+      incl += y;
+  }
+  if (lane == 31)
+    warp_sum[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+  for (int w = 0; w < kThreads / 32; ++w) {
+    const uint32_t u = warp_sum[w];
+    before += w < warp ? u : 0u;
+    total += u;
+  }
+  // 3. publish the tile's length; its text is staged from offset 0 while
+  // the tiles before it finish
+  if (threadIdx.x == 0)
+    st_relaxed(out.status + tile, (tile == 0 ? kTilePrefix : kTileAgg) | total);
+  uint32_t pos = before + incl - mine;
+  toff[threadIdx.x] = pos;
+#pragma unroll
+  for (int k = 0; k < kRun; ++k) {
+    if ((zero_mask >> k) & 1u) {
+      sbuf[pos] = '0';
+      sbuf[pos + 1] = ((end_mask >> k) & 1u) ? '\n' : ';';
+    }
+    pos += (run_len[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+  }
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+    const int o = queue[q];
+    const int t = o / kRun;
+    uint32_t at = toff[t];
+    for (int j = t * kRun; j < o; ++j)
+      at += len[j];
+    int c;
+    const float v = tile_value(s, tile, o, &c);
+    PtrOut w{reinterpret_cast<char*>(sbuf + at), 0};
+    format_g6_to(v, w);
+    w.put(c == s.n - 1 ? '\n' : ';');
+  }
+  // 4. the tile's place in the text
+  if (warp == 0) {
+    unsigned long long excl = 0;
+    if (tile > 0) {
+      excl = look_back(out, tile, lane);
+      if (lane == 0)
+        st_relaxed(out.status + tile, kTilePrefix | (excl + total));
+    }
+    if (lane == 0) {
+      s_prefix = excl;
+      if (tile == out.n_tiles - 1)
+        *out.total = excl + total;
+    }
+  }
+  __syncthreads();
+  const unsigned long long P = s_prefix;
+  if (P + total > out.cap) {
+    if (threadIdx.x == 0)
+      atomicOr(out.err, kFusedOverflow);
+    return;
+  }
+  // 5. copy the staged text to text + P: bytes up to the first 16-byte
+  // boundary, then 16-byte stores assembled from 32-bit shared words
+  // (funnel shifts by the staged offset's misalignment), then the tail
+  char* dst = out.text + P;
+  const uint32_t head = min(total, (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u));
+  const uint32_t body = (total - head) >> 4;
+  for (uint32_t i = threadIdx.x; i < head; i += kThreads)
+    dst[i] = (char)sbuf[i];
+  const uint32_t r8 = 8u * (head & 3u);
+  const uint32_t* sw = reinterpret_cast<const uint32_t*>(sbuf) + (head >> 2);
+  uint4* dv = reinterpret_cast<uint4*>(dst + head);
+  for (uint32_t i = threadIdx.x; i < body; i += kThreads) {
+    const uint32_t* w = sw + 4 * i;
+    const uint32_t a0 = w[0], a1 = w[1], a2 = w[2], a3 = w[3], a4 = w[4];
+    dv[i] = make_uint4(__funnelshift_r(a0, a1, r8), __funnelshift_r(a1, a2, r8), __funnelshift_r(a2, a3, r8),
+                       __funnelshift_r(a3, a4, r8));
+  }
+  for (uint32_t i = head + 16u * body + threadIdx.x; i < total; i += kThreads)
+    dst[i] = (char)sbuf[i];
 }
 #endif  // __CUDACC__
 

@@ -354,7 +354,8 @@ int ffb_obj_scene_set(ffb_ctx* ctx);
  * buffer of text_cap bytes, or NULL to get only the length in *text_len.
  * ffb_csv_format_counts: the same for counts normalised on the fly by their
  * row's outgoing rays, as ffb_normalise computes them (no float matrix is
- * formed).  FFB_ERR_ARG if the text does not fit text_cap.
+ * formed).  FFB_ERR_ARG if the text does not fit text_cap (*text_len then
+ * holds the length needed; a device buffer may hold part of the text).
  * ffb_csv_export / ffb_csv_export_counts: write the text to `filename`
  * (created or truncated); FFB_ERR_FILE when it cannot be opened or written,
  * where the reference returns -CSV_EXPORT_FILE_ERROR.  n == 0 writes an empty
