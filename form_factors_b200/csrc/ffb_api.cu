@@ -1587,7 +1587,8 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
                                 (int)csv::write_smem(csv::kTileBytes)));
   src.n_entries = (long long)src.n * src.n;
   const long long n_tiles = (src.n_entries + csv::kTile - 1) / csv::kTile;
-  FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * (size_t)n_tiles));
+  const long long n_fused = (src.n_entries + csv::kFusedTile - 1) / csv::kFusedTile;
+  FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * (size_t)std::max(n_tiles, n_fused)));
   FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (size_t)(n_tiles + 2)));
   auto* tile_len = dptr<unsigned long long>(c->csv_tile_len);
   auto* tile_off = dptr<unsigned long long>(c->csv_tile_off);
@@ -1597,7 +1598,7 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
     // the total
     FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)csv::kFusedSmem));
-    FFB_CUDA(cudaMemsetAsync(tile_len, 0, sizeof(unsigned long long) * (size_t)n_tiles, c->stream));
+    FFB_CUDA(cudaMemsetAsync(tile_len, 0, sizeof(unsigned long long) * (size_t)n_fused, c->stream));
     FFB_CUDA(cudaMemsetAsync(tile_off, 0, 2 * sizeof(unsigned long long), c->stream));
     csv::FusedSink sink;
     sink.text = text;
@@ -1606,8 +1607,8 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
     sink.ticket = reinterpret_cast<unsigned int*>(tile_off);
     sink.err = reinterpret_cast<unsigned int*>(tile_off) + 1;
     sink.total = tile_off + 1;
-    sink.n_tiles = n_tiles;
-    csv::k_csv_fused<<<(unsigned)n_tiles, csv::kThreads, csv::kFusedSmem, c->stream>>>(src, sink);
+    sink.n_tiles = n_fused;
+    csv::k_csv_fused<<<(unsigned)n_fused, csv::kFusedThreads, csv::kFusedSmem, c->stream>>>(src, sink);
     FFB_CUDA(cudaGetLastError());
     unsigned long long aux[2] = {0, 0};  // {ticket | err << 32, total}
     FFB_CUDA(cudaMemcpyAsync(aux, tile_off, sizeof aux, cudaMemcpyDeviceToHost, c->stream));

@@ -637,11 +637,19 @@ constexpr unsigned long long kTilePrefix = 2ull << 62;  // status: the inclusive
 constexpr unsigned long long kTileValue = (1ull << 62) - 1;
 constexpr unsigned kLookbackPolls = 1u << 22;           // polls of one status word before giving up
 enum : unsigned { kFusedTimeout = 1u, kFusedOverflow = 2u };
-constexpr int kRun = 16;                                 // consecutive entries per thread
-static_assert(kRun * kThreads == kTile, "a tile is one run per thread");
-constexpr int kFusedText = kTile * (kMaxEntry - 3) + 16;  // staged text of a tile at most, + one word read past it
+constexpr int kRun = 16;  // consecutive entries per thread
+#ifndef FFB_CSV_THREADS
+#define FFB_CSV_THREADS 256
+#endif
+#ifndef FFB_CSV_BLOCKS
+#define FFB_CSV_BLOCKS 3
+#endif
+constexpr int kFusedThreads = FFB_CSV_THREADS;
+constexpr int kFusedTile = kRun * kFusedThreads;              // entries per tile, one run per thread
+constexpr int kFusedText = kFusedTile * (kMaxEntry - 3) + 16;  // staged text of a tile at most, + one word read past it
 static_assert(kFusedText % 16 == 0, "the length bytes start 16-byte aligned");
-constexpr size_t kFusedSmem = kFusedText + kTile * (sizeof(uint8_t) + sizeof(uint16_t)) + kThreads * sizeof(uint32_t);
+constexpr size_t kFusedSmem =
+    kFusedText + kFusedTile * (sizeof(uint8_t) + sizeof(uint16_t)) + kFusedThreads * sizeof(uint32_t);
 
 struct FusedSink {
   char* text;
@@ -697,17 +705,26 @@ __device__ __forceinline__ unsigned long long look_back(const FusedSink& out, lo
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink out)
+// Value and column of entry o of a fused tile (queue work, one division).
+__device__ __forceinline__ float fused_value(const Source& s, long long tile, int o, int* col)
+{
+  const long long e = tile * kFusedTile + o;
+  const int row = (int)(e / s.n);
+  *col = (int)(e - (long long)row * s.n);
+  return entry_value(s, e, row_ratio(s, row));
+}
+
+__global__ void __launch_bounds__(kFusedThreads, FFB_CSV_BLOCKS) k_csv_fused(Source s, FusedSink out)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* sbuf = smem;                                         // staged text
   uint8_t* len = smem + kFusedText;                                   // entry lengths, run by run
-  uint16_t* queue = reinterpret_cast<uint16_t*>(len + kTile);         // nonzero entries
-  uint32_t* toff = reinterpret_cast<uint32_t*>(queue + kTile);       // staged offset of each run
+  uint16_t* queue = reinterpret_cast<uint16_t*>(len + kFusedTile);    // nonzero entries
+  uint32_t* toff = reinterpret_cast<uint32_t*>(queue + kFusedTile);  // staged offset of each run
   __shared__ uint32_t qn;
   __shared__ long long s_tile;
   __shared__ unsigned long long s_prefix;
-  __shared__ uint32_t warp_sum[kThreads / 32];
+  __shared__ uint32_t warp_sum[kFusedThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     qn = 0;
@@ -717,7 +734,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink o
   const long long tile = s_tile;
   // 1. the run's entries, their +0 / row-end flags and the +0 lengths
   const int o0 = kRun * (int)threadIdx.x;
-  const long long e0 = tile * kTile + o0;
+  const long long e0 = tile * kFusedTile + o0;
   const uint32_t* words = s.ff ? reinterpret_cast<const uint32_t*>(s.ff) : s.counts;
   uint32_t raw[kRun];
   if (e0 + kRun <= s.n_entries && ((uintptr_t)(words + e0) & 15u) == 0) {
@@ -757,10 +774,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink o
   *reinterpret_cast<uint4*>(len + o0) = make_uint4(lens[0], lens[1], lens[2], lens[3]);
   __syncthreads();
   const uint32_t n_q = qn;
-  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+  for (uint32_t q = threadIdx.x; q < n_q; q += kFusedThreads) {
     const int o = queue[q];
     int c;
-    len[o] = (uint8_t)(format_g6_len(tile_value(s, tile, o, &c)) + 1);
+    len[o] = (uint8_t)(format_g6_len(fused_value(s, tile, o, &c)) + 1);
   }
   __syncthreads();
   // 2. run lengths, the tile's length and each run's offset in the tile
@@ -778,7 +795,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink o
     warp_sum[warp] = incl;
   __syncthreads();
   uint32_t before = 0, total = 0;
-  for (int w = 0; w < kThreads / 32; ++w) {
+  for (int w = 0; w < kFusedThreads / 32; ++w) {
     const uint32_t u = warp_sum[w];
     before += w < warp ? u : 0u;
     total += u;
@@ -798,14 +815,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink o
     pos += (run_len[k >> 2] >> (8 * (k & 3))) & 0xFFu;
   }
   __syncthreads();
-  for (uint32_t q = threadIdx.x; q < n_q; q += kThreads) {
+  for (uint32_t q = threadIdx.x; q < n_q; q += kFusedThreads) {
     const int o = queue[q];
     const int t = o / kRun;
     uint32_t at = toff[t];
     for (int j = t * kRun; j < o; ++j)
       at += len[j];
     int c;
-    const float v = tile_value(s, tile, o, &c);
+    const float v = fused_value(s, tile, o, &c);
     PtrOut w{reinterpret_cast<char*>(sbuf + at), 0};
     format_g6_to(v, w);
     w.put(c == s.n - 1 ? '\n' : ';');
@@ -837,18 +854,18 @@ __global__ void __launch_bounds__(kThreads, 3) k_csv_fused(Source s, FusedSink o
   char* dst = out.text + P;
   const uint32_t head = min(total, (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u));
   const uint32_t body = (total - head) >> 4;
-  for (uint32_t i = threadIdx.x; i < head; i += kThreads)
+  for (uint32_t i = threadIdx.x; i < head; i += kFusedThreads)
     dst[i] = (char)sbuf[i];
   const uint32_t r8 = 8u * (head & 3u);
   const uint32_t* sw = reinterpret_cast<const uint32_t*>(sbuf) + (head >> 2);
   uint4* dv = reinterpret_cast<uint4*>(dst + head);
-  for (uint32_t i = threadIdx.x; i < body; i += kThreads) {
+  for (uint32_t i = threadIdx.x; i < body; i += kFusedThreads) {
     const uint32_t* w = sw + 4 * i;
     const uint32_t a0 = w[0], a1 = w[1], a2 = w[2], a3 = w[3], a4 = w[4];
     dv[i] = make_uint4(__funnelshift_r(a0, a1, r8), __funnelshift_r(a1, a2, r8), __funnelshift_r(a2, a3, r8),
                        __funnelshift_r(a3, a4, r8));
   }
-  for (uint32_t i = head + 16u * body + threadIdx.x; i < total; i += kThreads)
+  for (uint32_t i = head + 16u * body + threadIdx.x; i < total; i += kFusedThreads)
     dst[i] = (char)sbuf[i];
 }
 #endif  // __CUDACC__
