@@ -407,9 +407,12 @@ def thermal_section(ctx, faces, rays_per_face):
     from oracle_lib import Reference
     n = len(faces)
     n_sphere = n - 1600  # the two 20 x 20 plates come last
-    meshes = [(f, 1, 0 if f < n_sphere else 1) for f in range(n)]
+    # one mesh per face as (first face, face count, material), built once as
+    # the ffb_mesh layout: the scene is fixed across the controller's steps
+    meshes = np.stack([np.arange(n), np.ones(n, np.int64), (np.arange(n) >= n_sphere).astype(np.int64)],
+                      axis=1).astype(np.int32)
     # sphere: inward emitter only, so that every ray starts inside the scene
-    materials = [(0.9, 0.0, 0.8, 0.8), (0.7, 0.6, 0.5, 0.4)]
+    materials = np.array([(0.9, 0.0, 0.8, 0.8), (0.7, 0.6, 0.5, 0.4)], np.float32)
     temps = (300.0 + 100.0 * np.random.default_rng(5).random(n)).astype(np.float32)
     n_rays = rays_per_face * n
     ctx.radiance_step(faces, meshes, materials, temps, n_rays, seed=1, epoch=0)  # warm-up
