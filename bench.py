@@ -557,6 +557,27 @@ def traffic_per_launch():
         return None
 
 
+def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm):
+    """The bound the fused kernel meets: instruction issue.  Warp
+    instructions per ray from the committed ncu summary (profiles/
+    traffic.json) x rays per launch / kernel time, against 4 issue slots per
+    SM per cycle at the SM clock sampled during the timed region.  None when
+    an input is missing."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        ipr = float(d["k_form_factors_warp_inst_per_ray"])
+        if not sm_mhz or not k_ms or not n_sm:
+            return None
+        achieved = ipr * rays_per_launch / (k_ms * 1e-3)
+        peak = 4.0 * n_sm * float(sm_mhz) * 1e6
+        return {"achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G warp instructions/s",
+                "frac": achieved / peak, "warp_inst_per_ray": ipr,
+                "note": "instructions per ray from ncu (profiles/k_form_factors_enclosure.md); peak = 4 x SMs x "
+                        "sampled SM clock"}
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
+
+
 def ours(args):
     import torch
     import torch.distributed as dist
@@ -705,7 +726,9 @@ def ours(args):
                                  "peak_gbs": measured_hbm_gbs(),
                                  "frac": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
                                  "peak_source": hbm_peak()[1],
-                                 "note": "DRAM bytes per launch (ncu) / kernel time, of the copy bandwidth"}},
+                                 "note": "DRAM bytes per launch (ncu) / kernel time, of the copy bandwidth"},
+                         "issue": issue_roofline(k_ms, rays_per_step, clk.get("sm_mhz"),
+                                                 torch.cuda.get_device_properties(local).multi_processor_count)},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,
             "hit_fraction": hits / rays_per_step,
