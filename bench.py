@@ -673,10 +673,9 @@ def ours(args):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # host -> device per step: the 16-byte work chunks (256 rays each) built
-    # from the host ray counts
-    n_chunks = sum((int(f) + 255) // 256 for f in (front + rear))
-    h2d = 16 * n_chunks
+    # host -> device per step: one 16-byte record per emitting face (face,
+    # its ray counts, its first work chunk); the chunks are built on the GPU
+    h2d = 16 * int(np.count_nonzero(front.astype(np.int64) + rear))
     d2h = 4 * n * n
 
     batched = served = csv = thermal = None

@@ -6,6 +6,7 @@
 // host arguments.  No CPU fallback: every result is computed by the kernels of
 // ffb_grid.cuh / ffb_trace.cuh.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -119,7 +120,7 @@ struct ffb_ctx {
   cudaEvent_t batch_fork = nullptr, batch_join[4] = {};
 
   // per-call scratch
-  DevBuf scan_sums, chunks, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
+  DevBuf scan_sums, chunks, chunk_src, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
   DevBuf power_tab, absorb;                     // radiance sink
   // OBJ import: the text and its line tables, the parsed geometry
@@ -524,6 +525,38 @@ void add_chunks(std::vector<Chunk>& out, const int32_t* front, const int32_t* re
   }
 }
 
+// Chunk table of the emitting faces `faces` (in launch order) built on the
+// device: the host computes each face's first chunk (work linear in faces,
+// not in rays) and uploads 16 bytes per face; k_chunk_fill writes the
+// chunks.  first[i] gets the first chunk of faces[i], *n_chunks the total.
+int device_chunks(ffb_ctx* c, const std::vector<int32_t>& faces, const int32_t* front, const int32_t* rear,
+                  std::vector<long long>& first, long long* n_chunks)
+{
+  std::vector<int4> src(faces.size());
+  first.resize(faces.size());
+  long long next = 0;
+  for (size_t i = 0; i < faces.size(); ++i) {
+    const int f = faces[i];
+    const long long nf = (long long)front[f] + rear[f];
+    if (nf > INT_MAX - kChunkRays)
+      return fail(FFB_ERR_TOO_LARGE, "face %d emits %lld rays; at most %d", f, nf, INT_MAX - kChunkRays);
+    first[i] = next;
+    src[i] = make_int4(f, front[f], (int)nf, (int)next);
+    next += (nf + kChunkRays - 1) / kChunkRays;
+    if (next > INT_MAX)
+      return fail(FFB_ERR_TOO_LARGE, "more than %d work chunks", INT_MAX);
+  }
+  *n_chunks = next;
+  if (next > 0) {
+    FFB_TRY(ensure(c, c->chunks, sizeof(Chunk) * (size_t)next));
+    FFB_TRY(upload(c, c->chunk_src, src.data(), sizeof(int4) * src.size()));
+    k_chunk_fill<kChunkRays><<<grid_blocks((long long)src.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+        dptr<int4>(c->chunk_src), (int)src.size(), dptr<Chunk>(c->chunks));
+    FFB_CUDA(cudaGetLastError());
+  }
+  return FFB_OK;
+}
+
 int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long long* total)
 {
   if (!front || !rear)
@@ -625,7 +658,7 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   for (SceneData& s : c->batch)
     release_scene(c, s);
   DevBuf* bufs[] = {&c->frames,   &c->batch_frames, &c->batch_chunks, &c->batch_keys, &c->batch_epoch,
-                    &c->scan_sums, &c->chunks,      &c->rows,         &c->cursor,     &c->stats,
+                    &c->scan_sums, &c->chunks,      &c->chunk_src,    &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
                     &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
                     &c->power_tab, &c->absorb, &c->obj_text, &c->obj_chunk, &c->obj_chunk_off,
@@ -927,27 +960,29 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     if (row >= row_begin && row < row_end)
       face_block[f] = (int)(std::upper_bound(bounds.begin(), bounds.end(), row) - bounds.begin()) - 1;
   }
-  std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
-  std::vector<int> first(n_blocks + 1, 0);
+  // emitting faces block after block (ascending within a block)
+  std::vector<std::vector<int32_t>> by_block(n_blocks);
+  for (int f = 0; f < s.n_faces; ++f)
+    if (face_block[f] >= 0 && front[f] + (long long)rear[f] > 0)
+      by_block[face_block[f]].push_back(f);
+  std::vector<int32_t> order;
+  order.reserve((size_t)s.n_faces);
+  std::vector<size_t> block_pos(n_blocks + 1, 0);
   for (int b = 0; b < n_blocks; ++b) {
-    first[b] = (int)chunks.size();
-    for (int f = 0; f < s.n_faces; ++f) {
-      if (face_block[f] != b)
-        continue;
-      const int nf = front[f] + rear[f];
-      for (int j0 = 0; j0 < nf; j0 += kChunkRays)
-        chunks.push_back(Chunk{f, j0, (int16_t)std::min(kChunkRays, nf - j0), 0, front[f]});
-    }
+    block_pos[b] = order.size();
+    order.insert(order.end(), by_block[b].begin(), by_block[b].end());
   }
-  first[n_blocks] = (int)chunks.size();
+  block_pos[n_blocks] = order.size();
+  std::vector<long long> face_first;
+  long long n_chunks = 0;
+  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks));
+  std::vector<int> first(n_blocks + 1, 0);
+  for (int b = 0; b <= n_blocks; ++b)
+    first[b] = (int)(block_pos[b] < order.size() ? face_first[block_pos[b]] : n_chunks);
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
-  if (!chunks.empty()) {
-    FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
-    if (face_to_row)
-      FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)s.n_faces));
-  }
+  if (n_chunks > 0 && face_to_row)
+    FFB_TRY(upload(c, c->rows, face_to_row, sizeof(int32_t) * (size_t)s.n_faces));
   FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * kMaxPipeBlocks));
   if (n_blocks > 1)
     FFB_TRY(ensure_pipeline(c));
@@ -1092,15 +1127,19 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
     fixed[2 * (size_t)f + 1] = std::llround(std::ldexp((double)power_rear[f], scale_exp));
   }
   FFB_TRY(ensure_frames(c, flags));
-  std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / kChunkRays + s.n_faces));
-  add_chunks(chunks, front, rear, s.n_faces, 0);
+  std::vector<int32_t> order;
+  order.reserve((size_t)s.n_faces);
+  for (int f = 0; f < s.n_faces; ++f)
+    if (front[f] + (long long)rear[f] > 0)
+      order.push_back(f);
+  std::vector<long long> face_first;
+  long long n_chunks = 0;
+  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks));
   FFB_TRY(ensure(c, c->absorb, sizeof(unsigned long long) * (size_t)n_meshes));
   FFB_CUDA(cudaMemsetAsync(c->absorb.ptr, 0, sizeof(unsigned long long) * (size_t)n_meshes, c->stream));
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));
-  if (!chunks.empty()) {
-    FFB_TRY(upload(c, c->chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
+  if (n_chunks > 0) {
     FFB_TRY(upload(c, c->power_tab, fixed.data(), sizeof(long long) * fixed.size()));
     FFB_TRY(upload(c, c->rows, face_to_mesh, sizeof(int32_t) * (size_t)s.n_faces));
     FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t)));
@@ -1108,7 +1147,7 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
     TraceParams p;
     p.frames = dptr<float>(c->frames);
     p.chunks = dptr<Chunk>(c->chunks);
-    p.n_chunks = (int)chunks.size();
+    p.n_chunks = (int)n_chunks;
     p.key0 = (uint32_t)seed;
     p.key1 = (uint32_t)(seed >> 32);
     p.epoch = epoch;

@@ -18,6 +18,22 @@ struct Chunk {
   int32_t front;
 };
 
+// Writes the work chunks of the emitting faces: src[i] = {face, front rays,
+// front + rear rays, first chunk}; the face's rays [0, nf) become chunks of
+// kRays consecutive rays (the last one shorter), one warp per face.
+template <int kRays>
+__global__ void k_chunk_fill(const int4* __restrict__ src, int n, Chunk* __restrict__ chunks)
+{
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n; i += warps) {
+    const int4 f = src[i];
+    const int nc = (f.z + kRays - 1) / kRays;
+    for (int j = lane; j < nc; j += 32)
+      chunks[(uint32_t)f.w + (uint32_t)j] = Chunk{f.x, j * kRays, (int16_t)min(kRays, f.z - j * kRays), 0, f.y};
+  }
+}
+
 // Statistics slots (uint64 each), accumulated once per warp.
 enum { kStatTests = 0, kStatCells = 1, kStatRays = 2, kStatHits = 3, kStatJumps = 4, kStatSlots = 5 };
 
