@@ -644,6 +644,19 @@ extern "C" int ffb_ctx_create(int device, ffb_ctx** out)
     return fail(FFB_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
   }
   c->stream = c->own_stream;
+  // Keep freed blocks in this process's default memory pool instead of
+  // returning them at every synchronisation: contexts grow and release
+  // multi-GB buffers (count matrices), and mapping them again on the next
+  // allocation costs more than the trace of a small request.  Trimmed when
+  // a context is destroyed.
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   *out = c;
   return FFB_OK;
 }
@@ -685,6 +698,12 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+  }
   delete c;
 }
 

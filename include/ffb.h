@@ -74,7 +74,10 @@ typedef struct {
 } ffb_stats;
 
 /* Context: one device, one stream, resident scene and grid.
- * Replaces the state of ray_caster::system_create (ray_caster/system.cpp:65-90). */
+ * Replaces the state of ray_caster::system_create (ray_caster/system.cpp:65-90).
+ * Device buffers come from the device's default stream-ordered memory pool,
+ * which ffb_ctx_create sets to keep freed blocks for reuse (this process
+ * only); ffb_ctx_destroy trims the blocks no one uses back to the driver. */
 int ffb_ctx_create(int device, ffb_ctx** out);
 void ffb_ctx_destroy(ffb_ctx* ctx);
 /* Use `stream` (a cudaStream_t) instead of the context's own; NULL restores it. */
