@@ -1,4 +1,4 @@
-"""Row sharding across ranks (SURVEY multi-GPU row): balanced contiguous row
+"""Row sharding across ranks (the multi-GPU path): balanced contiguous row
 blocks, and the blocks of world_size ranks gathered with torch.distributed
 (gloo, CPU processes) reproduce the full matrix.  The per-rank rows come from
 the CPU oracle here; on GPUs each rank runs ffb_form_factor_counts_rows."""
