@@ -534,13 +534,13 @@ def fp32_peak(device):
 
 
 def measured_hbm_gbs():
-    """Copy bandwidth of this pool's B200s, measured by the driver (GB/s)."""
+    """Measured copy bandwidth of these B200s (GB/s), MEASURED_PEAKS.json or the fallback."""
     return hbm_peak()[0]
 
 
 def hbm_peak():
     """(GB/s, source): MEASURED_PEAKS.json's copy bandwidth, else the
-    fallback measured earlier on this pool."""
+    fallback from an earlier measurement of the same GPUs."""
     try:
         return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
     except (OSError, ValueError, KeyError):
