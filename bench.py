@@ -9,14 +9,16 @@ an N x N matrix (1.95 GB) resident on the device.  Synthetic and seeded; each
 step draws fresh rays (Philox epoch = step index).
 
 A step is one ffb_form_factor_counts call: zero the count matrix, fused
-emission + grid trace + shared-memory histogram + flush.  The 1.95 GB zeroing
+emission + grid trace + one global reduction per hit (matrices this large
+take no shared-memory histogram).  The 1.95 GB zeroing
 writes more than the 126 MB L2 every step, so no step starts with the previous
 step's lines in L2.
 
   value  rays/s with the scene, grid and matrix resident (CUDA events on the
          context stream around K steps, max over ranks)
   e2e    rays/s through the C ABI with host buffers: host ray counts in, the
-         count matrix copied to pinned host memory every step
+         count matrix copied to pinned host memory every step (in row blocks
+         whose copies overlap the next block's trace)
   --impl reference  the reference's own CPU path (zgrid_cpu caster + malley_cpu
          emission, compiled from its sources into oracle/_ref) on a bounded
          sample of the same workload, all host cores
