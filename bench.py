@@ -135,20 +135,23 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # the reference CPU path (oracle/_ref), bounded sample
 # ---------------------------------------------------------------------------
-def reference_sampler(faces, rays_per_face, every):
-    """Returns (run_step, describe): run_step() casts one bounded sample with
-    the reference's malley_cpu emission and zgrid_cpu caster on all cores and
-    returns (rays, seconds)."""
+def reference_sampler(faces, rays_per_face, every, threads=0, target_rays_per_s=0.25e6):
+    """Returns (run_step, describe, threads): run_step() casts one bounded
+    sample with the reference's malley_cpu emission and zgrid_cpu caster
+    (ray_caster/zgrid_cpu.cpp:115-132 cast over `threads` host threads on
+    disjoint ray slices; emission/malley_cpu.cpp:195-211 single-threaded, as
+    the reference's emitter is stateful) and returns (rays, seconds,
+    emit_seconds, cast_seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import ctypes as C
     from oracle_lib import Reference
     if not Reference.available():
-        return None, "oracle/_ref/libffref.so not built (reference sources absent when the tree was built)"
+        return None, "oracle/_ref/libffref.so not built (reference sources absent when the tree was built)", 0
     ref = Reference()
     n = len(faces)
-    cores = os.cpu_count() or 1
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
     if every <= 0:
-        every = max(1, int(round(n * rays_per_face / (0.25e6 * cores))))  # ~1-4 s per step
+        every = max(1, int(round(n * rays_per_face / (target_rays_per_s * cores))))  # ~1-4 s per step
     mask = np.zeros(n, np.uint8)
     mask[::every] = 1
     # front weight 1, rear 0, total 1, n_rays = rays_per_face: exactly
@@ -158,7 +161,7 @@ def reference_sampler(faces, rays_per_face, every):
     prep = C.c_double()
     h = ref.lib.ffref_step_open(Reference.ZGRID_CPU, n, np.ascontiguousarray(faces, np.float32), C.byref(prep))
     if not h:
-        return None, "reference zgrid_cpu prepare failed"
+        return None, "reference zgrid_cpu prepare failed", 0
     hist = np.zeros(n, np.uint32)
 
     def run():
@@ -166,12 +169,34 @@ def reference_sampler(faces, rays_per_face, every):
         t0 = time.perf_counter()
         k = ref.lib.ffref_step_run(h, rays_per_face, w, 1.0, mask, cores, hist.ctypes.data, C.byref(te),
                                    C.byref(tc))
-        return k, time.perf_counter() - t0
+        return k, time.perf_counter() - t0, te.value, tc.value
 
     desc = ("reference zgrid_cpu cast + malley_cpu emission (oracle/_ref) of every %d-th source face "
             "(%d faces, %d rays) against the full %d-face scene, cast on %d threads" %
             (every, int(mask.sum()), int(mask.sum()) * rays_per_face, n, cores))
     return run, desc, cores
+
+
+def cpu_baseline(faces, rays_per_face, every):
+    """The reference's zgrid_cpu path on the host cores: all threads (the
+    reported value: rays per second of emission + cast) and one thread, each
+    with its emission and cast seconds apart."""
+    out = reference_sampler(faces, rays_per_face, every)
+    if out[0] is None:
+        return {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": out[1]}
+    run, desc, cores = out
+    run()
+    k, s, te, tc = run()
+    line = {"value": k / s, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc,
+            "emit_s": te, "cast_s": tc, "cast_rays_per_s": k / tc if tc > 0 else None,
+            "emit_rays_per_s": k / te if te > 0 else None}
+    one = reference_sampler(faces, rays_per_face, 0, threads=1)
+    if one[0] is not None:
+        run1, desc1, _ = one
+        k1, s1, te1, tc1 = run1()
+        line["one_thread"] = {"value": k1 / s1, "cast_rays_per_s": k1 / tc1 if tc1 > 0 else None,
+                              "emit_s": te1, "cast_s": tc1, "sample": desc1}
+    return line
 
 
 def reference_arm(args):
@@ -187,18 +212,22 @@ def reference_arm(args):
     for _ in range(args.warmup):
         run()
     rays = 0
-    secs = 0.0
+    secs = emit_s = cast_s = 0.0
     for _ in range(args.steps):
-        k, s = run()
+        k, s, te, tc = run()
         rays += k
         secs += s
+        emit_s += te
+        cast_s += tc
     v = rays / secs
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": desc},
-        "cpu_baseline": {"value": v, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc,
+                         "emit_s": emit_s / args.steps, "cast_s": cast_s / args.steps,
+                         "cast_rays_per_s": rays / cast_s if cast_s > 0 else None},
         "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -208,10 +237,20 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------
 def batched_section(ctx, stream, args):
     """256 scenes, triangle counts log-uniform 200-20k (plate pairs, inward UV
-    spheres, clutter in a box), 1k-10k front rays per face.  Batched: the grids
-    and the 256 count matrices resident, one launch per scene over side
-    streams, replayed from a CUDA graph.  Plain: the same scenes one at a time
-    through the single-scene path (upload, grid build, counts)."""
+    spheres, clutter in a box), 1k-10k front rays per face.
+
+    batched: grids and the 256 count matrices resident, all scenes launched
+      from one CUDA graph replay (zeroing included).
+    plain: the same scenes one at a time through the single-scene path
+      (scene upload, grid build, zeroing and trace per scene), device matrices.
+    plain_dropin: the same through the reference-facing call with a host
+      float matrix per scene (ffb_form_factors: counts, normalisation and the
+      copy to the host), as a FORM_FACTORS_B200 calculate delivers it.
+    A second plain pass records CUDA events around each phase of each scene:
+    upload, grid build, and the counts call (zeroing + trace, of which the
+    trace kernel alone is also timed).  ceiling = plain_s / sum(trace): the
+    speed-up a batched form could reach if everything but the traces went
+    away."""
     import torch
     from form_factors_b200 import scenes
     sl, rpf = scenes.batch_workload(256, 200, 20000, 1000, 10000, seed=4)
@@ -220,10 +259,17 @@ def batched_section(ctx, stream, args):
     rears = [np.zeros(len(f), np.int32) for f in sl]
     seeds = np.arange(1, len(sl) + 1, dtype=np.uint64) * np.uint64(7919)
     rays = int(sum(int(f.sum()) for f in fronts))
+    skip = not args.no_skip
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
-    ctx.batch_set(sl, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
+    ev0.record(stream)
+    ctx.batch_set(sl, cells_per_face=args.cells_per_face, skip_empty=skip)
     ctx.batch_prepare(np.concatenate(fronts), np.concatenate(rears), seeds)
+    ev1.record(stream)
+    torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
+    build_dev_s = ev0.elapsed_time(ev1) / 1e3
     offs, words = ctx.batch_counts_layout()
     counts = torch.empty(words, dtype=torch.int32, device="cuda")
     graph = torch.cuda.CUDAGraph()
@@ -231,35 +277,88 @@ def batched_section(ctx, stream, args):
         ctx.batch_launch(counts, offs, advance_epoch=True)
     graph.replay()  # warm-up
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     graph.replay()
     ev1.record(stream)
     torch.cuda.synchronize()
     batched_s = ev0.elapsed_time(ev1) / 1e3
     del graph
+
+    def plain_scene(i, out=None):
+        n = len(sl[i])
+        ctx.scene_set(sl[i])
+        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2,
+                               out=counts[int(offs[i]):int(offs[i]) + n * n], n_rows=n)
+
     # plain: one scene at a time, grid built per scene
     t0 = time.perf_counter()
     ev0.record(stream)
-    for i, f in enumerate(sl):
-        n = len(f)
-        ctx.scene_set(f)
-        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
-        ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2, out=counts[int(offs[i]):int(offs[i]) + n * n],
-                               n_rows=n)
+    for i in range(len(sl)):
+        plain_scene(i)
     ev1.record(stream)
     torch.cuda.synchronize()
     plain_s = ev0.elapsed_time(ev1) / 1e3
     plain_wall = time.perf_counter() - t0
+    # phase breakdown of the plain path (a second pass, events per phase)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in sl]
+    trace_ms = []
+    for i, f in enumerate(sl):
+        n = len(f)
+        e = evs[i]
+        e[0].record(stream)
+        ctx.scene_set(f)
+        e[1].record(stream)
+        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        e[2].record(stream)
+        ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2,
+                               out=counts[int(offs[i]):int(offs[i]) + n * n], n_rows=n)
+        e[3].record(stream)
+        trace_ms.append(ctx.stats().kernel_ms)
+    torch.cuda.synchronize()
+    upload_s = sum(e[0].elapsed_time(e[1]) for e in evs) / 1e3
+    grid_s = sum(e[1].elapsed_time(e[2]) for e in evs) / 1e3
+    counts_s = sum(e[2].elapsed_time(e[3]) for e in evs) / 1e3
+    gaps_s = sum(evs[i][3].elapsed_time(evs[i + 1][0]) for i in range(len(evs) - 1)) / 1e3
+    # the zeroing alone, per scene (the counts call zeroes, then traces)
+    z0, z1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    z0.record(stream)
+    for i, f in enumerate(sl):
+        n = len(f)
+        counts[int(offs[i]):int(offs[i]) + n * n].zero_()
+    z1.record(stream)
+    torch.cuda.synchronize()
+    zero_s = z0.elapsed_time(z1) / 1e3
+    # stats().kernel_ms brackets the zeroing and the trace launch of a call
+    trace_s = max(sum(trace_ms) / 1e3 - zero_s, 1e-9)
     del counts
     torch.cuda.empty_cache()
+    # plain through the reference-facing call: a host float matrix per scene
+    host = torch.empty(int(sizes.max()) ** 2, dtype=torch.float32, pin_memory=True)
+    t0 = time.perf_counter()
+    for i, f in enumerate(sl):
+        n = len(f)
+        ctx.scene_set(f)
+        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        ctx.form_factors(fronts[i], rears[i], int(seeds[i]), epoch=2, n_rows=n,
+                         out=host[:n * n].numpy().reshape(n, n))
+    dropin_s = time.perf_counter() - t0
+    del host
     return {"workload": "256 scenes, faces log-uniform 200-20000 (plates/UV spheres/clutter), "
                         "1k-10k front rays/face, per-scene N^2 uint32 counts resident",
-            "faces_total": int(sizes.sum()), "rays": rays, "counts_gb": round(4 * float((sizes.astype(float) ** 2).sum()) / 1e9, 2),
-            "batched_s": batched_s, "plain_s": plain_s, "plain_wall_s": plain_wall, "grid_build_s": build_s,
+            "faces_total": int(sizes.sum()), "rays": rays,
+            "counts_gb": round(4 * float((sizes.astype(float) ** 2).sum()) / 1e9, 2),
+            "batched_s": batched_s, "batched_grid_build_s": build_s, "batched_grid_build_device_s": build_dev_s,
+            "plain_s": plain_s, "plain_wall_s": plain_wall, "plain_dropin_host_float_s": dropin_s,
+            "plain_breakdown_s": {"upload": upload_s, "grid_build": grid_s, "counts_call": counts_s,
+                                  "zeroing": zero_s, "trace": trace_s, "host_gaps": gaps_s},
             "batched_scenes_per_s": len(sl) / batched_s, "plain_scenes_per_s": len(sl) / plain_s,
+            "plain_dropin_scenes_per_s": len(sl) / dropin_s,
             "batched_rays_per_s": rays / batched_s, "plain_rays_per_s": rays / plain_s,
-            "speedup_scenes_per_s": plain_s / batched_s,
+            "speedup_trace_resident": plain_s / batched_s,
+            "speedup_grid_build_in_both": plain_s / (batched_s + build_dev_s),
+            "speedup_vs_dropin": dropin_s / batched_s,
+            "ceiling": plain_s / trace_s,
             "launches": "one fused launch per scene over 4 side streams, replayed as one CUDA graph"}
 
 
@@ -319,7 +418,7 @@ def served_section(args):
                "max_latency_s": float(sub_lat.max()), "wall_s": sub_wall, "peak_concurrent": int(sub_peak)}
     return {"workload": "%d requests, faces log-uniform 500-50000 (plates/UV spheres/clutter), 1k-100k front "
                         "rays/face, Poisson %.0f req/s, 80 GB budget, 4 slots" % (n, args.served_rate),
-            "rays": int(rays), "served_scenes_per_s": n / served_wall, "plain_scenes_per_s": n / plain_wall,
+            "requests": n, "rays": int(rays), "served_scenes_per_s": n / served_wall, "plain_scenes_per_s": n / plain_wall,
             "speedup_scenes_per_s": plain_wall / served_wall, "served_rays_per_s": rays / served_wall,
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "plain_p50_latency_s": float(np.percentile(plain_lat, 50)),
@@ -695,14 +794,7 @@ def ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out = reference_sampler(faces, args.rays_per_face, args.cpu_sample_every)
-        if out[0] is not None:
-            run, desc, cores = out
-            run()
-            k, s = run()
-            cpu = {"value": k / s, "unit": "rays/s", "cores": cores, "kind": "reference", "sample": desc}
-        else:
-            cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": out[1]}
+        cpu = cpu_baseline(faces, args.rays_per_face, args.cpu_sample_every)
 
     if rank == 0:
         line = {
@@ -737,16 +829,26 @@ def ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        for key, sec in (("csv", csv), ("thermal", thermal), ("obj", obj), ("batched", batched),
+                         ("served", served)):
+            if sec is not None:
+                line[key] = sec
+        # last, so that a reader of the line's tail sees the headline ratios
+        summary = {"value_g_rays_per_s": value / 1e9, "e2e_g_rays_per_s": line["e2e"]["value"] / 1e9}
+        if cpu is not None and cpu.get("value"):
+            summary["cpu_rays_per_s"] = cpu["value"]
+            summary["cpu_one_thread_rays_per_s"] = (cpu.get("one_thread") or {}).get("value")
         if batched is not None:
-            line["batched"] = batched
+            summary["batched_vs_plain"] = batched["speedup_trace_resident"]
+            summary["batched_vs_plain_grid_build_in_both"] = batched["speedup_grid_build_in_both"]
+            summary["batched_ceiling"] = batched["ceiling"]
         if served is not None:
-            line["served"] = served
-        if csv is not None:
-            line["csv"] = csv
-        if thermal is not None:
-            line["thermal"] = thermal
-        if obj is not None:
-            line["obj"] = obj
+            summary["served_vs_plain"] = served["speedup_scenes_per_s"]
+            summary["served_requests"] = served["requests"]
+            summary["served_p50_s"] = served["p50_latency_s"]
+            summary["served_p99_s"] = served["p99_latency_s"]
+            summary["served_ceiling"] = served.get("ceiling")
+        line["summary"] = summary
         print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -194,16 +194,30 @@ void release_scene(ffb_ctx* c, SceneData& s)
 template <class T>
 T* dptr(DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
 
-bool is_device_ptr(const void* p)
+// Where `p` lives: *dev is true for memory the context's device takes as a
+// kernel operand (device memory of that device, or managed memory) and false
+// for host memory (pageable or pinned).  Device memory of another device is
+// an argument error: a kernel would reach it only through peer access, and
+// fault without it.
+int ptr_kind(ffb_ctx* c, const void* p, bool* dev)
 {
+  *dev = false;
   if (!p)
-    return false;
+    return FFB_OK;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return FFB_OK;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) {
+    *dev = true;
+  } else if (a.type == cudaMemoryTypeDevice) {
+    if (a.device != c->device)
+      return fail(FFB_ERR_ARG, "device pointer %p belongs to device %d; the context runs on device %d", p, a.device,
+                  c->device);
+    *dev = true;
+  }
+  return FFB_OK;
 }
 
 // Pinned staging buffer; waits for the previous copy out of it first.
@@ -355,7 +369,9 @@ int scene_upload(ffb_ctx* c, SceneData& s, const float* faces9, int n_faces)
   if (n_faces == 0)
     return FFB_OK;
   const size_t bytes = sizeof(float) * 9 * (size_t)n_faces;
-  if (is_device_ptr(faces9)) {
+  bool dev = false;
+  FFB_TRY(ptr_kind(c, faces9, &dev));
+  if (dev) {
     FFB_TRY(ensure(c, s.faces, bytes));
     FFB_CUDA(cudaMemcpyAsync(s.faces.ptr, faces9, bytes, cudaMemcpyDeviceToDevice, c->stream));
   } else {
@@ -798,7 +814,9 @@ namespace {
 // into `tmp`.
 int input_ptr(ffb_ctx* c, const void* p, size_t bytes, DevBuf& tmp, const void** out)
 {
-  if (is_device_ptr(p)) {
+  bool dev = false;
+  FFB_TRY(ptr_kind(c, p, &dev));
+  if (dev) {
     *out = p;
     return FFB_OK;
   }
@@ -813,7 +831,9 @@ int input_ptr(ffb_ctx* c, const void* p, size_t bytes, DevBuf& tmp, const void**
 // device temporary copied back by finish_output.
 int output_ptr(ffb_ctx* c, void* p, size_t bytes, DevBuf& tmp, void** out, bool* host)
 {
-  *host = p && !is_device_ptr(p);
+  bool dev = false;
+  FFB_TRY(ptr_kind(c, p, &dev));
+  *host = p && !dev;
   if (!p || !*host) {
     *out = p;
     return FFB_OK;
@@ -844,7 +864,8 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
     return FFB_OK;
   const void* d_rays;
   void *d_hit, *d_pt;
-  bool host_hit, host_pt;
+  bool host_hit, host_pt, rays_dev = false;
+  FFB_TRY(ptr_kind(c, rays6, &rays_dev));
   FFB_TRY(input_ptr(c, rays6, sizeof(float) * 6 * (size_t)n_rays, c->tmp_in, &d_rays));
   FFB_TRY(output_ptr(c, hit_face, sizeof(int32_t) * (size_t)n_rays, c->tmp_out, &d_hit, &host_hit));
   FFB_TRY(output_ptr(c, hit_point, sizeof(float) * 3 * (size_t)n_rays, c->tmp_out2, &d_pt, &host_pt));
@@ -872,7 +893,7 @@ int cast_impl(ffb_ctx* c, const float* rays6, long long n_rays, int32_t* hit_fac
     FFB_TRY(finish_output(c, hit_face, d_hit, sizeof(int32_t) * (size_t)n_rays));
   if (host_pt)
     FFB_TRY(finish_output(c, hit_point, d_pt, sizeof(float) * 3 * (size_t)n_rays));
-  if (host_hit || host_pt || !is_device_ptr(rays6))
+  if (host_hit || host_pt || !rays_dev)
     FFB_CUDA(cudaStreamSynchronize(c->stream));
   return FFB_OK;
 }
@@ -1650,7 +1671,9 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
   FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (size_t)(n_tiles + 2)));
   auto* tile_len = dptr<unsigned long long>(c->csv_tile_len);
   auto* tile_off = dptr<unsigned long long>(c->csv_tile_off);
-  if (text && is_device_ptr(text)) {
+  bool text_dev = false;
+  FFB_TRY(ptr_kind(c, text, &text_dev));
+  if (text_dev) {
     // one pass: the tile-length buffer holds the look-back status words; the
     // first two words of the offset buffer the ticket and error bits, then
     // the total
@@ -1930,7 +1953,9 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     if (c->batch[s].n_faces > kMaxRows)
       return fail(FFB_ERR_TOO_LARGE, "scene %d has more than %d faces", s, kMaxRows);
   }
-  if (!is_device_ptr(counts))
+  bool counts_dev = false;
+  FFB_TRY(ptr_kind(c, counts, &counts_dev));
+  if (!counts_dev)
     return fail(FFB_ERR_ARG, "batched counts must be device memory");
   FFB_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * counts_words, c->stream));
   FFB_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sizeof(unsigned long long) * kStatSlots, c->stream));

@@ -46,6 +46,7 @@ struct Request {
   int error = 0;
   std::string message;
   uint32_t* counts = nullptr;      // device, n_faces^2, until released
+  int readers = 0;                 // ffb_server_result copies in progress (release waits for them)
   int device = 0;
   Clock::time_point t_submit, t_admit, t_done;
   double gpu_ms = 0;               // events around the request's device work
@@ -289,10 +290,16 @@ extern "C" int ffb_server_result(ffb_server* s, long long id, uint32_t* counts)
     if (it == s->all.end() || it->second->state != FFB_REQ_DONE || !it->second->counts)
       return ffb_set_error(FFB_ERR_ARG, "no finished result for this request");
     r = it->second;
+    ++r->readers;  // a concurrent release waits until this copy is done
   }
   cudaSetDevice(s->device);
   const size_t bytes = sizeof(uint32_t) * (size_t)r->n_faces * r->n_faces;
   cudaError_t e = cudaMemcpy(counts, r->counts, bytes, cudaMemcpyDefault);
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    --r->readers;
+  }
+  s->cv_done.notify_all();
   if (e != cudaSuccess)
     return ffb_set_error(FFB_ERR_CUDA, cudaGetErrorString(e));
   return FFB_OK;
@@ -302,13 +309,18 @@ extern "C" int ffb_server_release(ffb_server* s, long long id)
 {
   std::shared_ptr<Request> r;
   {
-    std::lock_guard<std::mutex> lock(s->mu);
+    std::unique_lock<std::mutex> lock(s->mu);
     auto it = s->all.find(id);
     if (it == s->all.end())
       return ffb_set_error(FFB_ERR_ARG, "unknown request");
     r = it->second;
     if (r->state != FFB_REQ_DONE && r->state != FFB_REQ_FAILED)
       return ffb_set_error(FFB_ERR_ARG, "request still queued or running");
+    // the matrix is freed below: wait for result copies still reading it
+    s->cv_done.wait(lock, [&] { return r->readers == 0; });
+    it = s->all.find(id);
+    if (it == s->all.end())
+      return ffb_set_error(FFB_ERR_ARG, "request released concurrently");
     s->all.erase(it);
     s->reserved -= r->reserve;
     r->reserve = 0;

@@ -33,6 +33,7 @@ constexpr int kStaticMaxFaces = 16384;
 constexpr int kThreads = 128;
 constexpr int kTile = 128;
 constexpr int kMaxDevices = 64;
+constexpr long long kMaxGridX = 0x7FFFFFFFLL;  // largest grid x dimension of a launch
 
 // The static scratch: one triangle record per face.
 __device__ __align__(256) ffb::TriRec g_static_records[kStaticMaxFaces];
@@ -101,14 +102,18 @@ __global__ void __launch_bounds__(kThreads) k_static_brute(const ffb::TriRec* __
   }
 }
 
-bool on_device(const void* p)
+// True for memory that device `dev` takes as a kernel operand: its own device
+// memory, or managed memory.  Host memory and another device's memory are
+// refused (the kernels would fault on them, or reach them only through peer
+// access).
+bool on_device(const void* p, int dev)
 {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
 }  // namespace
@@ -128,14 +133,18 @@ extern "C" int ffb_cast_bruteforce_static(const float* faces9, int n_faces, cons
     return FFB_OK;
   if (!rays6 || !hit_face || (n_faces > 0 && !faces9))
     return ffb_set_error(FFB_ERR_ARG, "ffb_cast_bruteforce_static: null pointer");
-  if ((n_faces > 0 && !on_device(faces9)) || !on_device(rays6) || !on_device(hit_face) ||
-      (hit_point && !on_device(hit_point)))
-    return ffb_set_error(FFB_ERR_ARG, "ffb_cast_bruteforce_static: every buffer must be device memory");
+  // one thread per ray: the grid's x dimension bounds the rays of one call
+  if ((n_rays + kThreads - 1) / kThreads > (long long)kMaxGridX)
+    return ffb_set_error(FFB_ERR_TOO_LARGE, "ffb_cast_bruteforce_static: n_rays above 2^31 - 1 blocks of 128 rays");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     return ffb_set_error(FFB_ERR_NO_DEVICE, "ffb_cast_bruteforce_static: no usable current device");
   }
+  if ((n_faces > 0 && !on_device(faces9, dev)) || !on_device(rays6, dev) || !on_device(hit_face, dev) ||
+      (hit_point && !on_device(hit_point, dev)))
+    return ffb_set_error(FFB_ERR_ARG,
+                         "ffb_cast_bruteforce_static: every buffer must be device memory of the current device");
   ffb::TriRec* rec = nullptr;
   {
     // set-up, once per device, with that device current

@@ -349,7 +349,6 @@ namespace b200_form_factors {
 
 struct ff_t : form_factors::system_t {
   emission::system_t* emitter;
-  int fused;  // emission + trace + counts on the GPU
   form_factors::scene_t* scene;
   ray_caster::scene_t rc_scene;
   float total_area;
@@ -363,10 +362,13 @@ struct ff_t : form_factors::system_t {
   int flags;
 };
 
+// Emission, trace and counting all run fused on the GPU, so the only
+// emitters accepted are the B200 Malley emitter (whose seed, epoch and flags
+// key the fused draws) and none at all.  Any other emitter is refused with
+// -FORM_FACTORS_ERROR: there is no host counting path.
 static int init(ff_t* s, emission::system_t* emitter)
 {
   s->emitter = emitter;
-  s->fused = emitter == 0 || emitter->methods == &b200_emission::methods;
   s->scene = 0;
   s->rc_scene = ray_caster::scene_t{0, 0};
   s->total_area = 0;
@@ -378,8 +380,8 @@ static int init(ff_t* s, emission::system_t* emitter)
   s->seed = 1;
   s->epoch = 0;
   s->flags = 0;
-  if (!s->fused)
-    return FORM_FACTORS_OK;
+  if (emitter != 0 && emitter->methods != &b200_emission::methods)
+    return -FORM_FACTORS_ERROR;
   const int rc = ffb_ctx_create(device_from_env(), &s->ctx);
   if (rc == FFB_OK)
     ffb_ctx_set_stats(s->ctx, 0);  // the calculator reports no counters
@@ -399,14 +401,12 @@ static int shutdown(ff_t* s)
   return FORM_FACTORS_OK;
 }
 
-// cpuFactorsCalculator/cpu_system.cpp:82-92; the fused path uploads the scene
-// and builds the grid here, where the reference's emitter prepares its caster.
+// cpuFactorsCalculator/cpu_system.cpp:82-92: the scene is uploaded and the
+// grid built here, where the reference's emitter prepares its caster.
 static int set_scene(ff_t* s, form_factors::scene_t* scene)
 {
   s->scene = scene;
   s->rc_scene = ray_caster::scene_t{scene->n_faces, scene->faces};
-  if (!s->fused)
-    return s->emitter->methods->set_scene(s->emitter, &s->rc_scene);
   if (scene->n_faces == 0)
     return -EMISSION_ERROR;
   if (!s->ctx)
@@ -473,48 +473,11 @@ static int calculate_fused(ff_t* s, form_factors::task_t* task)
                           outgoing.data(), task->form_factors);
 }
 
-// cpuFactorsCalculator/cpu_system.cpp:149-201 with any emitter.
-static int calculate_generic(ff_t* s, form_factors::task_t* task)
-{
-  malley_emission::task_t emission_task(task->n_rays, s->total_area, s->face_weights);
-  int r = s->emitter->methods->calculate(s->emitter, &emission_task);
-  if (r < 0) {
-    task_release(emission_task.rays);
-    return r;
-  }
-  const int n_meshes = s->scene->n_meshes;
-  memset(task->form_factors, 0, (size_t)n_meshes * n_meshes * sizeof(float));
-  ray_caster::task_t* rays = emission_task.rays;
-  const int n_tasks = rays ? rays->n_tasks : 0;
-  int n_ray = 0;
-  for (int m = 0; m != n_meshes; ++m) {
-    int mesh_outgoing_rays = 0;
-    const form_factors::mesh_t& mesh = s->scene->meshes[m];
-    for (int f = 0; f != mesh.n_faces; ++f) {
-      const int face_idx = mesh.first_idx + f;
-      const int face_rays = emitted(task->n_rays, s->face_weights[2 * face_idx], s->total_area) +
-                            emitted(task->n_rays, s->face_weights[2 * face_idx + 1], s->total_area);
-      for (int j = 0; j != face_rays && n_ray < n_tasks; ++j, ++n_ray) {
-        ++mesh_outgoing_rays;
-        if (rays->hit_face[n_ray]) {
-          const int hit_face_idx = (int)(rays->hit_face[n_ray] - s->rc_scene.faces);
-          task->form_factors[m * n_meshes + s->face_to_mesh[hit_face_idx]] += 1.f;
-        }
-      }
-    }
-    const float mesh_ratio = 1.f / (float)mesh_outgoing_rays;
-    for (int j = 0; j != n_meshes; ++j)
-      task->form_factors[m * n_meshes + j] *= mesh_ratio;
-  }
-  task_release(rays);
-  return FORM_FACTORS_OK;
-}
-
 static int calculate(ff_t* s, form_factors::task_t* task)
 {
   if (!s->scene || !s->face_weights)
     return -FORM_FACTORS_EMPTY_SCENE;
-  return s->fused ? calculate_fused(s, task) : calculate_generic(s, task);
+  return calculate_fused(s, task);
 }
 
 static const form_factors::system_methods_t methods = {
@@ -726,7 +689,6 @@ namespace {
 struct thermal_t : thermal_equation::system_t {
   emission::system_t* emitter;
   int n_rays;
-  int fused;
   subject::scene_t* scene;
   ray_caster::scene_t rc_scene;
   ffb_ctx* ctx;
@@ -750,26 +712,14 @@ void mesh_tables(const subject::scene_t* scene, std::vector<ffb_mesh>& meshes, s
   }
 }
 
-// subject::build_face_to_mesh_index (subject/system.cpp:93-108)
-std::vector<int> face_mesh_index(const subject::scene_t* scene)
-{
-  std::vector<int> idx((size_t)scene->n_faces, 0);
-  for (int m = 0; m < scene->n_meshes; ++m)
-    for (int f = 0; f < scene->meshes[m].n_faces; ++f)
-      idx[(size_t)(scene->meshes[m].first_idx + f)] = m;
-  return idx;
-}
-
-const subject::material_t& mesh_material(const subject::scene_t* scene, int m)
-{
-  return scene->materials[scene->meshes[m].material_idx];
-}
-
-int thermal_init(thermal_t* s, emission::system_t* emitter, int n_rays, bool fused)
+// The step runs fused on the GPU (emission, trace and the absorbed-power
+// scatter in one kernel), so the equation accepts only its own B200 emitter
+// type (`accepted`) or none; any other emitter is refused with
+// -THERMAL_EQUATION_ERROR: there is no host absorption path.
+int thermal_init(thermal_t* s, emission::system_t* emitter, int n_rays, bool accepted)
 {
   s->emitter = emitter;
   s->n_rays = n_rays;
-  s->fused = fused;
   s->scene = 0;
   s->rc_scene = ray_caster::scene_t{0, 0};
   s->ctx = nullptr;
@@ -778,8 +728,8 @@ int thermal_init(thermal_t* s, emission::system_t* emitter, int n_rays, bool fus
   s->epoch = 0;
   s->source_param = 0;
   s->source = 0;
-  if (!fused)
-    return THERMAL_EQUATION_OK;
+  if (!accepted)
+    return -THERMAL_EQUATION_ERROR;
   const int rc = ffb_ctx_create(device_from_env(), &s->ctx);
   if (rc == FFB_OK)
     ffb_ctx_set_stats(s->ctx, 0);
@@ -794,14 +744,12 @@ int thermal_shutdown(thermal_t* s)
   return THERMAL_EQUATION_OK;
 }
 
-// radiance_cpu.cpp:78-94 / parallel_rays_cpu.cpp:66-78: the fused path keeps
-// the scene and grid resident; the other path sets the emitter's scene.
+// radiance_cpu.cpp:78-94 / parallel_rays_cpu.cpp:66-78: the scene and its
+// grid stay resident on the device.
 int thermal_set_scene(thermal_t* s, subject::scene_t* scene)
 {
   s->scene = scene;
   s->rc_scene = ray_caster::scene_t{scene->n_faces, scene->faces};
-  if (!s->fused)
-    return s->emitter->methods->set_scene(s->emitter, &s->rc_scene);
   if (scene->n_faces == 0)
     return -EMISSION_ERROR;
   if (!s->ctx)
@@ -849,74 +797,11 @@ static int calculate_fused(thermal_t* s, thermal_equation::task_t* task)
                            seed, epoch, flags, task->emission, task->absorption);
 }
 
-// thermal_equation/radiance_cpu.cpp:96-190 over any Malley-style emitter
-static int calculate_generic(thermal_t* s, thermal_equation::task_t* task)
-{
-  const subject::scene_t* scene = s->scene;
-  const int n_faces = scene->n_faces;
-  std::vector<float> area((size_t)n_faces), w(2 * (size_t)n_faces, 0.f);
-  for (int f = 0; f < n_faces; ++f)
-    area[(size_t)f] = triangle_area(scene->faces[f]);
-  float total = 0;
-  for (int m = 0; m != scene->n_meshes; ++m) {
-    const subject::material_t& material = mesh_material(scene, m);
-    const float density = task->temperatures[m];
-    const float front_density = density * material.front.emissivity;
-    const float rear_density = density * material.rear.emissivity;
-    const subject::mesh_t& mesh = scene->meshes[m];
-    for (int f = mesh.first_idx; f != mesh.first_idx + mesh.n_faces; ++f) {
-      const float front = front_density * area[(size_t)f];
-      const float rear = rear_density * area[(size_t)f];
-      total += front + rear;
-      w[2 * (size_t)f] = front;
-      w[2 * (size_t)f + 1] = rear;
-    }
-  }
-  malley_emission::task_t et(s->n_rays, total, w.data());
-  int r = s->emitter->methods->calculate(s->emitter, &et);
-  if (r < 0) {
-    task_release(et.rays);
-    return r;
-  }
-  const ray_caster::task_t* rays = et.rays;
-  if (!rays)
-    return THERMAL_EQUATION_OK;
-  const std::vector<int> f2m = face_mesh_index(scene);
-  const float sigma = 5.670400e-8f;
-  int n_ray = 0;
-  for (int m = 0; m != scene->n_meshes; ++m) {
-    const subject::mesh_t& mesh = scene->meshes[m];
-    const subject::material_t& material = mesh_material(scene, m);
-    const float T = task->temperatures[m];
-    const float power_density = sigma * (T * T * T * T);
-    const float front_density = power_density * material.front.emissivity;
-    const float rear_density = power_density * material.rear.emissivity;
-    for (int f = mesh.first_idx; f != mesh.first_idx + mesh.n_faces; ++f) {
-      const float front_emission = front_density * area[(size_t)f];
-      const float rear_emission = rear_density * area[(size_t)f];
-      task->emission[m] += front_emission + rear_emission;
-      const int face_rays_front = emitted(s->n_rays, w[2 * (size_t)f], total);
-      const int face_rays_rear = emitted(s->n_rays, w[2 * (size_t)f + 1], total);
-      const int face_rays = face_rays_front + face_rays_rear;
-      for (int j = 0; j != face_rays && n_ray < rays->n_tasks; ++j, ++n_ray) {
-        if (rays->hit_face[n_ray]) {
-          const int hit_mesh = f2m[(size_t)(rays->hit_face[n_ray] - s->rc_scene.faces)];
-          const float ray_power =
-              j < face_rays_front ? (front_emission / face_rays_front) : (rear_emission / face_rays_rear);
-          task->absorption[hit_mesh] += ray_power;
-        }
-      }
-    }
-  }
-  task_release(et.rays);
-  return THERMAL_EQUATION_OK;
-}
-
 static int calculate(thermal_t* s, thermal_equation::task_t* task)
 {
   if (!s->scene)
     return -THERMAL_EQUATION_ERROR;
-  return s->fused ? calculate_fused(s, task) : calculate_generic(s, task);
+  return calculate_fused(s, task);
 }
 
 static const thermal_equation::system_methods_t methods = {
@@ -1003,49 +888,6 @@ static int calculate_fused(thermal_t* s, thermal_equation::task_t* task, const p
                                  seed, epoch, task->absorption);
 }
 
-// thermal_equation/parallel_rays_cpu.cpp:92-131 over any parallel-rays emitter
-static int calculate_generic(thermal_t* s, thermal_equation::task_t* task, const parallel_rays_cpu::source_t& src)
-{
-  const subject::scene_t* scene = s->scene;
-  float center[3], bradius;
-  int r = ffb_bounding_sphere(&scene->faces[0].points[0].x, scene->n_faces, center, &bradius);
-  if (r < 0)
-    return r;
-  const float radius = bradius * 1.1f;
-  parallel_rays_emission_cpu::task_t et(s->n_rays);
-  et.rays = 0;
-  et.center = math::vec3{center[0], center[1], center[2]};
-  et.distance = 1.1f + radius;
-  et.direction = src.direction;
-  et.radius = radius;
-  if ((r = s->emitter->methods->calculate(s->emitter, &et)) < 0) {
-    task_release(et.rays);
-    return r;
-  }
-  const ray_caster::task_t* rays = et.rays;
-  if (!rays)
-    return THERMAL_EQUATION_OK;
-  const std::vector<int> f2m = face_mesh_index(scene);
-  const float ray_power = src.power * (float(M_PI) * radius * radius) / s->n_rays;
-  for (int i = 0; i != rays->n_tasks; ++i) {
-    if (!rays->hit_face[i])
-      continue;
-    const math::triangle_t& t = *rays->hit_face[i];
-    // triangle_normal (math/triangle.cpp:114-119) and its side
-    const float vx = t.points[1].x - t.points[0].x, vy = t.points[1].y - t.points[0].y,
-                vz = t.points[1].z - t.points[0].z;
-    const float wx = t.points[2].x - t.points[0].x, wy = t.points[2].y - t.points[0].y,
-                wz = t.points[2].z - t.points[0].z;
-    const float nx = vy * wz - vz * wy, ny = vz * wx - vx * wz, nz = vx * wy - vy * wx;
-    const float side = nx * src.direction.x + ny * src.direction.y + nz * src.direction.z;
-    const int mesh = f2m[(size_t)(rays->hit_face[i] - s->rc_scene.faces)];
-    const subject::material_t& material = mesh_material(scene, mesh);
-    task->absorption[mesh] += (side < 0 ? material.front.absorbance : material.rear.absorbance) * ray_power;
-  }
-  task_release(et.rays);
-  return THERMAL_EQUATION_OK;
-}
-
 static int calculate(thermal_t* s, thermal_equation::task_t* task)
 {
   if (!s->scene)
@@ -1053,7 +895,7 @@ static int calculate(thermal_t* s, thermal_equation::task_t* task)
   if (s->source == 0)  // parallel_rays_cpu.cpp:94-95
     return THERMAL_EQUATION_OK;
   const parallel_rays_cpu::source_t src = s->source(s->source_param);
-  return s->fused ? calculate_fused(s, task, src) : calculate_generic(s, task, src);
+  return calculate_fused(s, task, src);
 }
 
 static const thermal_equation::system_methods_t methods = {

@@ -389,7 +389,9 @@ int ffb_stats_get(ffb_ctx* ctx, ffb_stats* out);
  * or in a plugin host that forbids device allocations after start-up).
  * Same results as ffb_cast_bruteforce, without
  * a context: faces9, rays6, hit_face and hit_point (may be NULL) must all be
- * device memory; the work is enqueued on `stream` (a cudaStream_t, NULL for
+ * device memory of the current device (or managed memory), else FFB_ERR_ARG;
+ * n_rays is at most (2^31 - 1) * 128, else FFB_ERR_TOO_LARGE.  The work is
+ * enqueued on `stream` (a cudaStream_t, NULL for
  * the default stream) and the call returns without waiting.  The only
  * scratch, the per-face triangle records, lives in a static device array of
  * 16384 faces (1 MiB, held by every GPU that loads the library until exit);

@@ -277,11 +277,12 @@ int set_flags(emission::system_t* system, int flags);
 }  // namespace b200_emission
 
 namespace b200_form_factors {
-/* Form factors between meshes.  With a B200 emitter (or a NULL emitter) the
- * whole calculation -- emission, grid trace, per-(mesh, mesh) counts and the
- * row normalisation -- runs fused on the GPU and no ray batch is ever
- * materialised; with any other emitter it calls that emitter and counts on the
- * host as cpuFactorsCalculator/cpu_system.cpp:149-201 does.  Weights, the
+/* Form factors between meshes (cpuFactorsCalculator/cpu_system.cpp:149-201).
+ * The whole calculation -- emission, grid trace, per-(mesh, mesh) counts and
+ * the row normalisation -- runs fused on the GPU and no ray batch is ever
+ * materialised.  The emitter must be a B200 Malley emitter (its seed and
+ * flags key the draws) or NULL; init refuses any other emitter with
+ * -FORM_FACTORS_ERROR, since there is no host counting path.  Weights, the
  * total area (accumulating over prepare calls, cpu_system.cpp:126) and the
  * per-face ray budget follow the reference.  The fused path needs meshes that
  * cover every face exactly once in face order (the layout the reference's
@@ -309,10 +310,10 @@ int set_seed(emission::system_t* system, uint64_t seed);
 
 namespace b200_radiance_equation {
 /* The radiance equation (thermal_equation/radiance_cpu.cpp) for
- * radiance_equation::params_t.  With a B200 Malley emitter or a NULL emitter
- * the step runs fused on the GPU (ffb_radiance_step: the scene and grid stay
- * resident from set_scene; needs meshes covering every face once); with any
- * other emitter it runs the reference's algorithm over that emitter. */
+ * radiance_equation::params_t.  The step runs fused on the GPU
+ * (ffb_radiance_step: the scene and grid stay resident from set_scene; needs
+ * meshes covering every face once).  The emitter must be a B200 Malley
+ * emitter or NULL; init refuses any other with -THERMAL_EQUATION_ERROR. */
 thermal_equation::system_t* system_create();
 thermal_equation::system_t* create(radiance_equation::params_t* params);
 void destroy(thermal_equation::system_t* system);
@@ -322,9 +323,9 @@ int set_grid(thermal_equation::system_t* system, int nx, int ny, int nz, float c
 
 namespace b200_distant_source {
 /* The distant source of parallel rays (thermal_equation/parallel_rays_cpu.cpp)
- * for parallel_rays_cpu::params_t.  With a B200 parallel-rays emitter or a
- * NULL emitter the step runs fused on the GPU (ffb_distant_source_step); with
- * any other emitter it runs the reference's algorithm over that emitter. */
+ * for parallel_rays_cpu::params_t.  The step runs fused on the GPU
+ * (ffb_distant_source_step).  The emitter must be a B200 parallel-rays emitter
+ * or NULL; init refuses any other with -THERMAL_EQUATION_ERROR. */
 thermal_equation::system_t* system_create();
 thermal_equation::system_t* create(parallel_rays_cpu::params_t* params);
 void destroy(thermal_equation::system_t* system);

@@ -249,18 +249,6 @@ static std::vector<Calculator> calculators()
                  emission::system_free(e);
                  b200_ray_caster::destroy(r);
                }});
-  // B200 calculator over the reference emitter and caster (host counting path)
-  v.push_back({"B200 calculator + malley_cpu + naive_cpu",
-               [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
-                 *r = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
-                 *e = emission::system_create(EMISSION_MALLEY_CPU, *r);
-                 *f = b200_form_factors::create(*e);
-               },
-               [](form_factors::system_t* f, emission::system_t* e, ray_caster::system_t* r) {
-                 b200_form_factors::destroy(f);
-                 emission::system_free(e);
-                 ray_caster::system_free(r);
-               }});
   // the reference alone, as the control
   v.push_back({"CPU reference",
                [](form_factors::system_t** f, emission::system_t** e, ray_caster::system_t** r) {
@@ -544,17 +532,11 @@ static void thermal_suite()
       CHECK(em[m] == rem[m]);
       CHECK(within(ab[m], rab[m], 0.03f));
     }
-    // the B200 equation over the reference's emitter (the non-fused path)
+    // the B200 equation has no host absorption path: over the reference's
+    // emitter it refuses at init
     radiance_equation::params_t gp = {me, n_rays};
-    thermal_equation::system_t* mixed = b200_radiance_equation::create(&gp);
-    CHECK(mixed->methods->set_scene(mixed, &scene) == THERMAL_EQUATION_OK);
-    float gem[6] = {0}, gab[6] = {0};
-    thermal_equation::task_t gt = {temps, gem, gab};
-    CHECK(mixed->methods->calculate(mixed, &gt) == THERMAL_EQUATION_OK);
-    for (int m = 0; m < 6; ++m) {
-      CHECK(gem[m] == rem[m]);
-      CHECK(within(gab[m], rab[m], 0.03f));
-    }
+    thermal_equation::system_t* mixed = b200_radiance_equation::system_create();
+    CHECK(mixed->methods->init(mixed, &gp) == -THERMAL_EQUATION_ERROR);
     b200_radiance_equation::destroy(mixed);
     thermal_equation::system_free(ref);
     emission::system_free(me);
@@ -573,13 +555,9 @@ static void thermal_suite()
     thermal_equation::task_t rt = {temps, re, ra};
     CHECK(thermal_equation::system_calculate(ref, &rt) == THERMAL_EQUATION_OK);
     CHECK(within(ra[1], 300.f, 0.02f));
-    // the B200 equation over the reference's emitter
-    thermal_equation::system_t* mixed = b200_distant_source::create(&rp);
-    CHECK(mixed->methods->set_scene(mixed, &scene) == THERMAL_EQUATION_OK);
-    float ga[6] = {0}, ge[6] = {0};
-    thermal_equation::task_t gt = {temps, ge, ga};
-    CHECK(mixed->methods->calculate(mixed, &gt) == THERMAL_EQUATION_OK);
-    CHECK(within(ga[1], ra[1], 0.03f));
+    // over the reference's emitter the B200 equation refuses at init
+    thermal_equation::system_t* mixed = b200_distant_source::system_create();
+    CHECK(mixed->methods->init(mixed, &rp) == -THERMAL_EQUATION_ERROR);
     b200_distant_source::destroy(mixed);
     thermal_equation::system_free(ref);
     emission::system_free(pe);
@@ -665,8 +643,58 @@ static void obj_suite()
   std::remove(path);
 }
 
+// The B200 form-factor and thermal types run emission, trace and tallies
+// fused on the GPU and have no host path: an emitter of another type is
+// refused at init with the type's negative error code.
+static int foreign_init(emission::system_t*, ray_caster::system_t*) { return EMISSION_OK; }
+static int foreign_shutdown(emission::system_t*) { return EMISSION_OK; }
+static int foreign_set_scene(emission::system_t*, ray_caster::scene_t*) { return EMISSION_OK; }
+static int foreign_calculate(emission::system_t*, emission::task_t*) { return EMISSION_OK; }
+
+static void refusal_suite()
+{
+  static const emission::system_methods_t foreign_methods = {&foreign_init, &foreign_shutdown, &foreign_set_scene,
+                                                             &foreign_calculate};
+  emission::system_t foreign;
+  foreign.methods = &foreign_methods;
+
+  g_case = "B200 form factors refuse a foreign emitter";
+  {
+    form_factors::system_t* f = b200_form_factors::system_create();
+    CHECK(f->methods->init(f, &foreign) == -FORM_FACTORS_ERROR);
+    b200_form_factors::destroy(f);
+  }
+  g_case = "B200 radiance refuses a foreign emitter";
+  {
+    radiance_equation::params_t p = {&foreign, 1000};
+    thermal_equation::system_t* eq = b200_radiance_equation::system_create();
+    CHECK(eq->methods->init(eq, &p) == -THERMAL_EQUATION_ERROR);
+    b200_radiance_equation::destroy(eq);
+  }
+  g_case = "B200 distant source refuses a foreign emitter";
+  {
+    parallel_rays_cpu::params_t p = {1000, &foreign, 0, &sun_from_above};
+    thermal_equation::system_t* eq = b200_distant_source::system_create();
+    CHECK(eq->methods->init(eq, &p) == -THERMAL_EQUATION_ERROR);
+    b200_distant_source::destroy(eq);
+  }
+#ifdef FFB_WITH_REFERENCE
+  g_case = "B200 form factors refuse the reference's malley_cpu";
+  {
+    ray_caster::system_t* r = ray_caster::system_create(RAY_CASTER_NAIVE_CPU);
+    emission::system_t* e = emission::system_create(EMISSION_MALLEY_CPU, r);
+    form_factors::system_t* f = b200_form_factors::system_create();
+    CHECK(f->methods->init(f, e) == -FORM_FACTORS_ERROR);
+    b200_form_factors::destroy(f);
+    emission::system_free(e);
+    ray_caster::system_free(r);
+  }
+#endif
+}
+
 int main()
 {
+  refusal_suite();
   csv_suite();
   obj_suite();
   thermal_suite();
