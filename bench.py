@@ -54,15 +54,17 @@ def parse():
     ap.add_argument("--cpu-sample-every", type=int, default=0, help="reference sample: every k-th source face")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="", help="grid dims nx,ny,nz (default: automatic)")
-    ap.add_argument("--cells-per-face", type=float, default=192.0,
-                    help="automatic grid sizing target (192-256 measured fastest on this workload; the library default is 32)")
+    ap.add_argument("--cells-per-face", type=float, default=0.0,
+                    help="fixed grid sizing target (0: the autotuner chooses the grid among 128, 192 and 256 cells "
+                         "per face and the kernel's launch shape; the library default is 32)")
     ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
     ap.add_argument("--no-thermal", action="store_true", help="skip the radiance / distant-source section")
     ap.add_argument("--no-obj", action="store_true", help="skip the OBJ-import section")
-    ap.add_argument("--served-requests", type=int, default=16)
+    ap.add_argument("--served-requests", type=int, default=256)
+    ap.add_argument("--served-slots", type=int, default=16, help="requests prepared and traced at once")
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--served-sub-rate", type=float, default=0.5,
                     help="arrival rate of the sub-saturation run, requests/s (0: skip it)")
@@ -264,7 +266,9 @@ def batched_section(ctx, stream, args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     ev0.record(stream)
-    ctx.batch_set(sl, cells_per_face=args.cells_per_face, skip_empty=skip)
+    tuned = args.cells_per_face <= 0
+    ctx.batch_set(sl, cells_per_face=args.cells_per_face if not tuned else 32.0, skip_empty=skip)
+    shapes = ctx.batch_autotune(np.concatenate(fronts), np.concatenate(rears)) if tuned else None
     ctx.batch_prepare(np.concatenate(fronts), np.concatenate(rears), seeds)
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -284,10 +288,17 @@ def batched_section(ctx, stream, args):
     batched_s = ev0.elapsed_time(ev1) / 1e3
     del graph
 
+    def grid(i):
+        # the batch's choice for the scene (a cache hit of the autotuner), or the fixed grid
+        if tuned:
+            ctx.autotune(fronts[i], rears[i], int(seeds[i]))
+        else:
+            ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+
     def plain_scene(i, out=None):
         n = len(sl[i])
         ctx.scene_set(sl[i])
-        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        grid(i)
         ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2,
                                out=counts[int(offs[i]):int(offs[i]) + n * n], n_rows=n)
 
@@ -309,7 +320,7 @@ def batched_section(ctx, stream, args):
         e[0].record(stream)
         ctx.scene_set(f)
         e[1].record(stream)
-        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        grid(i)
         e[2].record(stream)
         ctx.form_factor_counts(fronts[i], rears[i], int(seeds[i]), epoch=2,
                                out=counts[int(offs[i]):int(offs[i]) + n * n], n_rows=n)
@@ -339,7 +350,7 @@ def batched_section(ctx, stream, args):
     for i, f in enumerate(sl):
         n = len(f)
         ctx.scene_set(f)
-        ctx.grid_build(cells_per_face=args.cells_per_face, skip_empty=skip)
+        grid(i)
         ctx.form_factors(fronts[i], rears[i], int(seeds[i]), epoch=2, n_rows=n,
                          out=host[:n * n].numpy().reshape(n, n))
     dropin_s = time.perf_counter() - t0
@@ -359,17 +370,29 @@ def batched_section(ctx, stream, args):
             "speedup_grid_build_in_both": plain_s / (batched_s + build_dev_s),
             "speedup_vs_dropin": dropin_s / batched_s,
             "ceiling": plain_s / trace_s,
-            "launches": "one fused launch per scene over 4 side streams, replayed as one CUDA graph"}
+            "launches": "one fused launch per scene over 4 side streams, replayed as one CUDA graph",
+            "autotuned": bool(tuned),
+            "shapes_used": sorted(set(int(v) for v in shapes)) if shapes is not None else [0]}
 
 
 # ---------------------------------------------------------------------------
 # served requests (Poisson arrivals, admission by memory budget)
 # ---------------------------------------------------------------------------
-def served_section(args):
-    """Requests of scenes with faces log-uniform 500-50k (the three families),
-    1k-100k front rays per face, Poisson arrivals at args.served_rate/s,
-    admitted by an 80 GB device budget into 4 slots; each result stays
-    resident until released.  Plain: the same requests one at a time."""
+def served_section(args, ctx, stream):
+    """Requests of scenes with faces log-uniform 500-50k (the three
+    families), 1k-100k front rays per face, Poisson arrivals at
+    args.served_rate/s.
+
+    served: the C++ serving loop -- admission by an 80 GB device budget into
+      args.served_slots slots, preparation on the slots' threads, traces in
+      16 Mi-ray slices round-robin over the prepared requests with two slices
+      in flight; results resident until released.
+    plain: the single-scene path, one request at a time in arrival order
+      (scene upload, grid build, zeroing and trace into a resident device
+      matrix), each request's latency from its arrival to its result.
+    ceiling = plain_s / sum(trace): the speed-up left if everything but the
+    traces (timed per request with CUDA events in the plain arm) went away."""
+    import torch
     from form_factors_b200 import native, scenes
     rng = np.random.default_rng(9)
     n = args.served_requests
@@ -378,9 +401,10 @@ def served_section(args):
     reqs = [(scenes.family_scene(fams[i % 3], sizes[i], rng), int(rng.integers(1000, 100001)), 100 + i)
             for i in range(n)]
     gaps = rng.exponential(1.0 / args.served_rate, n)
+    arrivals = np.cumsum(gaps)
     rays = sum(len(f) * r for f, r, _ in reqs)
 
-    def run(slots, arrivals, reqs=reqs):
+    def served(slots, arrivals, reqs):
         server = native.Server(0, budget_bytes=int(80e9), slots=slots)
         t0 = time.perf_counter()
         ids = []
@@ -388,19 +412,54 @@ def served_section(args):
             delay = t0 + at - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            ids.append(server.submit(f, r, sd))
+            ids.append(server.submit(f, r, sd, cells_per_face=0.0))
         infos = []
         for i in ids:
-            infos.append(server.wait(i, timeout_s=600))
+            infos.append(server.wait(i, timeout_s=1200))
             server.release(i)
         wall = time.perf_counter() - t0
-        peak = server.stats().peak_running
+        st = server.stats()
         server.close()
         lat = np.array([inf.latency_s for inf in infos])
-        return wall, lat, peak
+        spans = [(inf.trace_start_ns, inf.trace_end_ns) for inf in infos]
+        return wall, lat, st, spans, [inf.slices for inf in infos]
 
-    served_wall, lat, peak = run(4, np.cumsum(gaps))
-    plain_wall, plain_lat, _ = run(1, np.zeros(n))
+    def plain(arrivals, reqs):
+        nmax = max(len(f) for f, _, _ in reqs)
+        out = torch.empty(nmax * nmax, dtype=torch.int32, device="cuda")
+        lat, trace = [], []
+        ctx.set_stats(False)
+        t0 = time.perf_counter()
+        for (f, r, sd), at in zip(reqs, arrivals):
+            delay = t0 + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            k = len(f)
+            fr, re = np.full(k, r, np.int32), np.zeros(k, np.int32)
+            ctx.scene_set(f)
+            ctx.autotune(fr, re, sd)  # the cached choice: the grid and shape the server uses
+            ctx.form_factor_counts(fr, re, sd, epoch=0, out=out[:k * k], n_rows=k)
+            trace.append(ctx.stats().kernel_ms * 1e-3)  # synchronises: the result is resident
+            lat.append(time.perf_counter() - t0 - at)
+        wall = time.perf_counter() - t0
+        del out
+        torch.cuda.empty_cache()
+        return wall, np.array(lat), np.array(trace)
+
+    # both arms take the autotuner's cached choices: tune every request's
+    # scene class once, before either arm is timed
+    t0 = time.perf_counter()
+    for f, r, sd in reqs:
+        k = len(f)
+        ctx.scene_set(f)
+        ctx.autotune(np.full(k, r, np.int32), np.zeros(k, np.int32), sd)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    plain_wall, plain_lat, plain_trace = plain(arrivals, reqs)
+    served_wall, lat, st, spans, slices = served(args.served_slots, arrivals, reqs)
+    # device overlap: pairs of requests whose trace spans intersect
+    ordered = sorted((a, b) for a, b in spans if b > a)
+    overlaps = sum(1 for i in range(1, len(ordered)) if ordered[i][0] < max(e for _, e in ordered[:i]))
     sub = None
     if args.served_sub_rate > 0:
         # the same kind of requests at a rate the server keeps up with:
@@ -408,22 +467,34 @@ def served_section(args):
         m = args.served_sub_requests
         sub_reqs = [(scenes.family_scene(fams[i % 3], sizes[i % n], rng), int(rng.integers(1000, 100001)), 500 + i)
                     for i in range(m)]
-        sub_gaps = rng.exponential(1.0 / args.served_sub_rate, m)
-        sub_wall, sub_lat, sub_peak = run(4, np.cumsum(sub_gaps), sub_reqs)
+        for f, r, sd in sub_reqs:
+            ctx.scene_set(f)
+            ctx.autotune(np.full(len(f), r, np.int32), np.zeros(len(f), np.int32), sd)
+        sub_arr = np.cumsum(rng.exponential(1.0 / args.served_sub_rate, m))
+        sub_wall, sub_lat, sub_st, _, _ = served(args.served_slots, sub_arr, sub_reqs)
         sub_rays = sum(len(f) * r for f, r, _ in sub_reqs)
         sub = {"rate_per_s": args.served_sub_rate, "requests": m, "rays": int(sub_rays),
-               "offered_rays_per_s": sub_rays / max(float(np.sum(sub_gaps)), 1e-9),
+               "offered_rays_per_s": sub_rays / max(float(sub_arr[-1]), 1e-9),
                "p50_latency_s": float(np.percentile(sub_lat, 50)),
                "p99_latency_s": float(np.percentile(sub_lat, 99)),
-               "max_latency_s": float(sub_lat.max()), "wall_s": sub_wall, "peak_concurrent": int(sub_peak)}
+               "max_latency_s": float(sub_lat.max()), "wall_s": sub_wall, "peak_concurrent": int(sub_st.peak_running)}
     return {"workload": "%d requests, faces log-uniform 500-50000 (plates/UV spheres/clutter), 1k-100k front "
-                        "rays/face, Poisson %.0f req/s, 80 GB budget, 4 slots" % (n, args.served_rate),
-            "requests": n, "rays": int(rays), "served_scenes_per_s": n / served_wall, "plain_scenes_per_s": n / plain_wall,
-            "speedup_scenes_per_s": plain_wall / served_wall, "served_rays_per_s": rays / served_wall,
+                        "rays/face, Poisson %.0f req/s, 80 GB budget, %d slots" % (n, args.served_rate,
+                                                                                  args.served_slots),
+            "requests": n, "rays": int(rays), "served_scenes_per_s": n / served_wall,
+            "plain_scenes_per_s": n / plain_wall, "speedup_scenes_per_s": plain_wall / served_wall,
+            "served_rays_per_s": rays / served_wall, "plain_rays_per_s": rays / plain_wall,
+            "served_wall_s": served_wall, "plain_wall_s": plain_wall, "plain_trace_s": float(plain_trace.sum()),
+            "ceiling": plain_wall / float(plain_trace.sum()),
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "plain_p50_latency_s": float(np.percentile(plain_lat, 50)),
-            "offered_rays_per_s": rays / max(float(np.sum(gaps)), 1e-9), "peak_concurrent": int(peak),
+            "plain_p99_latency_s": float(np.percentile(plain_lat, 99)),
+            "latency_samples": int(len(lat)),
+            "offered_rays_per_s": rays / max(float(arrivals[-1]), 1e-9), "peak_concurrent": int(st.peak_running),
+            "peak_tracing": int(st.peak_tracing), "trace_slices": int(sum(slices)),
+            "requests_overlapping_on_device": int(overlaps),
             "note": "offered load far above capacity: latency is queueing under saturation",
+            "autotune_warmup_s": tune_s,
             "sub_saturation": sub}
 
 
@@ -682,7 +753,7 @@ def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm):
 def ours(args):
     import torch
     import torch.distributed as dist
-    from form_factors_b200 import build, native
+    from form_factors_b200 import build, native, shard
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -704,16 +775,38 @@ def ours(args):
     ctx.scene_set(faces)
     ctx.set_stats(False)  # timed launches run the kernel without counters
     dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
+    tune = None
+    if dims is None and args.cells_per_face <= 0:
+        # grid and launch shape chosen by the autotuner on a ~4 Mi-ray sample
+        # (rank 0's choice on every rank)
+        t0 = time.perf_counter()
+        tune = ctx.autotune(front, rear, SEED, candidates=[dict(cells_per_face=c, skip_empty=not args.no_skip)
+                                                           for c in (128.0, 192.0, 256.0)], force=True)
+        tune["tuning_s"] = time.perf_counter() - t0
+        if world > 1:
+            pick = torch.tensor([tune["cells_per_face"], float(tune["shape"])], device="cuda")
+            dist.broadcast(pick, 0)
+            tune["cells_per_face"], tune["shape"] = float(pick[0].item()), int(pick[1].item())
+            ctx.set_trace_shape(tune["shape"])
+        tune["shape_params"] = native.trace_shapes()[tune["shape"]]
+        ctx.set_stats(False)
     t0 = time.perf_counter()
-    ctx.grid_build(dims=dims, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
+    if tune is None:
+        ctx.grid_build(dims=dims, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
+    else:
+        ctx.grid_build(cells_per_face=tune["cells_per_face"], skip_empty=tune["skip_empty"])
     torch.cuda.synchronize()
     grid_s = time.perf_counter() - t0
     info = ctx.grid_info()
-    counts = torch.empty(n * n, dtype=torch.int32, device="cuda")  # uint32 bit patterns
+    # source rows of this rank (all of them on one GPU): ranks split the rows
+    # of the one solve, balanced by rays, and exchange nothing while tracing
+    row_b, row_e = shard.rank_rows(front, rear, rank, world)
+    rows = row_e - row_b
+    counts = torch.empty(rows * n, dtype=torch.int32, device="cuda")  # uint32 bit patterns
 
     def step(i, out=counts):
-        # replicas: each rank solves the same scene with its own Philox epoch
-        ctx.form_factor_counts(front, rear, SEED, epoch=1000 * rank + i, out=out, n_rows=n)
+        # every rank draws the rays of its own rows of the same solve (epoch i)
+        ctx.form_factor_counts_rows(front, rear, SEED, row_b, row_e, epoch=i, out=out)
 
     for i in range(args.warmup):
         step(i)
@@ -741,7 +834,7 @@ def ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_step = ms / args.steps
-    value = world * rays_per_step / (ms_step * 1e-3)
+    value = rays_per_step / (ms_step * 1e-3)  # all ranks' rays of one solve per step
 
     # kernel-only time of the fused kernel (one launch per step), then one
     # untimed launch of the variant with counters for the work per launch
@@ -754,13 +847,19 @@ def ours(args):
     step(10_003)
     s = ctx.stats()
     ctx.set_stats(False)
-    tests, cells, hits, jumps = s.tests, s.cells, s.hits, s.jumps
+    work = torch.tensor([s.tests, s.cells, s.hits, s.jumps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(work)
+        t = torch.tensor([k_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        k_ms = float(t.item())
+    tests, cells, hits, jumps = [float(x) for x in work.tolist()]
     tests_per_launch = tests
     achieved = tests_per_launch * FLOPS_PER_TEST / (k_ms * 1e-3)
     peak = fp32_peak(local)
 
     # end to end through the C ABI with host buffers
-    host_counts = torch.empty(n * n, dtype=torch.int32, pin_memory=True)
+    host_counts = torch.empty(rows * n, dtype=torch.int32, pin_memory=True)
     e2e_steps = max(2, min(args.steps, 5))
     step(20_000, out=host_counts)
     torch.cuda.synchronize()
@@ -774,10 +873,23 @@ def ours(args):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # host -> device per step: one 16-byte record per emitting face (face,
-    # its ray counts, its first work chunk); the chunks are built on the GPU
+    # host -> device per step (all ranks): one 16-byte record per emitting
+    # face (face, its ray counts, its first work chunk), the chunks built on
+    # the GPU; device -> host: every rank's row block, the whole matrix
     h2d = 16 * int(np.count_nonzero(front.astype(np.int64) + rear))
     d2h = 4 * n * n
+    gather = None
+    if world > 1:
+        # the full matrix on every rank: one NCCL all_gather of the row
+        # blocks, after the timed region
+        torch.cuda.synchronize()
+        g0 = time.perf_counter()
+        full = shard.gather_rows(counts.view(rows, n), row_b, row_e, n)
+        torch.cuda.synchronize()
+        ok = torch.equal(full[row_b:row_e], counts.view(rows, n))
+        gather = {"s": time.perf_counter() - g0, "bytes": 4 * n * n, "own_rows_equal": bool(ok),
+                  "rows": [row_b, row_e]}
+        del full
 
     batched = served = csv = thermal = None
     if rank == 0 and world == 1 and not args.no_csv:
@@ -790,7 +902,7 @@ def ours(args):
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_section(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_served:
-        served = served_section(args)
+        served = served_section(args, ctx, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -799,12 +911,17 @@ def ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "faces": n, "rays_per_step": rays_per_step,
-                       "grid": [info.nx, info.ny, info.nz], "cells_per_face": args.cells_per_face,
+                       "grid": [info.nx, info.ny, info.nz],
+                       "cells_per_face": tune["cells_per_face"] if tune else args.cells_per_face,
+                       "autotune": tune, "trace_shape": ctx.trace_shape(),
                        "grid_refs": int(info.n_refs),
-                       "grid_build_ms": 1e3 * grid_s, "parallelism": "replicas" if world > 1 else "single",
+                       "grid_build_ms": 1e3 * grid_s,
+                       "parallelism": "source rows split over %d ranks (one solve)" % world if world > 1 else "single",
+                       "gather": gather,
                        "l2": "flushed each step by zeroing the 1.95 GB count matrix"},
             "e2e": {"value": world * rays_per_step / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -820,7 +937,7 @@ def ours(args):
                                  "frac": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
                                  "peak_source": hbm_peak()[1],
                                  "note": "DRAM bytes per launch (ncu) / kernel time, of the copy bandwidth"},
-                         "issue": issue_roofline(k_ms, rays_per_step, clk.get("sm_mhz"),
+                         "issue": issue_roofline(k_ms, rays_per_step / world, clk.get("sm_mhz"),
                                                  torch.cuda.get_device_properties(local).multi_processor_count)},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,

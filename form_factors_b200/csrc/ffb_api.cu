@@ -16,11 +16,15 @@
 #include <vector>
 
 #include <map>
+#include <mutex>
+#include <tuple>
+#include <utility>
 
 #include <cuda_runtime.h>
 
 #include "ffb.h"
 #include "ffb_csv.cuh"
+#include "ffb_internal.h"
 #include "ffb_obj.cuh"
 #include "ffb_trace.cuh"
 
@@ -103,6 +107,7 @@ struct ffb_ctx {
   unsigned long long budget = 0;  // 0 = unlimited
   unsigned long long bytes = 0;   // device bytes held in DevBufs
   bool stats_on = true;           // fused kernel with counters
+  int trace_shape = 0;            // launch shape of the fused kernel (trace_shape(), chosen by ffb_autotune)
 
   SceneData main;                 // the scene of the single-scene calls
   DevBuf frames;                  // emission frames of the main scene
@@ -114,6 +119,7 @@ struct ffb_ctx {
   int batch_frames_mode = -1;
   int batch_n_chunks = 0;
   std::vector<int> batch_chunk_first;  // first chunk of each scene (scene-major), plus the total
+  std::vector<int> batch_shape;        // launch shape of each scene (ffb_batch_autotune), default 0
   // side streams of the batched launch: one launch per scene, spread over
   // them so that a scene's launch tail overlaps the next scenes
   cudaStream_t batch_streams[4] = {};
@@ -123,6 +129,10 @@ struct ffb_ctx {
   DevBuf scan_sums, chunks, chunk_src, rows, cursor, stats, tmp_in, tmp_out, tmp_out2, offsets, front_dev, ray_cursor, ff_counts;
   DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
   DevBuf power_tab, absorb;                     // radiance sink
+  DevBuf span;                                  // sliced traces: earliest start / latest end (globaltimer ns)
+  TraceParams slice_params{};                   // sliced traces: the prepared launch
+  bool slice_ready = false;
+  long long slice_chunks = 0;
   // OBJ import: the text and its line tables, the parsed geometry
   DevBuf obj_text, obj_chunk, obj_chunk_off, obj_starts, obj_flags, obj_ords, obj_vertices, obj_face_idx,
       obj_face_line, obj_special, obj_ranges, obj_faces, obj_err;
@@ -532,12 +542,12 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
 }
 
 // Appends the chunks of face rays [0, front + rear) of every face.
-void add_chunks(std::vector<Chunk>& out, const int32_t* front, const int32_t* rear, int n_faces, int scene)
+void add_chunks(std::vector<Chunk>& out, const int32_t* front, const int32_t* rear, int n_faces)
 {
   for (int f = 0; f < n_faces; ++f) {
     const int nf = front[f] + rear[f];
     for (int j0 = 0; j0 < nf; j0 += kChunkRays)
-      out.push_back(Chunk{f, j0, (int16_t)std::min(kChunkRays, nf - j0), (int16_t)scene, front[f]});
+      out.push_back(Chunk{f, j0, std::min(kChunkRays, nf - j0), front[f]});
   }
 }
 
@@ -593,18 +603,32 @@ int check_counts(int n_faces, const int32_t* front, const int32_t* rear, long lo
 #define FFB_DIRECT_MIN_WORDS (1ull << 22)
 #endif
 
-// Occupancy-sized persistent launch of the fused kernel for p.n_chunks chunks.
+// The timed kernel variant (no counters, matrix sink) for each launch shape.
+template <bool kSkip, bool kHash, int... S>
+void (*shaped_kernel(int shape, std::integer_sequence<int, S...>))(TraceParams)
+{
+  static void (*const table[])(TraceParams) = {k_form_factors<kSkip, false, kHash, false, S>...};
+  return table[shape];
+}
+
+// Occupancy-sized persistent launch of the fused kernel for p.n_chunks
+// chunks, in the context's launch shape (the counter and radiance variants
+// always take shape 0).
 template <bool kSkip>
-int launch_fused(ffb_ctx* c, const TraceParams& p, bool timed, cudaStream_t stream = nullptr)
+int launch_fused(ffb_ctx* c, const TraceParams& p, bool timed, cudaStream_t stream = nullptr, int shape = -1)
 {
   if (!stream)
     stream = c->stream;
+  if (shape < 0)
+    shape = c->trace_shape;
   bool hash = (unsigned long long)p.scene.n_cols * (unsigned long long)p.scene.n_cols < FFB_DIRECT_MIN_WORDS;
   void (*kern)(TraceParams);
   if (p.stats)
     kern = hash ? k_form_factors<kSkip, true, true> : k_form_factors<kSkip, true, false>;
+  else if (hash)
+    kern = shaped_kernel<kSkip, true>(shape, std::make_integer_sequence<int, kNumShapes>{});
   else
-    kern = hash ? k_form_factors<kSkip, false, true> : k_form_factors<kSkip, false, false>;
+    kern = shaped_kernel<kSkip, false>(shape, std::make_integer_sequence<int, kNumShapes>{});
   if (p.power) {  // radiance sink: no matrix, no histogram
     kern = p.stats ? k_form_factors<kSkip, true, false, true> : k_form_factors<kSkip, false, false, true>;
     hash = false;
@@ -690,7 +714,7 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
                     &c->scan_sums, &c->chunks,      &c->chunk_src,    &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
                     &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
-                    &c->power_tab, &c->absorb, &c->obj_text, &c->obj_chunk, &c->obj_chunk_off,
+                    &c->power_tab, &c->absorb, &c->span, &c->obj_text, &c->obj_chunk, &c->obj_chunk_off,
                     &c->obj_starts, &c->obj_flags, &c->obj_ords, &c->obj_vertices, &c->obj_face_idx,
                     &c->obj_face_line, &c->obj_special, &c->obj_ranges, &c->obj_faces, &c->obj_err};
   for (DevBuf* b : bufs)
@@ -1036,6 +1060,7 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
   p.power = nullptr;
   p.absorb = nullptr;
+  p.span = nullptr;
   p.scene.g = make_view(s);
   // the kernel adds at row * n_rows + col; the output holds rows from
   // row_begin, so its base is moved back by row_begin rows (only rows of the
@@ -1083,6 +1108,99 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     FFB_CUDA(cudaStreamWaitEvent(c->stream, c->copies_done, 0));
   }
   FFB_CUDA(cudaStreamSynchronize(c->stream));
+  return FFB_OK;
+}
+
+// ===========================================================================
+// Sliced traces (the serving loop of ffb_server.cpp): one prepared launch
+// whose chunk table is traced in consecutive slices, each its own launch on
+// the context stream, all adding into the same device count matrix.
+// ===========================================================================
+int ffb_trace_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
+                      uint32_t* counts, long long* n_chunks)
+{
+  FFB_TRY(check_ctx(c));
+  c->slice_ready = false;
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (!s.grid_ok)
+    return fail(FFB_ERR_NO_GRID, "sliced trace before ffb_grid_build");
+  if (s.n_faces > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "%d faces; at most %d", s.n_faces, kMaxRows);
+  long long total = 0;
+  FFB_TRY(check_counts(s.n_faces, front, rear, &total));
+  bool dev = false;
+  FFB_TRY(ptr_kind(c, counts, &dev));
+  if (!counts || !dev || !n_chunks)
+    return fail(FFB_ERR_ARG, "sliced traces need a device count matrix and a chunk-count output");
+  FFB_TRY(ensure_frames(c, flags));
+  std::vector<int32_t> order;
+  order.reserve((size_t)s.n_faces);
+  for (int f = 0; f < s.n_faces; ++f)
+    if (front[f] + (long long)rear[f] > 0)
+      order.push_back(f);
+  std::vector<long long> first;
+  long long nch = 0;
+  FFB_TRY(device_chunks(c, order, front, rear, first, &nch));
+  FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * kMaxPipeBlocks));
+  FFB_TRY(ensure(c, c->span, 2 * sizeof(unsigned long long)));
+  const unsigned long long span0[2] = {~0ull, 0ull};
+  FFB_TRY(upload(c, c->span, span0, sizeof span0));
+  FFB_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)s.n_faces * s.n_faces, c->stream));
+  TraceParams& p = c->slice_params;
+  p.frames = dptr<float>(c->frames);
+  p.chunks = dptr<Chunk>(c->chunks);
+  p.n_chunks = 0;
+  p.key0 = (uint32_t)seed;
+  p.key1 = (uint32_t)(seed >> 32);
+  p.epoch = epoch;
+  p.epoch_ptr = nullptr;
+  p.scene_keys = nullptr;
+  p.chunk_cursor = dptr<uint32_t>(c->cursor);
+  p.stats = nullptr;
+  p.power = nullptr;
+  p.absorb = nullptr;
+  p.span = dptr<unsigned long long>(c->span);
+  p.scene.g = make_view(s);
+  p.scene.counts = counts;
+  p.scene.face_to_row = nullptr;
+  p.scene.face_base = 0;
+  p.scene.n_cols = s.n_faces;
+  c->slice_chunks = nch;
+  c->slice_ready = true;
+  *n_chunks = nch;
+  return FFB_OK;
+}
+
+int ffb_trace_slice(ffb_ctx* c, long long first, long long count)
+{
+  FFB_TRY(check_ctx(c));
+  if (!c->slice_ready)
+    return fail(FFB_ERR_ARG, "ffb_trace_slice before ffb_trace_prepare");
+  if (first < 0 || count <= 0 || first + count > c->slice_chunks || count > INT_MAX)
+    return fail(FFB_ERR_ARG, "slice [%lld, %lld) outside the %lld prepared chunks", first, first + count,
+                c->slice_chunks);
+  TraceParams p = c->slice_params;
+  p.chunks = dptr<Chunk>(c->chunks) + first;
+  p.n_chunks = (int)count;
+  // slices of one context run in stream order, so one cursor serves them all
+  FFB_CUDA(cudaMemsetAsync(p.chunk_cursor, 0, sizeof(uint32_t), c->stream));
+  if (c->main.info.skip_empty)
+    return launch_fused<true>(c, p, false);
+  return launch_fused<false>(c, p, false);
+}
+
+int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long* end_ns)
+{
+  FFB_TRY(check_ctx(c));
+  unsigned long long v[2] = {0, 0};
+  if (c->span.ptr) {
+    FFB_CUDA(cudaMemcpyAsync(v, c->span.ptr, sizeof v, cudaMemcpyDeviceToHost, c->stream));
+    FFB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  *start_ns = v[0] == ~0ull ? 0 : v[0];
+  *end_ns = v[1];
   return FFB_OK;
 }
 
@@ -1197,6 +1315,7 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
     p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
     p.power = dptr<unsigned long long>(c->power_tab);
     p.absorb = dptr<unsigned long long>(c->absorb);
+    p.span = nullptr;
     p.scene.g = make_view(s);
     p.scene.counts = nullptr;
     p.scene.face_to_row = dptr<int32_t>(c->rows);
@@ -1876,6 +1995,7 @@ extern "C" int ffb_batch_set(ffb_ctx* c, int n_scenes, const long long* face_off
   c->batch_offsets.assign(face_offsets, face_offsets + n_scenes + 1);
   c->batch_frames_mode = -1;
   c->batch_n_chunks = 0;
+  c->batch_shape.assign((size_t)n_scenes, 0);
   for (int s = 0; s < n_scenes; ++s) {
     const long long f0 = face_offsets[s];
     const int n = (int)(face_offsets[s + 1] - f0);
@@ -1909,7 +2029,7 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
   for (int s = 0; s < n_scenes; ++s) {
     const long long f0 = c->batch_offsets[s];
     c->batch_chunk_first[s] = (int)chunks.size();
-    add_chunks(chunks, front + f0, rear + f0, c->batch[s].n_faces, s);
+    add_chunks(chunks, front + f0, rear + f0, c->batch[s].n_faces);
   }
   c->batch_chunk_first[n_scenes] = (int)chunks.size();
   c->batch_n_chunks = (int)chunks.size();
@@ -1993,6 +2113,7 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     p.stats = c->stats_on ? dptr<unsigned long long>(c->stats) : nullptr;
     p.power = nullptr;
     p.absorb = nullptr;
+    p.span = nullptr;
     SceneSlot& slot = p.scene;
     slot.g = make_view(c->batch[s]);
     slot.counts = counts + counts_offsets[s];
@@ -2000,10 +2121,11 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
     slot.face_base = (int)c->batch_offsets[s];
     slot.n_cols = c->batch[s].n_faces;
     cudaStream_t st = c->batch_streams[k++ % kSide];
+    const int shape = s < (int)c->batch_shape.size() ? c->batch_shape[(size_t)s] : 0;
     if (c->batch[s].info.skip_empty)
-      FFB_TRY((launch_fused<true>(c, p, false, st)));
+      FFB_TRY((launch_fused<true>(c, p, false, st, shape)));
     else
-      FFB_TRY((launch_fused<false>(c, p, false, st)));
+      FFB_TRY((launch_fused<false>(c, p, false, st, shape)));
   }
   for (int j = 0; j < kSide; ++j) {
     FFB_CUDA(cudaEventRecord(c->batch_join[j], c->batch_streams[j]));
@@ -2013,45 +2135,234 @@ extern "C" int ffb_batch_launch(ffb_ctx* c, uint32_t* counts, const unsigned lon
 }
 
 // ===========================================================================
-// Autotuning of the grid
+// Autotuning: grid and launch shape
 // ===========================================================================
-extern "C" int ffb_autotune_grid(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
-                                 const ffb_grid_params* candidates, int n_candidates, int sample_every,
-                                 ffb_grid_params* best, float* best_ms)
+namespace {
+
+// Process-wide cache of tuning choices: (faces in half-octaves, scene-box
+// aspect in octaves, rays per emitting face in octaves, jumps on/off).
+typedef std::tuple<int, int, int, int> TuneKey;
+struct TuneChoice {
+  ffb_grid_params grid;
+  int shape;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+int tune_key(ffb_ctx* c, SceneData& s, const int32_t* front, const int32_t* rear, int skip, TuneKey* key)
+{
+  uint32_t ord[6];
+  FFB_CUDA(cudaMemcpyAsync(ord, s.scene_ord.ptr, sizeof ord, cudaMemcpyDeviceToHost, c->stream));
+  FFB_CUDA(cudaStreamSynchronize(c->stream));
+  double lo = INFINITY, hi = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double e = (double)ord2f(ord[3 + a]) - (double)ord2f(ord[a]);
+    if (e > 0.0 && std::isfinite(e)) {
+      lo = std::min(lo, e);
+      hi = std::max(hi, e);
+    }
+  }
+  const int aspect = hi > 0.0 ? (int)std::lround(std::log2(hi / std::max(lo, hi * 1e-3))) : 0;
+  long long rays = 0, emitting = 0;
+  for (int f = 0; f < s.n_faces; ++f) {
+    const long long nf = (long long)front[f] + rear[f];
+    rays += nf;
+    emitting += nf > 0;
+  }
+  const int per_face = emitting ? (int)std::lround(std::log2(std::max(1.0, (double)rays / emitting))) : 0;
+  *key = TuneKey((int)std::lround(2.0 * std::log2((double)std::max(s.n_faces, 1))), aspect, per_face, skip);
+  return FFB_OK;
+}
+
+// Kernel time (ms, best of two runs: the first warms the grid into L2) of
+// the sample trace in launch shape `shape`, counts into device `counts`.
+int time_sample(ffb_ctx* c, const int32_t* fr, const int32_t* re, uint64_t seed, uint32_t* counts, int shape,
+                float* ms)
+{
+  const int saved_shape = c->trace_shape;
+  const bool saved_stats = c->stats_on;
+  c->trace_shape = shape;
+  c->stats_on = false;
+  float best = INFINITY;
+  int rc = FFB_OK;
+  for (int rep = 0; rep < 2 && rc == FFB_OK; ++rep) {
+    rc = ffb_form_factor_counts(c, fr, re, seed, 0, 0, nullptr, c->main.n_faces, counts);
+    float t = 0;
+    if (rc == FFB_OK && cudaStreamSynchronize(c->stream) == cudaSuccess &&
+        cudaEventElapsedTime(&t, c->ev0, c->ev1) == cudaSuccess)
+      best = std::min(best, t);
+    else if (rc == FFB_OK)
+      rc = fail(FFB_ERR_CUDA, "timing of a tuning sample failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  c->trace_shape = saved_shape;
+  c->stats_on = saved_stats;
+  *ms = best;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int ffb_trace_shape_count(void) { return kNumShapes; }
+
+extern "C" int ffb_trace_shape_get(int shape, ffb_trace_shape* out)
+{
+  if (shape < 0 || shape >= kNumShapes || !out)
+    return fail(FFB_ERR_ARG, "shape %d outside [0, %d)", shape, kNumShapes);
+  const TraceShape t = trace_shape(shape);
+  *out = ffb_trace_shape{t.adv, t.test, t.refill, t.blocks};
+  return FFB_OK;
+}
+
+extern "C" int ffb_ctx_set_trace_shape(ffb_ctx* c, int shape)
+{
+  if (!c)
+    return fail(FFB_ERR_ARG, "null context");
+  if (shape < 0 || shape >= kNumShapes)
+    return fail(FFB_ERR_ARG, "shape %d outside [0, %d)", shape, kNumShapes);
+  c->trace_shape = shape;
+  return FFB_OK;
+}
+
+extern "C" int ffb_ctx_trace_shape(ffb_ctx* c) { return c ? c->trace_shape : FFB_ERR_ARG; }
+
+extern "C" int ffb_autotune(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                            const ffb_grid_params* candidates, int n_candidates, int sample_every, int flags,
+                            uint32_t* scratch, ffb_tune_result* out)
 {
   FFB_TRY(check_ctx(c));
   SceneData& s = c->main;
   if (s.n_faces <= 0)
     return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (s.n_faces > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "scene of %d faces; at most %d", s.n_faces, kMaxRows);
+  if (candidates && n_candidates <= 0)
+    return fail(FFB_ERR_ARG, "no candidates");
+  long long total = 0;
+  FFB_TRY(check_counts(s.n_faces, front, rear, &total));
+  std::vector<ffb_grid_params> cands;
+  if (candidates) {
+    cands.assign(candidates, candidates + n_candidates);
+  } else {
+    for (float cpf : {32.f, 64.f, 128.f, 192.f, 256.f})
+      cands.push_back(ffb_grid_params{0, 0, 0, cpf, 1});
+  }
+  int skip_key = 0;
+  for (const ffb_grid_params& g : cands)
+    skip_key |= g.skip_empty ? 1 : 2;
+  ffb_tune_result res{};
+  TuneKey key;
+  FFB_TRY(tune_key(c, s, front, rear, skip_key, &key));
+  if (!(flags & FFB_TUNE_FORCE)) {
+    TuneChoice hit{};
+    bool found = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        hit = it->second;
+        found = true;
+      }
+    }
+    if (found) {
+      FFB_TRY(grid_build(c, s, &hit.grid));
+      c->trace_shape = hit.shape;
+      res.grid = hit.grid;
+      res.shape = hit.shape;
+      res.from_cache = 1;
+      if (out)
+        *out = res;
+      return FFB_OK;
+    }
+  }
+  // the sample: every k-th face emits its rays (the same rays as in the full solve)
+  if (sample_every <= 0)
+    sample_every = (int)std::max<long long>(1, (total + (2ll << 20)) / (4ll << 20));
+  std::vector<int32_t> fr((size_t)s.n_faces, 0), re((size_t)s.n_faces, 0);
+  long long sample_rays = 0;
+  for (int f = 0; f < s.n_faces; f += sample_every) {
+    fr[f] = front[f];
+    re[f] = rear[f];
+    sample_rays += (long long)front[f] + rear[f];
+  }
+  res.sample_rays = sample_rays;
+  uint32_t* counts = scratch;
+  if (counts) {
+    bool dev = false;
+    FFB_TRY(ptr_kind(c, counts, &dev));
+    if (!dev)
+      return fail(FFB_ERR_ARG, "tuning scratch must be device memory");
+  } else {
+    FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * (size_t)s.n_faces * s.n_faces));
+    counts = dptr<uint32_t>(c->ff_counts);
+  }
+  int best_g = 0, best_shape = 0;
+  float best_t = INFINITY;
+  if (sample_rays > 0) {
+    for (size_t i = 0; i < cands.size(); ++i) {
+      FFB_TRY(grid_build(c, s, &cands[i]));
+      float t;
+      FFB_TRY(time_sample(c, fr.data(), re.data(), seed, counts, 0, &t));
+      ++res.timed;
+      if (t < best_t) {
+        best_t = t;
+        best_g = (int)i;
+      }
+    }
+    FFB_TRY(grid_build(c, s, &cands[(size_t)best_g]));
+    for (int shape = 1; shape < kNumShapes; ++shape) {
+      float t;
+      FFB_TRY(time_sample(c, fr.data(), re.data(), seed, counts, shape, &t));
+      ++res.timed;
+      if (t < best_t) {
+        best_t = t;
+        best_shape = shape;
+      }
+    }
+  } else {
+    FFB_TRY(grid_build(c, s, &cands[0]));
+    best_t = 0.f;
+  }
+  c->trace_shape = best_shape;
+  res.grid = cands[(size_t)best_g];
+  res.shape = best_shape;
+  res.sample_ms = best_t;
+  if (sample_rays > 0) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = TuneChoice{res.grid, res.shape};
+  }
+  if (out)
+    *out = res;
+  return FFB_OK;
+}
+
+extern "C" int ffb_autotune_grid(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                 const ffb_grid_params* candidates, int n_candidates, int sample_every,
+                                 ffb_grid_params* best, float* best_ms)
+{
+  FFB_TRY(check_ctx(c));
   if (!candidates || n_candidates <= 0 || !best)
     return fail(FFB_ERR_ARG, "no candidates");
+  SceneData& s = c->main;
+  if (s.n_faces <= 0)
+    return fail(FFB_ERR_NO_SCENE, "no scene");
+  if (s.n_faces > kMaxRows)
+    return fail(FFB_ERR_TOO_LARGE, "scene too large");
   long long total = 0;
   FFB_TRY(check_counts(s.n_faces, front, rear, &total));
   if (sample_every < 1)
     sample_every = 1;
-  // sample: every k-th face emits (same rays as in the full solve)
   std::vector<int32_t> fr((size_t)s.n_faces, 0), re((size_t)s.n_faces, 0);
   for (int f = 0; f < s.n_faces; f += sample_every) {
     fr[f] = front[f];
     re[f] = rear[f];
   }
-  const size_t mat = (size_t)s.n_faces * s.n_faces;
-  if (s.n_faces > kMaxRows)
-    return fail(FFB_ERR_TOO_LARGE, "scene too large");
-  FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * mat));
+  FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * (size_t)s.n_faces * s.n_faces));
   float best_t = INFINITY;
-  int best_i = -1;
+  int best_i = 0;
   for (int i = 0; i < n_candidates; ++i) {
     FFB_TRY(grid_build(c, s, candidates + i));
-    float t = INFINITY;
-    for (int rep = 0; rep < 2; ++rep) {  // first run warms the grid into L2
-      FFB_TRY(ffb_form_factor_counts(c, fr.data(), re.data(), seed, 0, 0, nullptr, s.n_faces,
-                                     dptr<uint32_t>(c->ff_counts)));
-      FFB_CUDA(cudaStreamSynchronize(c->stream));
-      float ms = 0;
-      FFB_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-      t = std::min(t, ms);
-    }
+    float t;
+    FFB_TRY(time_sample(c, fr.data(), re.data(), seed, dptr<uint32_t>(c->ff_counts), c->trace_shape, &t));
     if (t < best_t) {
       best_t = t;
       best_i = i;
@@ -2061,6 +2372,46 @@ extern "C" int ffb_autotune_grid(ffb_ctx* c, const int32_t* front, const int32_t
   if (best_ms)
     *best_ms = best_t;
   return grid_build(c, s, best);
+}
+
+extern "C" int ffb_batch_autotune(ffb_ctx* c, const int32_t* front, const int32_t* rear, int* shapes)
+{
+  FFB_TRY(check_ctx(c));
+  const int n_scenes = (int)c->batch.size();
+  if (!n_scenes)
+    return fail(FFB_ERR_NO_SCENE, "no batch set");
+  long long total = 0;
+  FFB_TRY(check_counts((int)c->batch_offsets[n_scenes], front, rear, &total));
+  c->batch_shape.assign((size_t)n_scenes, 0);
+  for (int i = 0; i < n_scenes; ++i) {
+    SceneData& b = c->batch[i];
+    const long long f0 = c->batch_offsets[i];
+    TuneKey key;
+    FFB_TRY(tune_key(c, b, front + f0, rear + f0, 1, &key));
+    TuneChoice choice{};
+    bool found = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        choice = it->second;
+        found = true;
+      }
+    }
+    if (!found) {
+      // tune on this scene through the main scene (the faces copy on the device)
+      c->frames_mode = -1;
+      FFB_TRY(scene_upload(c, c->main, dptr<float>(b.faces), b.n_faces));
+      ffb_tune_result r;
+      FFB_TRY(ffb_autotune(c, front + f0, rear + f0, 1, nullptr, 0, 0, FFB_TUNE_FORCE, nullptr, &r));
+      choice = TuneChoice{r.grid, r.shape};
+    }
+    FFB_TRY(grid_build(c, b, &choice.grid));
+    c->batch_shape[(size_t)i] = choice.shape;
+    if (shapes)
+      shapes[i] = choice.shape;
+  }
+  return FFB_OK;
 }
 
 extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)

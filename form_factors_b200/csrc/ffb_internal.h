@@ -1,0 +1,27 @@
+// ffb_internal.h -- library-internal entry points shared by the translation
+// units of libffb200.so (not part of the public C ABI in include/ffb.h).
+#pragma once
+
+#include <cstdint>
+
+#include "ffb.h"
+
+// Records an error for ffb_last_error and returns `code`.
+int ffb_set_error(int code, const char* msg);
+
+// Sliced traces, for the serving loop.  ffb_trace_prepare readies one fused
+// form-factor trace of the context's scene (grid built) with per-face
+// (front, rear) ray counts, Philox (seed, epoch) and emission flags: it
+// builds the chunk table (256 consecutive rays of one face per chunk), zeroes
+// the device matrix `counts` (n_faces^2 uint32) and returns the number of
+// chunks.  ffb_trace_slice enqueues the launch over chunks
+// [first, first + count) on the context stream; the slices of a prepared
+// trace may come in any split, and once every chunk has been traced exactly
+// once `counts` equals what ffb_form_factor_counts gives for the same
+// arguments (integer sums do not depend on the order).  ffb_trace_span
+// returns the earliest block start and latest warp end of all slices since
+// the prepare, in %globaltimer nanoseconds (synchronises the stream).
+int ffb_trace_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
+                      uint32_t* counts, long long* n_chunks);
+int ffb_trace_slice(ffb_ctx* c, long long first, long long count);
+int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long* end_ns);

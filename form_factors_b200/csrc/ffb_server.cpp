@@ -1,14 +1,30 @@
 // ffb_server.cpp -- a serving loop for form-factor solves (include/ffb.h,
-// ffb_server_*): requests of different sizes are admitted by a device-memory
-// budget into a fixed number of slots, each slot a context with its own CUDA
-// stream and worker thread, so that the device work of admitted requests
-// overlaps (grid builds, zeroing, traces and result copies of different
-// requests run concurrently).  Each request's scene, grid and count matrix
-// stay resident on the device until the client releases the result.
+// ffb_server_*) with continuous batching on the device.
+//
+// Requests of different sizes are admitted in arrival order while a slot is
+// free and the device-memory budget allows.  Each slot is a context (its own
+// CUDA stream and resident scene) with a worker thread that prepares its
+// request: uploads the scene, builds the grid, allocates and zeroes the
+// count matrix and builds the chunk table.  A prepared request joins the
+// trace rotation of one scheduler thread, which launches the requests'
+// traces in slices of at most kSliceRays rays, round-robin over the
+// prepared requests, with kWindow slices in flight: the next slice is
+// queued while the current one runs, and slices of different requests run
+// on different streams, so a request admitted while others trace starts at
+// the next slice boundary and its kernels overlap theirs on the device (a
+// small request's launch shares the SMs; a large one's blocks take over SMs
+// as the previous slice's blocks retire).  Round-robin over slices is
+// processor sharing: a small request finishes within its first turn
+// instead of waiting behind a large one.  Each request's scene, grid and
+// count matrix stay resident until the client releases the result.
 //
 // A request's counts depend only on its scene, ray budget, seed and flags
-// (Philox keyed by seed, epoch 0, face, ray), never on what else runs: the
-// result is bit-identical alone and in the mix.
+// (Philox keyed by seed, epoch 0, face, ray) and are integer sums, so the
+// result is bit-identical alone and in the mix, whatever the slicing.
+//
+// The consumer this stands in for is the per-scene form-factor solve of the
+// reference's thermal model (thermal_equation/form_factors.cpp:88-98), one
+// scene after another.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -24,14 +40,21 @@
 #include <cuda_runtime.h>
 
 #include "ffb.h"
-
-int ffb_set_error(int code, const char* msg);
+#include "ffb_internal.h"
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
 
 double secs(Clock::time_point t0, Clock::time_point t1) { return std::chrono::duration<double>(t1 - t0).count(); }
+
+// Rays per trace slice: about 7 ms of trace on a B200, long against a
+// launch and its tail, short against the large requests that small ones
+// would otherwise wait behind.
+constexpr long long kSliceRays = 16ll << 20;
+constexpr long long kChunkRays = 256;  // rays per chunk of the fused kernel
+constexpr long long kSliceChunks = kSliceRays / kChunkRays;
+constexpr int kWindow = 2;  // slices in flight
 
 struct Request {
   long long id = 0;
@@ -40,16 +63,38 @@ struct Request {
   int rays_per_face = 0;
   uint64_t seed = 0;
   int flags = 0;
-  float cells_per_face = 32.f;
+  float cells_per_face = 32.f;     // 0: grid and launch shape autotuned
+  int tuned_shape = 0;
+  float tuned_cells_per_face = 0.f;
   unsigned long long reserve = 0;  // bytes reserved in the budget
   int state = FFB_REQ_QUEUED;
   int error = 0;
   std::string message;
   uint32_t* counts = nullptr;      // device, n_faces^2, until released
   int readers = 0;                 // ffb_server_result copies in progress (release waits for them)
-  int device = 0;
   Clock::time_point t_submit, t_admit, t_done;
-  double gpu_ms = 0;               // events around the request's device work
+  unsigned long long start_ns = 0, end_ns = 0;  // trace span on the device (%globaltimer)
+  int slices = 0;
+};
+
+// A slot: one context and its worker.  `phase` is guarded by the server
+// mutex: the worker prepares (kPreparing), the scheduler traces
+// (kTracing: chunks handed out up to `next`), then the worker finishes.
+enum Phase { kIdle, kPreparing, kTracing, kTraced };
+
+struct Slot {
+  ffb_ctx* ctx = nullptr;
+  std::shared_ptr<Request> req;
+  Phase phase = kIdle;
+  long long n_chunks = 0, next = 0;
+  int in_flight = 0;  // launched slices not yet retired
+  int error = 0;      // a failed slice launch
+  std::string message;
+};
+
+struct Inflight {
+  int slot;
+  cudaEvent_t done;
 };
 
 }  // namespace
@@ -60,39 +105,40 @@ struct ffb_server {
   unsigned long long reserved = 0;
   int n_slots = 0;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_sched, cv_slot;
   std::deque<std::shared_ptr<Request>> queue;
   std::map<long long, std::shared_ptr<Request>> all;
   long long next_id = 1;
   bool stopping = false;
+  std::vector<Slot> slots;
   std::vector<std::thread> workers;
+  std::thread scheduler;
   int running = 0;
   int peak_running = 0;
-  // Held around each request's trace: the fused kernel fills the whole GPU,
-  // so two traces at once only share it (and mix their grids in L2); the
-  // other slots meanwhile upload scenes and build grids.
-  std::mutex trace_mu;
+  int peak_tracing = 0;  // most requests in the trace rotation at once
 };
 
 namespace {
 
 // Device bytes a request may hold: its count matrix plus a generous bound on
-// the scene, records, grid and per-reference copies of a 32-cells-per-face
-// grid (about 1.3 KB per face).
-unsigned long long estimate_bytes(int n_faces)
+// the scene, records, grid and per-reference copies: about 1.3 KB per face
+// for a grid of cells_per_face 32, and 10 KB per face for an autotuned one
+// (its grid candidates go up to 256 cells per face).
+unsigned long long estimate_bytes(int n_faces, bool tuned)
 {
   const unsigned long long n = (unsigned long long)n_faces;
-  return 4ull * n * n + 1536ull * n + (8ull << 20);
+  return 4ull * n * n + (tuned ? 10240ull : 1536ull) * n + (8ull << 20);
 }
 
-int run_request(ffb_server* s, ffb_ctx* ctx, cudaStream_t stream, Request& r)
+// The worker's part of a request before its trace: scene, grid, matrix,
+// chunk table.
+int prepare(Slot& sl, Request& r, long long* n_chunks)
 {
+  ffb_ctx* ctx = sl.ctx;
   int rc = ffb_scene_set(ctx, r.faces.data(), r.n_faces);
-  ffb_grid_params gp = {0, 0, 0, r.cells_per_face, 1};
-  if (rc >= 0)
-    rc = ffb_grid_build(ctx, &gp);
   if (rc < 0)
     return rc;
+  cudaStream_t stream = (cudaStream_t)ffb_ctx_stream(ctx);
   const size_t mat = (size_t)r.n_faces * r.n_faces;
   cudaError_t e = cudaMallocAsync((void**)&r.counts, sizeof(uint32_t) * mat, stream);
   if (e != cudaSuccess) {
@@ -101,10 +147,22 @@ int run_request(ffb_server* s, ffb_ctx* ctx, cudaStream_t stream, Request& r)
     return ffb_set_error(FFB_ERR_NO_MEMORY, "request matrix allocation failed");
   }
   std::vector<int32_t> front((size_t)r.n_faces, r.rays_per_face), rear((size_t)r.n_faces, 0);
-  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess)  // preparation done before taking the GPU
-    return ffb_set_error(FFB_ERR_CUDA, cudaGetErrorString(e));
-  std::lock_guard<std::mutex> trace(s->trace_mu);
-  rc = ffb_form_factor_counts(ctx, front.data(), rear.data(), r.seed, 0, r.flags, nullptr, r.n_faces, r.counts);
+  if (r.cells_per_face > 0) {
+    ffb_grid_params gp = {0, 0, 0, r.cells_per_face, 1};
+    rc = ffb_ctx_set_trace_shape(ctx, 0);
+    if (rc >= 0)
+      rc = ffb_grid_build(ctx, &gp);
+  } else {
+    // grid and launch shape from the tuning cache (a tuning run on a miss,
+    // with the request's own matrix as the sample's scratch)
+    ffb_tune_result tr{};
+    rc = ffb_autotune(ctx, front.data(), rear.data(), r.seed, nullptr, 0, 0, 0, r.counts, &tr);
+    r.tuned_shape = tr.shape;
+    r.tuned_cells_per_face = tr.grid.cells_per_face;
+  }
+  if (rc < 0)
+    return rc;
+  rc = ffb_trace_prepare(ctx, front.data(), rear.data(), r.seed, 0, r.flags, r.counts, n_chunks);
   if (rc < 0)
     return rc;
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess)
@@ -112,18 +170,38 @@ int run_request(ffb_server* s, ffb_ctx* ctx, cudaStream_t stream, Request& r)
   return FFB_OK;
 }
 
+void finish(ffb_server* s, Slot& sl, const std::shared_ptr<Request>& r, int err, const std::string& msg)
+{
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->t_done = Clock::now();
+    --s->running;
+    r->faces.clear();
+    r->faces.shrink_to_fit();
+    if (err < 0) {
+      r->state = FFB_REQ_FAILED;
+      r->error = err;
+      r->message = msg;
+      if (r->counts) {
+        cudaFree(r->counts);
+        r->counts = nullptr;
+      }
+      s->reserved -= r->reserve;
+      r->reserve = 0;
+    } else {
+      r->state = FFB_REQ_DONE;
+    }
+    sl.req.reset();
+    sl.phase = kIdle;
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();
+}
+
 void worker_main(ffb_server* s, int slot)
 {
   cudaSetDevice(s->device);
-  ffb_ctx* ctx = nullptr;
-  int rc = ffb_ctx_create(s->device, &ctx);
-  if (ctx)
-    ffb_ctx_set_stats(ctx, 0);  // requests return counts only
-  cudaStream_t stream = ctx ? (cudaStream_t)ffb_ctx_stream(ctx) : nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  (void)slot;
+  Slot& sl = s->slots[(size_t)slot];
   for (;;) {
     std::shared_ptr<Request> r;
     {
@@ -144,44 +222,123 @@ void worker_main(ffb_server* s, int slot)
       r->t_admit = Clock::now();
       ++s->running;
       s->peak_running = std::max(s->peak_running, s->running);
+      sl.req = r;
+      sl.phase = kPreparing;
     }
-    int err = rc;
-    if (err >= 0) {
-      cudaEventRecord(e0, stream);
-      err = run_request(s, ctx, stream, *r);
-      cudaEventRecord(e1, stream);
-      cudaEventSynchronize(e1);
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      r->gpu_ms = ms;
-    }
+    long long n_chunks = 0;
+    int err = prepare(sl, *r, &n_chunks);
     std::string msg = err < 0 ? ffb_last_error() : "";
+    if (err >= 0 && n_chunks > 0) {
+      // hand the trace to the scheduler and wait for its last slice
+      std::unique_lock<std::mutex> lock(s->mu);
+      sl.n_chunks = n_chunks;
+      sl.next = 0;
+      sl.in_flight = 0;
+      sl.error = 0;
+      sl.phase = kTracing;
+      int tracing = 0;
+      for (const Slot& o : s->slots)
+        tracing += o.phase == kTracing;
+      s->peak_tracing = std::max(s->peak_tracing, tracing);
+      s->cv_sched.notify_all();
+      s->cv_slot.wait(lock, [&] { return sl.phase == kTraced; });
+      err = sl.error;
+      msg = sl.message;
+    }
+    if (err >= 0) {
+      unsigned long long t0 = 0, t1 = 0;
+      err = ffb_trace_span(sl.ctx, &t0, &t1);
+      r->start_ns = t0;
+      r->end_ns = t1;
+      if (err < 0)
+        msg = ffb_last_error();
+    }
+    finish(s, sl, r, err, msg);
+  }
+}
+
+// Launches slices round-robin over the slots in kTracing, keeping kWindow
+// in flight, and retires them in launch order.  A slot leaves the rotation
+// (kTraced) when its last slice has retired.
+void scheduler_main(ffb_server* s)
+{
+  cudaSetDevice(s->device);
+  std::vector<cudaEvent_t> pool;
+  for (int k = 0; k < kWindow; ++k) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync);
+    pool.push_back(e);
+  }
+  std::deque<Inflight> inflight;
+  size_t rr = 0;
+  for (;;) {
     {
-      std::lock_guard<std::mutex> lock(s->mu);
-      r->t_done = Clock::now();
-      --s->running;
-      r->faces.clear();
-      r->faces.shrink_to_fit();
-      if (err < 0) {
-        r->state = FFB_REQ_FAILED;
-        r->error = err;
-        r->message = msg;
-        if (r->counts) {
-          cudaFree(r->counts);
-          r->counts = nullptr;
+      std::unique_lock<std::mutex> lock(s->mu);
+      // fill the window: the next slot in round-robin order with chunks left
+      while ((int)inflight.size() < kWindow) {
+        int pick = -1;
+        for (size_t k = 0; k < s->slots.size(); ++k) {
+          const size_t i = (rr + k) % s->slots.size();
+          const Slot& sl = s->slots[i];
+          if (sl.phase == kTracing && sl.error == 0 && sl.next < sl.n_chunks) {
+            pick = (int)i;
+            break;
+          }
         }
-        s->reserved -= r->reserve;
-        r->reserve = 0;
-      } else {
-        r->state = FFB_REQ_DONE;
+        if (pick < 0)
+          break;
+        rr = (size_t)pick + 1;
+        Slot& sl = s->slots[(size_t)pick];
+        const long long first = sl.next, count = std::min(kSliceChunks, sl.n_chunks - sl.next);
+        sl.next += count;
+        int rc = ffb_trace_slice(sl.ctx, first, count);
+        cudaEvent_t ev = pool.back();
+        if (rc >= 0 && cudaEventRecord(ev, (cudaStream_t)ffb_ctx_stream(sl.ctx)) != cudaSuccess) {
+          cudaGetLastError();
+          rc = ffb_set_error(FFB_ERR_CUDA, "event record after a trace slice failed");
+        }
+        if (rc < 0) {
+          sl.error = rc;
+          sl.message = ffb_last_error();
+          sl.next = sl.n_chunks;  // no more slices for this request
+          if (sl.in_flight == 0) {
+            sl.phase = kTraced;
+            s->cv_slot.notify_all();
+          }
+          continue;
+        }
+        pool.pop_back();
+        ++sl.in_flight;
+        ++sl.req->slices;
+        inflight.push_back(Inflight{pick, ev});
+      }
+      if (inflight.empty()) {
+        if (s->stopping)
+          break;
+        s->cv_sched.wait(lock);
+        continue;
       }
     }
-    s->cv_done.notify_all();
-    s->cv_work.notify_all();
+    // retire the oldest slice (no lock held while the device runs)
+    Inflight f = inflight.front();
+    inflight.pop_front();
+    cudaError_t e = cudaEventSynchronize(f.done);
+    pool.push_back(f.done);
+    std::lock_guard<std::mutex> lock(s->mu);
+    Slot& sl = s->slots[(size_t)f.slot];
+    --sl.in_flight;
+    if (e != cudaSuccess && sl.error == 0) {
+      sl.error = ffb_set_error(FFB_ERR_CUDA, cudaGetErrorString(e));
+      sl.message = cudaGetErrorString(e);
+      sl.next = sl.n_chunks;
+    }
+    if (sl.next >= sl.n_chunks && sl.in_flight == 0) {
+      sl.phase = kTraced;
+      s->cv_slot.notify_all();
+    }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  ffb_ctx_destroy(ctx);
+  for (cudaEvent_t e : pool)
+    cudaEventDestroy(e);
 }
 
 }  // namespace
@@ -190,6 +347,7 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
 {
   if (!out || n_slots <= 0 || n_slots > 64)
     return ffb_set_error(FFB_ERR_ARG, "ffb_server_create: bad arguments (1..64 slots)");
+  *out = nullptr;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
     cudaGetLastError();
@@ -199,6 +357,18 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
   s->device = device;
   s->budget = budget_bytes;
   s->n_slots = n_slots;
+  s->slots.resize((size_t)n_slots);
+  for (Slot& sl : s->slots) {
+    int rc = ffb_ctx_create(device, &sl.ctx);
+    if (rc < 0) {
+      for (Slot& o : s->slots)
+        ffb_ctx_destroy(o.ctx);
+      delete s;
+      return rc;
+    }
+    ffb_ctx_set_stats(sl.ctx, 0);  // requests return counts only
+  }
+  s->scheduler = std::thread(scheduler_main, s);
   for (int i = 0; i < n_slots; ++i)
     s->workers.emplace_back(worker_main, s, i);
   *out = s;
@@ -213,20 +383,28 @@ extern "C" void ffb_server_destroy(ffb_server* s)
     std::lock_guard<std::mutex> lock(s->mu);
     s->stopping = true;
   }
+  // workers stop between requests: a request being traced finishes first
   s->cv_work.notify_all();
   for (auto& t : s->workers)
     t.join();
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->cv_sched.notify_all();
+  }
+  s->scheduler.join();
   cudaSetDevice(s->device);
   for (auto& kv : s->all)
     if (kv.second->counts)
       cudaFree(kv.second->counts);
+  for (Slot& sl : s->slots)
+    ffb_ctx_destroy(sl.ctx);
   delete s;
 }
 
 extern "C" int ffb_server_submit(ffb_server* s, const float* faces9, int n_faces, int rays_per_face, uint64_t seed,
                                  int flags, float cells_per_face, long long* request_id)
 {
-  if (!s || !faces9 || n_faces <= 0 || rays_per_face < 0 || !request_id)
+  if (!s || !faces9 || n_faces <= 0 || rays_per_face < 0 || !request_id || !(cells_per_face >= 0.f))
     return ffb_set_error(FFB_ERR_ARG, "ffb_server_submit: bad arguments");
   if (n_faces > 65535)
     return ffb_set_error(FFB_ERR_TOO_LARGE, "ffb_server_submit: more than 65535 faces");
@@ -236,9 +414,8 @@ extern "C" int ffb_server_submit(ffb_server* s, const float* faces9, int n_faces
   r->rays_per_face = rays_per_face;
   r->seed = seed;
   r->flags = flags;
-  r->cells_per_face = cells_per_face > 0 ? cells_per_face : 32.f;
-  r->reserve = estimate_bytes(n_faces);
-  r->device = s->device;
+  r->cells_per_face = cells_per_face > 0 ? cells_per_face : 0.f;
+  r->reserve = estimate_bytes(n_faces, r->cells_per_face == 0.f);
   r->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -274,7 +451,12 @@ extern "C" int ffb_server_wait(ffb_server* s, long long id, double timeout_s, ff
     info->n_faces = r->n_faces;
     info->queue_s = r->state >= FFB_REQ_RUNNING ? secs(r->t_submit, r->t_admit) : secs(r->t_submit, Clock::now());
     info->latency_s = done() ? secs(r->t_submit, r->t_done) : 0.0;
-    info->gpu_ms = r->gpu_ms;
+    info->gpu_ms = r->end_ns > r->start_ns ? 1e-6 * (double)(r->end_ns - r->start_ns) : 0.0;
+    info->trace_start_ns = r->start_ns;
+    info->trace_end_ns = r->end_ns;
+    info->slices = r->slices;
+    info->shape = r->tuned_shape;
+    info->cells_per_face = r->cells_per_face > 0 ? r->cells_per_face : r->tuned_cells_per_face;
   }
   if (r->state == FFB_REQ_FAILED)
     return ffb_set_error(r->error, r->message.c_str());
@@ -283,6 +465,8 @@ extern "C" int ffb_server_wait(ffb_server* s, long long id, double timeout_s, ff
 
 extern "C" int ffb_server_result(ffb_server* s, long long id, uint32_t* counts)
 {
+  if (!s || !counts)
+    return ffb_set_error(FFB_ERR_ARG, "null argument");
   std::shared_ptr<Request> r;
   {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -307,6 +491,8 @@ extern "C" int ffb_server_result(ffb_server* s, long long id, uint32_t* counts)
 
 extern "C" int ffb_server_release(ffb_server* s, long long id)
 {
+  if (!s)
+    return ffb_set_error(FFB_ERR_ARG, "null server");
   std::shared_ptr<Request> r;
   {
     std::unique_lock<std::mutex> lock(s->mu);
@@ -345,5 +531,6 @@ extern "C" int ffb_server_stats(ffb_server* s, ffb_server_info* out)
   out->peak_running = s->peak_running;
   out->reserved_bytes = s->reserved;
   out->budget_bytes = s->budget;
+  out->peak_tracing = s->peak_tracing;
   return FFB_OK;
 }

@@ -8,13 +8,12 @@
 namespace ffb {
 
 // A unit of work of the fused kernel: `count` consecutive rays [j0, j0+count)
-// of face `face` (index within its scene) of scene `scene`.  Rays j < front
-// leave the front side, the others the rear.
+// of face `face` (index within its scene).  Rays j < front leave the front
+// side, the others the rear.
 struct Chunk {
   int32_t face;
   int32_t j0;
-  int16_t count;
-  int16_t scene;  // scene of a batched work list (informational: each scene has its own launch)
+  int32_t count;
   int32_t front;
 };
 
@@ -30,7 +29,7 @@ __global__ void k_chunk_fill(const int4* __restrict__ src, int n, Chunk* __restr
     const int4 f = src[i];
     const int nc = (f.z + kRays - 1) / kRays;
     for (int j = lane; j < nc; j += 32)
-      chunks[(uint32_t)f.w + (uint32_t)j] = Chunk{f.x, j * kRays, (int16_t)min(kRays, f.z - j * kRays), 0, f.y};
+      chunks[(uint32_t)f.w + (uint32_t)j] = Chunk{f.x, j * kRays, min(kRays, f.z - j * kRays), f.y};
   }
 }
 
@@ -64,8 +63,19 @@ struct TraceParams {
   // scene's face_to_row of the hit face)
   const unsigned long long* __restrict__ power;
   unsigned long long* __restrict__ absorb;
+  // when set: [0] gets the earliest block start and [1] the latest warp end
+  // of the launch, in %globaltimer nanoseconds (atomicMin / atomicMax, so
+  // several launches may share one pair)
+  unsigned long long* __restrict__ span;
   SceneSlot scene;
 };
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 constexpr int kTraceThreads = 128;
 constexpr int kWarpsPerBlock = kTraceThreads / 32;
@@ -141,22 +151,17 @@ __device__ __forceinline__ void warp_hash_flush(uint32_t* keys, uint32_t* vals, 
 // keeps a current chunk (consecutive rays of one face) and hands its rays to
 // lanes as they fall idle (one ballot per refill, one global atomic per
 // chunk), so a warp may hold rays of several faces at once.  Idle lanes are
-// refilled together once at least kRefillMin of them wait (or the whole warp
-// is idle): emission and ray setup then run with several lanes at once
-// instead of one lane at a time.  Each iteration a lane whose cell is
-// exhausted moves on (stop, DDA step or empty-space jump; up to
-// FFB_ADV_PER_ITER moves while it lands in empty cells) and then tests up to
-// FFB_TEST_PER_ITER references of its cell.  Doing both kinds of work in one
+// refilled together once at least the shape's `refill` of them wait (or the
+// whole warp is idle): emission and ray setup then run with several lanes at
+// once instead of one lane at a time.  Each iteration a lane whose cell is
+// exhausted moves on (stop, DDA step or empty-space jump; up to the shape's
+// `adv` moves while it lands in empty cells) and then tests up to its `test`
+// references of its cell.  Doing both kinds of work in one
 // iteration keeps lanes of a warp in the same code more of the time than
 // one kind per iteration does.  A finished hit adds one to the
 // warp's shared-memory hash histogram keyed by the matrix index
 // row(f) * n_cols + row(h); the warp flushes the table to the global uint32
-// matrix with atomic adds when it is half full, when it changes scene and at
-// the end.
-//
-// With several scenes in one launch a warp works on one scene at a time: a
-// chunk of another scene is taken only once every lane is idle (drain before
-// switch), so that the scene's grid is warp-uniform.
+// matrix with atomic adds when it is half full and at the end.
 //
 // kPower (the radiance equation, thermal_equation/radiance_cpu.cpp:142-180)
 // replaces the matrix: a hit adds the per-ray power of the ray's (source
@@ -180,11 +185,37 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 #define FFB_TEST_PER_ITER 2
 #endif
 
-template <bool kSkip, bool kStats, bool kHash, bool kPower = false>
-__global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(const __grid_constant__ TraceParams p)
+// Launch shapes of the fused kernel, the choices of the autotuner
+// (ffb_autotune): cell advances and triangle tests a lane may do per
+// iteration, the idle lanes a warp waits for before it refills them, and the
+// resident blocks of 128 threads per SM the kernel is compiled for (which
+// caps its registers at 65536 / (128 * blocks)).  Shape 0 is the default.
+// The shape changes only the order in which lanes do their work, never a
+// ray's result or the counts.
+struct TraceShape {
+  int adv, test, refill, blocks;
+};
+constexpr int kNumShapes = 7;
+__host__ __device__ constexpr TraceShape trace_shape(int v)
 {
+  return v == 1 ? TraceShape{1, 1, 4, 8}
+       : v == 2 ? TraceShape{2, 1, 6, 8}
+       : v == 3 ? TraceShape{1, 2, 6, 8}
+       : v == 4 ? TraceShape{3, 3, 6, 8}
+       : v == 5 ? TraceShape{2, 2, 10, 8}
+       : v == 6 ? TraceShape{2, 2, 6, 6}
+                : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS};
+}
+
+template <bool kSkip, bool kStats, bool kHash, bool kPower = false, int kShape = 0>
+__global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
+    k_form_factors(const __grid_constant__ TraceParams p)
+{
+  constexpr TraceShape kS = trace_shape(kShape);
   extern __shared__ uint32_t s_hash[];  // kWarpsPerBlock x (keys, values) when kHash
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (p.span && threadIdx.x == 0)
+    atomicMin(p.span, global_ns());
   uint32_t* keys = s_hash + warp * 2 * kWarpHash;
   uint32_t* vals = keys + kWarpHash;
   if (kHash) {
@@ -214,7 +245,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
   uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0, n_jumps = 0;
   for (;;) {
     unsigned need = __ballot_sync(kFull, !active);
-    if (__popc(need) < kRefillMin && need != kFull)
+    if (__popc(need) < kS.refill && need != kFull)
       need = 0;
     while (need && !exhausted) {
       if (c_left == 0) {
@@ -254,7 +285,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     if (active) {
       bool live = true;
 #pragma unroll
-      for (int k = 0; k < FFB_ADV_PER_ITER; ++k)
+      for (int k = 0; k < kS.adv; ++k)
         if (live && T.i >= T.en)
           live = tracer_advance<kSkip>(T, S.g, n_cells, n_jumps);
       if (!live) {
@@ -262,7 +293,7 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
         hit = tracer_result(T, S.g);
       } else {
 #pragma unroll
-        for (int k = 0; k < FFB_TEST_PER_ITER; ++k)
+        for (int k = 0; k < kS.test; ++k)
           if (T.i < T.en)
             tracer_test(T, S.g, n_tests);
       }
@@ -293,6 +324,8 @@ __global__ void __launch_bounds__(kTraceThreads, FFB_MIN_BLOCKS) k_form_factors(
     warp_hash_flush(keys, vals, S.counts, lane);
   if (kStats)
     warp_stats(p.stats, n_tests, n_cells, n_rays, n_hits, n_jumps);
+  if (p.span && lane == 0)
+    atomicMax(p.span + 1, global_ns());
 }
 
 // ---------------------------------------------------------------------------

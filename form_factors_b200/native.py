@@ -96,14 +96,26 @@ def bounding_sphere(faces):
     return np.array(list(c), np.float32), np.float32(r.value)
 
 
+class TraceShape(C.Structure):
+    _fields_ = [("adv_per_iter", C.c_int), ("test_per_iter", C.c_int), ("refill_min", C.c_int),
+                ("blocks_per_sm", C.c_int)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("grid", GridParams), ("shape", C.c_int), ("sample_ms", C.c_float), ("from_cache", C.c_int),
+                ("timed", C.c_int), ("sample_rays", C.c_longlong)]
+
+
 class RequestInfo(C.Structure):
     _fields_ = [("state", C.c_int), ("error", C.c_int), ("n_faces", C.c_int), ("queue_s", C.c_double),
-                ("latency_s", C.c_double), ("gpu_ms", C.c_double)]
+                ("latency_s", C.c_double), ("gpu_ms", C.c_double), ("trace_start_ns", C.c_ulonglong),
+                ("trace_end_ns", C.c_ulonglong), ("slices", C.c_int), ("shape", C.c_int),
+                ("cells_per_face", C.c_float)]
 
 
 class ServerInfo(C.Structure):
     _fields_ = [("queued", C.c_int), ("running", C.c_int), ("peak_running", C.c_int),
-                ("reserved_bytes", C.c_ulonglong), ("budget_bytes", C.c_ulonglong)]
+                ("reserved_bytes", C.c_ulonglong), ("budget_bytes", C.c_ulonglong), ("peak_tracing", C.c_int)]
 
 
 _lib = None
@@ -163,6 +175,12 @@ def load(path=LIB_PATH):
         "ffb_form_factors": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, vp, vp]),
         "ffb_form_factor_counts_rows": (i32, [vp, vp, vp, u64, u32, i32, vp, i32, i32, i32, vp]),
         "ffb_autotune_grid": (i32, [vp, vp, vp, u64, vp, i32, i32, C.POINTER(GridParams), C.POINTER(C.c_float)]),
+        "ffb_trace_shape_count": (i32, []),
+        "ffb_trace_shape_get": (i32, [i32, C.POINTER(TraceShape)]),
+        "ffb_ctx_set_trace_shape": (i32, [vp, i32]),
+        "ffb_ctx_trace_shape": (i32, [vp]),
+        "ffb_autotune": (i32, [vp, vp, vp, u64, vp, i32, i32, i32, vp, C.POINTER(TuneResult)]),
+        "ffb_batch_autotune": (i32, [vp, vp, vp, vp]),
         "ffb_batch_set": (i32, [vp, i32, vp, vp, vp]),
         "ffb_batch_grid_info": (i32, [vp, i32, C.POINTER(GridInfo)]),
         "ffb_batch_prepare": (i32, [vp, vp, vp, vp, i32]),
@@ -200,6 +218,24 @@ def _check(code):
     if code < 0:
         raise FFBError(code, load().ffb_last_error().decode(errors="replace"))
     return code
+
+
+def trace_shapes():
+    """The fused kernel's launch shapes (the autotuner's kernel choices)."""
+    lib = load()
+    out = []
+    for v in range(lib.ffb_trace_shape_count()):
+        t = TraceShape()
+        _check(lib.ffb_trace_shape_get(v, C.byref(t)))
+        out.append(dict(adv_per_iter=t.adv_per_iter, test_per_iter=t.test_per_iter, refill_min=t.refill_min,
+                        blocks_per_sm=t.blocks_per_sm))
+    return out
+
+
+def _tune_dict(r):
+    return dict(dims=(r.grid.nx, r.grid.ny, r.grid.nz), cells_per_face=r.grid.cells_per_face,
+                skip_empty=bool(r.grid.skip_empty), shape=r.shape, sample_ms=r.sample_ms,
+                from_cache=bool(r.from_cache), timed=r.timed, sample_rays=r.sample_rays)
 
 
 def cast_bruteforce_static(faces, rays, hit, points=None, stream=None):
@@ -301,6 +337,34 @@ class Context:
                                            len(candidates), int(sample_every), C.byref(best), C.byref(ms)))
         return dict(dims=(best.nx, best.ny, best.nz), cells_per_face=best.cells_per_face,
                     skip_empty=bool(best.skip_empty), sample_ms=ms.value)
+
+    def autotune(self, front, rear, seed=1, candidates=None, sample_every=0, force=False, scratch=None):
+        """ffb_autotune: chooses the grid (candidates: dicts with dims /
+        cells_per_face / skip_empty, None for the library's set) and the
+        kernel's launch shape on a sample of the ray budget; builds the grid
+        and sets the shape.  Cached per process by scene and budget class."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        arr = None
+        if candidates is not None:
+            arr = (GridParams * len(candidates))()
+            for i, cand in enumerate(candidates):
+                arr[i] = GridParams(0, 0, 0, float(cand.get("cells_per_face", 32.0)),
+                                    int(cand.get("skip_empty", True)))
+                if cand.get("dims"):
+                    arr[i].nx, arr[i].ny, arr[i].nz = cand["dims"]
+        res = TuneResult()
+        _check(self._lib.ffb_autotune(self._h, _ptr(front), _ptr(rear), int(seed),
+                                      C.cast(arr, C.c_void_p) if arr is not None else None,
+                                      len(candidates) if candidates is not None else 0, int(sample_every),
+                                      1 if force else 0, _ptr(scratch), C.byref(res)))
+        return _tune_dict(res)
+
+    def set_trace_shape(self, shape):
+        _check(self._lib.ffb_ctx_set_trace_shape(self._h, int(shape)))
+
+    def trace_shape(self):
+        return _check(self._lib.ffb_ctx_trace_shape(self._h))
 
     def grid_info(self):
         info = GridInfo()
@@ -566,6 +630,15 @@ class Context:
         if seeds is not None:
             seeds = np.ascontiguousarray(seeds, np.uint64)
         _check(self._lib.ffb_batch_prepare(self._h, _ptr(front), _ptr(rear), _ptr(seeds), int(flags)))
+
+    def batch_autotune(self, front, rear):
+        """ffb_batch_autotune: each scene's grid and launch shape from the
+        tuning cache, tuning the scenes it has no choice for."""
+        front = np.ascontiguousarray(front, np.int32)
+        rear = np.ascontiguousarray(rear, np.int32)
+        shapes = np.zeros(len(self.batch_sizes), np.int32)
+        _check(self._lib.ffb_batch_autotune(self._h, _ptr(front), _ptr(rear), _ptr(shapes)))
+        return shapes
 
     def batch_counts_layout(self):
         """(offsets, words): where each scene's N x N matrix starts in one buffer."""

@@ -1,10 +1,14 @@
 """Row sharding of the form-factor matrix across ranks (one process per GPU).
 
-Source rows are independent: rank r traces only the rays of the faces whose
-row falls in its contiguous block and owns those rows of the matrix; nothing
-is exchanged while tracing.  Blocks are balanced by the rays they emit.  When
-a rank needs the whole matrix, `gather_rows` assembles the blocks with one
+Source rows are independent (the per-source-face loop of
+cpuFactorsCalculator/cpu_system.cpp:167-196 splits by source without any
+exchange): rank r traces only the rays of the faces whose row falls in its
+contiguous block and owns those rows of the matrix; nothing is exchanged
+while tracing.  Blocks are balanced by the rays they emit.  When a rank
+needs the whole matrix, `gather_rows` assembles the blocks with one
 all_gather of padded row blocks (NCCL between GPUs, gloo on CPU).
+`solve_rows` is the per-rank step of a sharded solve; on a GPU rank its
+rows function is Context.form_factor_counts_rows.
 """
 import numpy as np
 
@@ -60,3 +64,22 @@ def gather_rows(block, begin, end, n_rows, group=None):
         b, e = int(m[0]), int(m[1])
         full[b:e] = part[: e - b]
     return full
+
+
+def rank_rows(front, rear, rank, world, face_to_row=None, n_rows=None):
+    """This rank's [begin, end) block of source rows, balanced by rays."""
+    return row_ranges(rays_per_row(front, rear, face_to_row, n_rows), world)[rank]
+
+
+def solve_rows(rows_fn, front, rear, rank, world, n_rows, face_to_row=None, gather=False, group=None):
+    """The per-rank step of a row-sharded solve.  rows_fn(begin, end) returns
+    the (end - begin, n_rows) count block of this rank's source rows (on a GPU
+    rank: Context.form_factor_counts_rows into a device tensor); no data
+    moves between ranks while it runs.  With gather=True every rank then
+    receives the full matrix through one all_gather.  Returns
+    ((begin, end), block or full matrix)."""
+    begin, end = rank_rows(front, rear, rank, world, face_to_row, n_rows)
+    block = rows_fn(begin, end)
+    if not gather:
+        return (begin, end), block
+    return (begin, end), gather_rows(block, begin, end, n_rows, group)

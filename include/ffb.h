@@ -195,16 +195,26 @@ int ffb_batch_prepare(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, c
 int ffb_batch_launch(ffb_ctx* ctx, uint32_t* counts, const unsigned long long* counts_offsets,
                      unsigned long long counts_words, int advance_epoch);
 
-/* Serving: form-factor solves submitted as requests of different sizes
- * (BASELINE config "served"), admitted in arrival order into `n_slots`
- * concurrent slots while the device-memory budget allows (0 = no budget); a
- * finished result keeps its reservation until released.  Each slot is a context with
- * its own stream and worker thread so that admitted requests overlap on the
- * device.  A request is a scene (host faces9, copied at submit),
- * rays_per_face front-side rays per face, a Philox seed and emission flags;
- * its per-face N x N uint32 counts stay resident on the device until
+/* Serving: form-factor solves submitted as requests of different sizes,
+ * admitted in arrival order into `n_slots` slots while the device-memory
+ * budget allows (0 = no budget); a finished result keeps its reservation
+ * until released.  Each slot is a context (own stream, resident scene) whose
+ * worker thread prepares its request -- scene upload, grid build, zeroed
+ * count matrix, chunk table -- while other requests trace.  One scheduler
+ * thread then traces the prepared requests in slices of at most 16 Mi rays,
+ * round-robin over them, with two slices in flight on the requests' own
+ * streams: a request admitted while others are on the GPU joins at the next
+ * slice boundary, its kernels overlap theirs on the device, and a small
+ * request finishes within its first turn instead of queueing behind a large
+ * one (processor sharing).  A request is a scene (host faces9, copied at
+ * submit), rays_per_face front-side rays per face, a Philox seed, emission
+ * flags and a grid target cells_per_face (0: grid and launch shape chosen by
+ * ffb_autotune, through its process-wide cache; the budget then reserves
+ * room for its largest grid); its per-face N x N uint32 counts stay resident
+ * on the device until
  * ffb_server_release.  The result of a request does not depend on the other
- * requests in flight. */
+ * requests in flight or on the slicing: it equals ffb_form_factor_counts on
+ * the same scene with epoch 0. */
 #define FFB_REQ_QUEUED 0
 #define FFB_REQ_RUNNING 1
 #define FFB_REQ_DONE 2
@@ -218,12 +228,18 @@ typedef struct {
   int n_faces;
   double queue_s;    /* submit -> admission */
   double latency_s;  /* submit -> result resident */
-  double gpu_ms;     /* time on the slot stream from the request's first to its last device operation (includes waiting for another request's trace) */
+  double gpu_ms;     /* trace_end_ns - trace_start_ns, in ms */
+  unsigned long long trace_start_ns; /* %globaltimer at the first block start of the request's first trace slice */
+  unsigned long long trace_end_ns;   /* %globaltimer at the last warp end of its last trace slice */
+  int slices;        /* trace launches the request took */
+  int shape;         /* launch shape of its trace */
+  float cells_per_face; /* grid target of its trace (the autotuner's choice when submitted with 0) */
 } ffb_request_info;
 
 typedef struct {
   int queued, running, peak_running;
   unsigned long long reserved_bytes, budget_bytes;
+  int peak_tracing;  /* most requests in the trace rotation at once */
 } ffb_server_info;
 
 int ffb_server_create(int device, unsigned long long budget_bytes, int n_slots, ffb_server** out);
@@ -378,6 +394,59 @@ int ffb_csv_export_counts(ffb_ctx* ctx, const char* filename, const uint32_t* co
 int ffb_autotune_grid(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed,
                       const ffb_grid_params* candidates, int n_candidates, int sample_every, ffb_grid_params* best,
                       float* best_ms);
+
+/* Launch shapes of the fused kernel: the kernel-side choices of the
+ * autotuner.  A shape changes only the order in which a warp's lanes do their
+ * work, never a ray's result or the counts. */
+typedef struct {
+  int adv_per_iter;   /* cell advances a lane may make per loop iteration */
+  int test_per_iter;  /* triangle tests a lane may make per loop iteration */
+  int refill_min;     /* idle lanes a warp waits for before it refills them */
+  int blocks_per_sm;  /* resident 128-thread blocks per SM the kernel is built for */
+} ffb_trace_shape;
+
+int ffb_trace_shape_count(void);
+int ffb_trace_shape_get(int shape, ffb_trace_shape* out);
+/* Launch shape of the context's form-factor traces (default 0). */
+int ffb_ctx_set_trace_shape(ffb_ctx* ctx, int shape);
+int ffb_ctx_trace_shape(ffb_ctx* ctx);
+
+typedef struct {
+  ffb_grid_params grid;  /* the chosen grid */
+  int shape;             /* the chosen launch shape */
+  float sample_ms;       /* its kernel time on the sample (0 when cached) */
+  int from_cache;        /* 1: taken from the process-wide cache, not timed */
+  int timed;             /* candidate runs timed */
+  long long sample_rays; /* rays of the timing sample */
+} ffb_tune_result;
+
+#define FFB_TUNE_FORCE 1 /* time the candidates even when the cache holds a choice */
+
+/* Autotuner of the fused form-factor trace for the context's scene and ray
+ * budget (the reference's only tuning is the grid side of
+ * math/grid.cpp:376-386 with a fixed 128-thread block,
+ * cuda_ray_caster/system.cu:61).  Times the fused kernel on a sample of the
+ * source faces (every sample_every-th face emits its rays; 0: a sample of
+ * about 4 Mi rays): each grid candidate (`candidates`, or NULL for targets of
+ * 32, 64, 128, 192 and 256 cells per face with empty-space jumps) with shape
+ * 0, then every launch shape on the fastest grid.  Builds the chosen grid and
+ * sets the context's shape.  The choice is cached per process under a key of
+ * face count (half-octave steps), scene-box aspect and rays per emitting face
+ * (octave steps); a cached choice is applied without timing unless flags has
+ * FFB_TUNE_FORCE.  scratch: a device buffer of n_faces^2 uint32 the sample
+ * traces may use (NULL: context memory).  Results never depend on the
+ * choice. */
+int ffb_autotune(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, uint64_t seed,
+                 const ffb_grid_params* candidates, int n_candidates, int sample_every, int flags,
+                 uint32_t* scratch, ffb_tune_result* out);
+
+/* The autotuner over the scenes of a batch (after ffb_batch_set, before
+ * ffb_batch_prepare): per scene, the cached choice for its key, or a tuning
+ * run on that scene (through the context's main scene, which it replaces)
+ * when the cache has none; each scene's grid is rebuilt with its choice and
+ * its launch uses its shape.  front/rear as ffb_batch_prepare.  shapes (may
+ * be NULL) gets each scene's shape. */
+int ffb_batch_autotune(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, int* shapes);
 
 /* Counters and kernel time of the last ffb_cast / ffb_form_factor_counts
  * (synchronises the stream). */

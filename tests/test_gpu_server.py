@@ -1,5 +1,7 @@
 """Serving loop (ffb_server_*): requests admitted by memory budget into
-concurrent slots; each result equals the same solve run alone."""
+concurrent slots and traced in slices, round-robin; each result equals the
+same solve run alone, and the traces of different requests interleave on the
+device."""
 import numpy as np
 import pytest
 
@@ -54,4 +56,30 @@ def test_admission_by_memory_budget():
         server.submit(big, 10, 1)
     assert e.value.code == -305
     assert server.stats().reserved_bytes == 0
+    server.close()
+
+
+def test_traces_of_requests_overlap_on_the_device(ctx):
+    """Two requests of 20 480 faces x 3000 rays (four 16 Mi-ray slices each)
+    submitted together: their traces interleave on the device -- each
+    request's span, from its first trace block's start to its last warp's end
+    (%globaltimer, stamped by the kernel itself), overlaps the other's -- and
+    each result equals the same solve run alone."""
+    faces = scenes.icosphere(5, 1.0, inward=True)
+    n = len(faces)
+    server = native.Server(0, budget_bytes=0, slots=2)
+    ids = [server.submit(faces, 3000, seed) for seed in (41, 42)]
+    infos = [server.wait(i, timeout_s=300) for i in ids]
+    assert all(inf.state == 2 for inf in infos)
+    assert all(inf.slices == 4 for inf in infos), [inf.slices for inf in infos]
+    (a0, a1), (b0, b1) = [(inf.trace_start_ns, inf.trace_end_ns) for inf in infos]
+    assert 0 < a0 < a1 and 0 < b0 < b1
+    assert max(a0, b0) < min(a1, b1), "device spans do not overlap: %s" % ([(a0, a1), (b0, b1)],)
+    assert server.stats().peak_tracing == 2
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=32)
+    for rid, seed in zip(ids, (41, 42)):
+        want = ctx.form_factor_counts(np.full(n, 3000, np.int32), np.zeros(n, np.int32), seed=seed, epoch=0)
+        assert np.array_equal(server.result(rid, n), want)
+        server.release(rid)
     server.close()

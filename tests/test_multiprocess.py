@@ -1,7 +1,8 @@
 """Row sharding across ranks (the multi-GPU path): balanced contiguous row
-blocks, and the blocks of world_size ranks gathered with torch.distributed
-(gloo, CPU processes) reproduce the full matrix.  The per-rank rows come from
-the CPU oracle here; on GPUs each rank runs ffb_form_factor_counts_rows."""
+blocks, and the per-rank step shard.solve_rows -- the same call the GPU
+ranks of bench.py make -- run on world_size gloo ranks reproduces the full
+matrix.  Its rows function is the CPU oracle here (the rows of the faces the
+rank emits); on GPUs it is Context.form_factor_counts_rows."""
 import os
 import socket
 
@@ -53,12 +54,15 @@ def _rank_main(rank, world, port, out_dir):
         n = len(faces)
         w, total = emission.two_sided_weights(faces)
         front, rear = emission.ray_counts(300 * n, w, total)
-        ranges = shard.row_ranges(shard.rays_per_row(front, rear), world)
-        b, e = ranges[rank]
-        fr = np.where((np.arange(n) >= b) & (np.arange(n) < e), front, 0).astype(np.int32)
-        re = np.where((np.arange(n) >= b) & (np.arange(n) < e), rear, 0).astype(np.int32)
-        mine = oracle.form_factor_counts(faces, fr, re, seed=4)[b:e]
-        full = shard.gather_rows(torch.from_numpy(mine.astype(np.int64)), b, e, n)
+
+        def rows_fn(b, e):
+            emit = (np.arange(n) >= b) & (np.arange(n) < e)
+            fr = np.where(emit, front, 0).astype(np.int32)
+            re = np.where(emit, rear, 0).astype(np.int32)
+            return torch.from_numpy(oracle.form_factor_counts(faces, fr, re, seed=4)[b:e].astype(np.int64))
+
+        (b, e), full = shard.solve_rows(rows_fn, front, rear, rank, world, n, gather=True)
+        assert (b, e) == shard.row_ranges(shard.rays_per_row(front, rear), world)[rank]
         if rank == 0:
             want = oracle.form_factor_counts(faces, front, rear, seed=4).astype(np.int64)
             np.save(os.path.join(out_dir, "ok.npy"), np.array([np.array_equal(full.numpy(), want)]))
