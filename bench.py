@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
     ap.add_argument("--no-thermal", action="store_true", help="skip the radiance / distant-source section")
     ap.add_argument("--no-obj", action="store_true", help="skip the OBJ-import section")
+    ap.add_argument("--grid-build-only", type=int, default=0,
+                    help="build the workload's grid this many times, print one JSON line of build times and exit "
+                         "(a small command for profiling the grid-build kernels)")
     ap.add_argument("--served-requests", type=int, default=256)
     ap.add_argument("--served-slots", type=int, default=16, help="requests prepared and traced at once")
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
@@ -744,7 +747,7 @@ def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm):
         peak = 4.0 * n_sm * float(sm_mhz) * 1e6
         return {"achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G warp instructions/s",
                 "frac": achieved / peak, "warp_inst_per_ray": ipr,
-                "note": "instructions per ray from ncu (profiles/k_form_factors_enclosure.md); peak = 4 x SMs x "
+                "note": "instructions per ray from the committed ncu capture (profiles/traffic.json); peak = 4 x SMs x "
                         "sampled SM clock"}
     except (OSError, ValueError, KeyError, TypeError):
         return None
@@ -972,8 +975,36 @@ def ours(args):
         dist.destroy_process_group()
 
 
+def grid_build_only(args):
+    """Builds the workload's grid args.grid_build_only times (192 cells per
+    face unless --cells-per-face or --grid says otherwise) and prints the
+    device time of each build: the grid-build kernels alone, for profiling."""
+    import torch
+    from form_factors_b200 import build, native
+    build.build()
+    faces, _, _ = workload(args.rays_per_face)
+    ctx = native.Context(0)
+    ctx.scene_set(faces)
+    dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
+    cpf = args.cells_per_face if args.cells_per_face > 0 else 192.0
+    times = []
+    for _ in range(args.grid_build_only):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.grid_build(dims=dims, cells_per_face=cpf, skip_empty=not args.no_skip)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    info = ctx.grid_info()
+    ctx.close()
+    print(json.dumps({"grid_build_ms": [1e3 * t for t in times], "grid": [info.nx, info.ny, info.nz],
+                      "refs": int(info.n_refs), "faces": len(faces)}))
+
+
 def main():
     args = parse()
+    if args.grid_build_only > 0:
+        grid_build_only(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     else:

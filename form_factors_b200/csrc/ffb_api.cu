@@ -67,6 +67,7 @@ struct DevBuf {
 };
 
 constexpr int kChunkRays = 256;  // rays per work chunk of the fused kernel
+static_assert(kChunkRays == kChunkRaysMax, "the coherent hand-out orders whole chunks");
 constexpr int kMaxRows = 65535;  // matrix index row * n + col stays below 0xFFFFFFFF
 constexpr int kMaxPipeBlocks = 16;  // row blocks of a pipelined host output
 
@@ -2209,7 +2210,7 @@ extern "C" int ffb_trace_shape_get(int shape, ffb_trace_shape* out)
   if (shape < 0 || shape >= kNumShapes || !out)
     return fail(FFB_ERR_ARG, "shape %d outside [0, %d)", shape, kNumShapes);
   const TraceShape t = trace_shape(shape);
-  *out = ffb_trace_shape{t.adv, t.test, t.refill, t.blocks};
+  *out = ffb_trace_shape{t.adv, t.test, t.refill, t.blocks, t.coherent};
   return FFB_OK;
 }
 

@@ -192,19 +192,86 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 // caps its registers at 65536 / (128 * blocks)).  Shape 0 is the default.
 // The shape changes only the order in which lanes do their work, never a
 // ray's result or the counts.
+// With `coherent` set, a warp hands out the rays of each chunk it takes in
+// the order of their directions (bins of an 8 x 8 Morton order on the Malley
+// disk) instead of in index order, so that lanes refilled together trace
+// rays of similar direction from the same face.
 struct TraceShape {
-  int adv, test, refill, blocks;
+  int adv, test, refill, blocks, coherent;
 };
-constexpr int kNumShapes = 7;
+constexpr int kNumShapes = 9;
 __host__ __device__ constexpr TraceShape trace_shape(int v)
 {
-  return v == 1 ? TraceShape{1, 1, 4, 8}
-       : v == 2 ? TraceShape{2, 1, 6, 8}
-       : v == 3 ? TraceShape{1, 2, 6, 8}
-       : v == 4 ? TraceShape{3, 3, 6, 8}
-       : v == 5 ? TraceShape{2, 2, 10, 8}
-       : v == 6 ? TraceShape{2, 2, 6, 6}
-                : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS};
+  return v == 1 ? TraceShape{1, 1, 4, 8, 0}
+       : v == 2 ? TraceShape{2, 1, 6, 8, 0}
+       : v == 3 ? TraceShape{1, 2, 6, 8, 0}
+       : v == 4 ? TraceShape{3, 3, 6, 8, 0}
+       : v == 5 ? TraceShape{2, 2, 10, 8, 0}
+       : v == 6 ? TraceShape{2, 2, 6, 6, 0}
+       : v == 7 ? TraceShape{2, 2, 6, 8, 1}
+       : v == 8 ? TraceShape{2, 2, 10, 8, 1}
+                : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS, 0};
+}
+
+constexpr int kChunkRaysMax = 256;  // rays per chunk (the host's chunk size)
+constexpr int kDirBins = 64;        // direction bins of the coherent hand-out
+
+// Direction bin of ray j of a face (the draws of emit_ray): the Malley disk
+// point (sqrt(r) cos phi, sqrt(r) sin phi) on an 8 x 8 grid, in Morton order.
+__device__ __forceinline__ int direction_bin(uint32_t face, uint32_t j, uint32_t key0, uint32_t key1, uint32_t epoch)
+{
+  const uint4 x = philox4x32_10(make_uint4(j, face, epoch, 0x46464231u), key0, key1);
+  const float rad = sqrtf(u01(x.z));
+  float sphi, cphi;
+  sincos_turn24(x.w >> 8, sphi, cphi);
+  const int qx = min(7, max(0, (int)((rad * cphi + 1.f) * 4.f)));
+  const int qy = min(7, max(0, (int)((rad * sphi + 1.f) * 4.f)));
+  int code = 0;
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+    code |= (((qx >> b) & 1) << (2 * b)) | (((qy >> b) & 1) << (2 * b + 1));
+  return code;
+}
+
+// Order of the chunk's rays [0, count) by direction bin (a counting sort in
+// the warp's shared memory: `cnt` kDirBins counters, `perm` the order).
+__device__ __forceinline__ void direction_order(uint32_t face, uint32_t j0, int count, uint32_t key0, uint32_t key1,
+                                                uint32_t epoch, uint32_t* cnt, uint8_t* perm, int lane)
+{
+  cnt[lane] = 0;
+  cnt[lane + 32] = 0;
+  __syncwarp();
+  uint32_t code[kChunkRaysMax / 32];
+#pragma unroll
+  for (int m = 0; m < kChunkRaysMax / 32; ++m) {
+    const int idx = m * 32 + lane;
+    code[m] = 0;
+    if (idx < count) {
+      const int bin = direction_bin(face, j0 + (uint32_t)idx, key0, key1, epoch);
+      code[m] = (uint32_t)bin | (atomicAdd(cnt + bin, 1u) << 8);
+    }
+  }
+  __syncwarp();
+  // exclusive scan of the counters, two per lane
+  const uint32_t a = cnt[2 * lane], b = cnt[2 * lane + 1];
+  uint32_t incl = a + b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o)
+      incl += y;
+  }
+  __syncwarp();
+  cnt[2 * lane] = incl - a - b;
+  cnt[2 * lane + 1] = incl - b;
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < kChunkRaysMax / 32; ++m) {
+    const int idx = m * 32 + lane;
+    if (idx < count)
+      perm[cnt[code[m] & 0xFFu] + (code[m] >> 8)] = (uint8_t)idx;
+  }
+  __syncwarp();
 }
 
 template <bool kSkip, bool kStats, bool kHash, bool kPower = false, int kShape = 0>
@@ -213,6 +280,9 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
 {
   constexpr TraceShape kS = trace_shape(kShape);
   extern __shared__ uint32_t s_hash[];  // kWarpsPerBlock x (keys, values) when kHash
+  // coherent hand-out: per warp, direction-bin counters and the chunk's ray order
+  __shared__ uint32_t s_bins[kS.coherent ? kWarpsPerBlock * kDirBins : 1];
+  __shared__ uint8_t s_perm[kS.coherent ? kWarpsPerBlock * kChunkRaysMax : 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (p.span && threadIdx.x == 0)
     atomicMin(p.span, global_ns());
@@ -228,8 +298,8 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
   const uint32_t epoch = p.epoch_ptr ? *p.epoch_ptr : p.epoch;
   const unsigned lane_below = (1u << lane) - 1u;
   int fill = 0;  // occupied slots (warp-uniform)
-  // current chunk (warp-uniform)
-  int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0;
+  // current chunk (warp-uniform); c_pos: its rays handed out so far
+  int c_face = 0, c_j = 0, c_left = 0, c_front = 0, c_row = 0, c_pos = 0;
   const SceneSlot& S = p.scene;
   uint32_t key0 = p.key0, key1 = p.key1;
   if (p.scene_keys) {
@@ -263,20 +333,25 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
         c_left = ch.count;
         c_front = ch.front;
         c_row = S.face_to_row ? __ldg(S.face_to_row + ch.face) : ch.face;
+        c_pos = 0;
+        if (kS.coherent)
+          direction_order((uint32_t)c_face, (uint32_t)c_j, c_left, key0, key1, epoch, s_bins + warp * kDirBins,
+                          s_perm + warp * kChunkRaysMax, lane);
       }
       const int take = min(__popc(need), c_left);
       const int rank = __popc(need & lane_below);
       const bool mine = ((need >> lane) & 1u) && rank < take;
       if (mine) {
+        const int j = c_j + (kS.coherent ? (int)s_perm[warp * kChunkRaysMax + c_pos + rank] : c_pos + rank);
         float3 o, e;
-        emit_ray(p.frames + 20 * ((size_t)S.face_base + c_face), (uint32_t)c_face, (uint32_t)(c_j + rank), c_front,
-                 key0, key1, epoch, o, e);
+        emit_ray(p.frames + 20 * ((size_t)S.face_base + c_face), (uint32_t)c_face, (uint32_t)j, c_front, key0, key1,
+                 epoch, o, e);
         ++n_rays;
-        my_row = kPower ? 2 * c_face + (c_j + rank >= c_front ? 1 : 0) : c_row;
+        my_row = kPower ? 2 * c_face + (j >= c_front ? 1 : 0) : c_row;
         active = tracer_begin<kSkip>(T, S.g, o, e, n_cells);
       }
       need &= ~__ballot_sync(kFull, mine);
-      c_j += take;
+      c_pos += take;
       c_left -= take;
     }
     if (exhausted && !__any_sync(kFull, active))

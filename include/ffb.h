@@ -172,7 +172,7 @@ int ffb_form_factors(ffb_ctx* ctx, const int32_t* front, const int32_t* rear, ui
                      int flags, const int32_t* face_to_row, int n_rows, const int32_t* outgoing, float* ff);
 
 /* Batched scenes: up to 4096 independent scenes, each with its own resident
- * grid and count matrix (BASELINE config "batched").  Scene s is faces [face_offsets[s], face_offsets[s+1]) of
+ * grid and count matrix (the batched workload: many scenes of uneven size).  Scene s is faces [face_offsets[s], face_offsets[s+1]) of
  * faces9 (host or device); params: one ffb_grid_params per scene, or NULL
  * (automatic).  The batch is separate from the scene of the single-scene
  * calls above, which keep working. */
@@ -403,6 +403,7 @@ typedef struct {
   int test_per_iter;  /* triangle tests a lane may make per loop iteration */
   int refill_min;     /* idle lanes a warp waits for before it refills them */
   int blocks_per_sm;  /* resident 128-thread blocks per SM the kernel is built for */
+  int coherent;       /* 1: a chunk's rays are handed out in direction order */
 } ffb_trace_shape;
 
 int ffb_trace_shape_count(void);

@@ -1,6 +1,7 @@
-"""Batched scenes in one fused launch (ffb_batch_*) give, scene by scene,
-exactly the counts of the single-scene path with the same seed and epoch;
-a CUDA graph that captured the launch draws fresh rays on every replay."""
+"""Batched scenes (ffb_batch_*: one single-scene launch per scene over side
+streams, capturable as one CUDA graph) give, scene by scene, exactly the
+counts of the single-scene path with the same seed and epoch; a CUDA graph
+that captured the launches draws fresh rays on every replay."""
 import numpy as np
 import pytest
 

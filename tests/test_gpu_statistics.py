@@ -99,8 +99,8 @@ def test_reference_test_scenes_within_4_sigma_of_reference(ctx, oracle, case):
 
 
 def test_per_face_matrix_within_4_sigma_of_live_reference(ctx, reference):
-    """Per-face meshes (the form of BASELINE's N x N matrix) on a clutter
-    scene: every entry with enough expected hits within 4 sigma of the
+    """Per-face meshes (the per-face N x N matrix of the benchmarked
+    workloads) on a clutter scene: every entry with enough expected hits within 4 sigma of the
     reference calculator run live (oracle/_ref), raw-normal emission as the
     reference's."""
     faces = scenes.clutter(40, 0.15, seed=8, enclosure_cells=2)
