@@ -58,6 +58,8 @@ def parse():
                     help="fixed grid sizing target (0: the autotuner chooses the grid among 128, 192 and 256 cells "
                          "per face and the kernel's launch shape; the library default is 32)")
     ap.add_argument("--no-skip", action="store_true", help="plain DDA without empty-space jumps")
+    ap.add_argument("--trace-shape", type=int, default=-1,
+                    help="launch shape of the fused kernel with a fixed grid (-1: shape 0, or the autotuner's)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes section")
     ap.add_argument("--no-served", action="store_true", help="skip the served-requests section")
     ap.add_argument("--no-csv", action="store_true", help="skip the CSV-export section")
@@ -793,6 +795,8 @@ def ours(args):
             ctx.set_trace_shape(tune["shape"])
         tune["shape_params"] = native.trace_shapes()[tune["shape"]]
         ctx.set_stats(False)
+    if tune is None and args.trace_shape >= 0:
+        ctx.set_trace_shape(args.trace_shape)
     t0 = time.perf_counter()
     if tune is None:
         ctx.grid_build(dims=dims, cells_per_face=args.cells_per_face, skip_empty=not args.no_skip)
