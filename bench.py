@@ -805,6 +805,7 @@ def ours(args):
     torch.cuda.synchronize()
     grid_s = time.perf_counter() - t0
     info = ctx.grid_info()
+    timed_shape = ctx.trace_shape()
     # source rows of this rank (all of them on one GPU): ranks split the rows
     # of the one solve, balanced by rays, and exchange nothing while tracing
     row_b, row_e = shard.rank_rows(front, rear, rank, world)
@@ -924,7 +925,7 @@ def ours(args):
             "config": {"workload": WORKLOAD, "faces": n, "rays_per_step": rays_per_step,
                        "grid": [info.nx, info.ny, info.nz],
                        "cells_per_face": tune["cells_per_face"] if tune else args.cells_per_face,
-                       "autotune": tune, "trace_shape": ctx.trace_shape(),
+                       "autotune": tune, "trace_shape": timed_shape,
                        "grid_refs": int(info.n_refs),
                        "grid_build_ms": 1e3 * grid_s,
                        "parallelism": "source rows split over %d ranks (one solve)" % world if world > 1 else "single",

@@ -240,7 +240,9 @@ int stage(ffb_ctx* c, size_t bytes, void** out)
     if (c->pinned)
       cudaFreeHost(c->pinned);
     c->pinned = nullptr;
-    size_t want = std::max(bytes, c->pinned_cap * 2);
+    // at least 8 MiB, doubling: page-locked allocations synchronise the
+    // device, so the staging buffer grows rarely
+    size_t want = std::max(std::max(bytes, c->pinned_cap * 2), (size_t)8 << 20);
     FFB_CUDA(cudaMallocHost(&c->pinned, want));
     c->pinned_cap = want;
   }

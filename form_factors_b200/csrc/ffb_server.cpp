@@ -7,8 +7,9 @@
 // request: uploads the scene, builds the grid, allocates and zeroes the
 // count matrix and builds the chunk table.  A prepared request joins the
 // trace rotation of one scheduler thread, which launches the requests'
-// traces in slices of at most kSliceRays rays, round-robin over the
-// prepared requests, with kWindow slices in flight: the next slice is
+// traces in slices of at most `slice_rays` rays (ffb_server_set_slicing),
+// round-robin over the prepared requests, with `window` slices in flight:
+// the next slice is
 // queued while the current one runs, and slices of different requests run
 // on different streams, so a request admitted while others trace starts at
 // the next slice boundary and its kernels overlap theirs on the device (a
@@ -48,13 +49,13 @@ using Clock = std::chrono::steady_clock;
 
 double secs(Clock::time_point t0, Clock::time_point t1) { return std::chrono::duration<double>(t1 - t0).count(); }
 
-// Rays per trace slice: about 7 ms of trace on a B200, long against a
-// launch and its tail, short against the large requests that small ones
-// would otherwise wait behind.
-constexpr long long kSliceRays = 16ll << 20;
+// Default rays per trace slice: about 25 ms of trace on a B200, long
+// against a launch and its tail, short against the large requests that
+// small ones would otherwise wait behind.
+constexpr long long kSliceRays = 64ll << 20;
 constexpr long long kChunkRays = 256;  // rays per chunk of the fused kernel
-constexpr long long kSliceChunks = kSliceRays / kChunkRays;
-constexpr int kWindow = 2;  // slices in flight
+constexpr int kWindow = 2;             // default slices in flight
+constexpr int kMaxWindow = 8;
 
 struct Request {
   long long id = 0;
@@ -116,6 +117,11 @@ struct ffb_server {
   int running = 0;
   int peak_running = 0;
   int peak_tracing = 0;  // most requests in the trace rotation at once
+  long long slice_chunks = kSliceRays / kChunkRays;
+  int window = kWindow;
+  // frees of released matrices, off every slot's stream: a synchronous
+  // cudaFree would wait for the whole device and drain the slice pipeline
+  cudaStream_t free_stream = nullptr;
 };
 
 namespace {
@@ -183,7 +189,7 @@ void finish(ffb_server* s, Slot& sl, const std::shared_ptr<Request>& r, int err,
       r->error = err;
       r->message = msg;
       if (r->counts) {
-        cudaFree(r->counts);
+        cudaFreeAsync(r->counts, s->free_stream);
         r->counts = nullptr;
       }
       s->reserved -= r->reserve;
@@ -264,7 +270,7 @@ void scheduler_main(ffb_server* s)
 {
   cudaSetDevice(s->device);
   std::vector<cudaEvent_t> pool;
-  for (int k = 0; k < kWindow; ++k) {
+  for (int k = 0; k < kMaxWindow; ++k) {
     cudaEvent_t e = nullptr;
     cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync);
     pool.push_back(e);
@@ -275,7 +281,7 @@ void scheduler_main(ffb_server* s)
     {
       std::unique_lock<std::mutex> lock(s->mu);
       // fill the window: the next slot in round-robin order with chunks left
-      while ((int)inflight.size() < kWindow) {
+      while ((int)inflight.size() < s->window) {
         int pick = -1;
         for (size_t k = 0; k < s->slots.size(); ++k) {
           const size_t i = (rr + k) % s->slots.size();
@@ -289,7 +295,7 @@ void scheduler_main(ffb_server* s)
           break;
         rr = (size_t)pick + 1;
         Slot& sl = s->slots[(size_t)pick];
-        const long long first = sl.next, count = std::min(kSliceChunks, sl.n_chunks - sl.next);
+        const long long first = sl.next, count = std::min(s->slice_chunks, sl.n_chunks - sl.next);
         sl.next += count;
         int rc = ffb_trace_slice(sl.ctx, first, count);
         cudaEvent_t ev = pool.back();
@@ -358,11 +364,18 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
   s->budget = budget_bytes;
   s->n_slots = n_slots;
   s->slots.resize((size_t)n_slots);
+  cudaSetDevice(device);
+  if (cudaStreamCreateWithFlags(&s->free_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete s;
+    return ffb_set_error(FFB_ERR_CUDA, "ffb_server_create: stream creation failed");
+  }
   for (Slot& sl : s->slots) {
     int rc = ffb_ctx_create(device, &sl.ctx);
     if (rc < 0) {
       for (Slot& o : s->slots)
         ffb_ctx_destroy(o.ctx);
+      cudaStreamDestroy(s->free_stream);
       delete s;
       return rc;
     }
@@ -395,7 +408,9 @@ extern "C" void ffb_server_destroy(ffb_server* s)
   cudaSetDevice(s->device);
   for (auto& kv : s->all)
     if (kv.second->counts)
-      cudaFree(kv.second->counts);
+      cudaFreeAsync(kv.second->counts, s->free_stream);
+  cudaStreamSynchronize(s->free_stream);
+  cudaStreamDestroy(s->free_stream);
   for (Slot& sl : s->slots)
     ffb_ctx_destroy(sl.ctx);
   delete s;
@@ -512,11 +527,22 @@ extern "C" int ffb_server_release(ffb_server* s, long long id)
     r->reserve = 0;
   }
   if (r->counts) {
+    // the request's trace has retired and no result copy is in progress
     cudaSetDevice(s->device);
-    cudaFree(r->counts);
+    cudaFreeAsync(r->counts, s->free_stream);
     r->counts = nullptr;
   }
   s->cv_work.notify_all();
+  return FFB_OK;
+}
+
+extern "C" int ffb_server_set_slicing(ffb_server* s, long long slice_rays, int window)
+{
+  if (!s || slice_rays < kChunkRays || window < 1 || window > kMaxWindow)
+    return ffb_set_error(FFB_ERR_ARG, "ffb_server_set_slicing: slice_rays >= 256 and 1 <= window <= 8");
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->slice_chunks = slice_rays / kChunkRays;
+  s->window = window;
   return FFB_OK;
 }
 

@@ -192,6 +192,7 @@ def load(path=LIB_PATH):
         "ffb_server_result": (i32, [vp, C.c_longlong, vp]),
         "ffb_server_release": (i32, [vp, C.c_longlong]),
         "ffb_server_stats": (i32, [vp, C.POINTER(ServerInfo)]),
+        "ffb_server_set_slicing": (i32, [vp, C.c_longlong, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -696,6 +697,10 @@ class Server:
             out = np.empty((n_faces, n_faces), np.uint32)
         _check(self._lib.ffb_server_result(self._h, int(rid), _ptr(out)))
         return out
+
+    def set_slicing(self, slice_rays, window=2):
+        """Rays per trace slice and slices in flight (ffb_server_set_slicing)."""
+        _check(self._lib.ffb_server_set_slicing(self._h, int(slice_rays), int(window)))
 
     def release(self, rid):
         _check(self._lib.ffb_server_release(self._h, int(rid)))

@@ -201,8 +201,8 @@ int ffb_batch_launch(ffb_ctx* ctx, uint32_t* counts, const unsigned long long* c
  * until released.  Each slot is a context (own stream, resident scene) whose
  * worker thread prepares its request -- scene upload, grid build, zeroed
  * count matrix, chunk table -- while other requests trace.  One scheduler
- * thread then traces the prepared requests in slices of at most 16 Mi rays,
- * round-robin over them, with two slices in flight on the requests' own
+ * thread then traces the prepared requests in slices (64 Mi rays by default,
+ * ffb_server_set_slicing), round-robin over them, two in flight on the requests' own
  * streams: a request admitted while others are on the GPU joins at the next
  * slice boundary, its kernels overlap theirs on the device, and a small
  * request finishes within its first turn instead of queueing behind a large
@@ -254,6 +254,10 @@ int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts
 /* Frees a finished request's resident matrix and its budget reservation. */
 int ffb_server_release(ffb_server* server, long long request_id);
 int ffb_server_stats(ffb_server* server, ffb_server_info* out);
+/* Trace slicing of the server: at most slice_rays rays per slice (default
+ * 64 Mi, rounded down to whole 256-ray chunks) and `window` slices in flight
+ * (default 2, at most 8).  Applies to the slices launched after the call. */
+int ffb_server_set_slicing(ffb_server* server, long long slice_rays, int window);
 
 /* One step of the radiance equation (thermal_equation/radiance_cpu.cpp:96-190)
  * on the resident scene and grid: every face emits front[f] + rear[f] Malley

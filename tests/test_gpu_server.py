@@ -68,6 +68,7 @@ def test_traces_of_requests_overlap_on_the_device(ctx):
     faces = scenes.icosphere(5, 1.0, inward=True)
     n = len(faces)
     server = native.Server(0, budget_bytes=0, slots=2)
+    server.set_slicing(16 << 20, 2)
     ids = [server.submit(faces, 3000, seed) for seed in (41, 42)]
     infos = [server.wait(i, timeout_s=300) for i in ids]
     assert all(inf.state == 2 for inf in infos)
