@@ -370,6 +370,7 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
     delete s;
     return ffb_set_error(FFB_ERR_CUDA, "ffb_server_create: stream creation failed");
   }
+
   for (Slot& sl : s->slots) {
     int rc = ffb_ctx_create(device, &sl.ctx);
     if (rc < 0) {
@@ -380,6 +381,18 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
       return rc;
     }
     ffb_ctx_set_stats(sl.ctx, 0);  // requests return counts only
+  }
+  if (budget_bytes > 0) {
+    // Map the budget into the device's stream-ordered pool once (the contexts set it to keep
+    // freed memory): the requests' matrices are then
+    // carved out of memory that is already mapped, instead of growing the
+    // pool -- new mappings while other requests' kernels run -- on the way.
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, (size_t)budget_bytes, s->free_stream) == cudaSuccess) {
+      cudaFreeAsync(p, s->free_stream);
+      cudaStreamSynchronize(s->free_stream);
+    }
+    cudaGetLastError();  // a budget beyond the free memory is not an error here
   }
   s->scheduler = std::thread(scheduler_main, s);
   for (int i = 0; i < n_slots; ++i)
