@@ -734,7 +734,7 @@ def traffic_per_launch():
         return None
 
 
-def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm):
+def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm, shape=0):
     """The bound the fused kernel meets: instruction issue.  Warp
     instructions per ray from the committed ncu summary (profiles/
     traffic.json) x rays per launch / kernel time, against 4 issue slots per
@@ -742,7 +742,7 @@ def issue_roofline(k_ms, rays_per_launch, sm_mhz, n_sm):
     an input is missing."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        ipr = float(d["k_form_factors_warp_inst_per_ray"])
+        ipr = float(d.get("warp_inst_per_ray_by_shape", {}).get(str(shape), d["k_form_factors_warp_inst_per_ray"]))
         if not sm_mhz or not k_ms or not n_sm:
             return None
         achieved = ipr * rays_per_launch / (k_ms * 1e-3)
@@ -945,7 +945,8 @@ def ours(args):
                                  "frac": (traffic_per_launch() or 0) / (k_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
                                  "peak_source": hbm_peak()[1],
                                  "note": "DRAM bytes per launch (ncu) / kernel time, of the copy bandwidth"},
-                         "issue": issue_roofline(k_ms, rays_per_step / world, clk.get("sm_mhz"),
+                         "issue": issue_roofline(k_ms, rays_per_step / world, clk.get("sm_mhz"), shape=timed_shape,
+                                                 n_sm=
                                                  torch.cuda.get_device_properties(local).multi_processor_count)},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,

@@ -1176,7 +1176,7 @@ int ffb_trace_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, uin
   return FFB_OK;
 }
 
-int ffb_trace_slice(ffb_ctx* c, long long first, long long count)
+int ffb_trace_slice(ffb_ctx* c, long long first, long long count, void* stream)
 {
   FFB_TRY(check_ctx(c));
   if (!c->slice_ready)
@@ -1187,11 +1187,12 @@ int ffb_trace_slice(ffb_ctx* c, long long first, long long count)
   TraceParams p = c->slice_params;
   p.chunks = dptr<Chunk>(c->chunks) + first;
   p.n_chunks = (int)count;
-  // slices of one context run in stream order, so one cursor serves them all
-  FFB_CUDA(cudaMemsetAsync(p.chunk_cursor, 0, sizeof(uint32_t), c->stream));
+  // slices of one prepared trace run in stream order, so one cursor serves them all
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  FFB_CUDA(cudaMemsetAsync(p.chunk_cursor, 0, sizeof(uint32_t), st));
   if (c->main.info.skip_empty)
-    return launch_fused<true>(c, p, false);
-  return launch_fused<false>(c, p, false);
+    return launch_fused<true>(c, p, false, st);
+  return launch_fused<false>(c, p, false, st);
 }
 
 int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long* end_ns)

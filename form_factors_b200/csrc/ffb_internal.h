@@ -15,7 +15,10 @@ int ffb_set_error(int code, const char* msg);
 // builds the chunk table (256 consecutive rays of one face per chunk), zeroes
 // the device matrix `counts` (n_faces^2 uint32) and returns the number of
 // chunks.  ffb_trace_slice enqueues the launch over chunks
-// [first, first + count) on the context stream; the slices of a prepared
+// [first, first + count) on `stream` (NULL: the context stream; the
+// prepare's work must be complete or ordered before it, and all slices of
+// one prepared trace must go to one stream: they share its chunk cursor);
+// the slices of a prepared
 // trace may come in any split, and once every chunk has been traced exactly
 // once `counts` equals what ffb_form_factor_counts gives for the same
 // arguments (integer sums do not depend on the order).  ffb_trace_span
@@ -23,5 +26,5 @@ int ffb_set_error(int code, const char* msg);
 // the prepare, in %globaltimer nanoseconds (synchronises the stream).
 int ffb_trace_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
                       uint32_t* counts, long long* n_chunks);
-int ffb_trace_slice(ffb_ctx* c, long long first, long long count);
+int ffb_trace_slice(ffb_ctx* c, long long first, long long count, void* stream);
 int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long* end_ns);

@@ -84,7 +84,9 @@ struct Request {
 enum Phase { kIdle, kPreparing, kTracing, kTraced };
 
 struct Slot {
-  ffb_ctx* ctx = nullptr;
+  ffb_ctx* ctx = nullptr;       // on `prep`: the preparation
+  cudaStream_t prep = nullptr;  // low priority
+  cudaStream_t trace = nullptr; // high priority: the trace slices
   std::shared_ptr<Request> req;
   Phase phase = kIdle;
   long long n_chunks = 0, next = 0;
@@ -297,9 +299,9 @@ void scheduler_main(ffb_server* s)
         Slot& sl = s->slots[(size_t)pick];
         const long long first = sl.next, count = std::min(s->slice_chunks, sl.n_chunks - sl.next);
         sl.next += count;
-        int rc = ffb_trace_slice(sl.ctx, first, count);
+        int rc = ffb_trace_slice(sl.ctx, first, count, sl.trace);
         cudaEvent_t ev = pool.back();
-        if (rc >= 0 && cudaEventRecord(ev, (cudaStream_t)ffb_ctx_stream(sl.ctx)) != cudaSuccess) {
+        if (rc >= 0 && cudaEventRecord(ev, sl.trace) != cudaSuccess) {
           cudaGetLastError();
           rc = ffb_set_error(FFB_ERR_CUDA, "event record after a trace slice failed");
         }
@@ -371,11 +373,30 @@ extern "C" int ffb_server_create(int device, unsigned long long budget_bytes, in
     return ffb_set_error(FFB_ERR_CUDA, "ffb_server_create: stream creation failed");
   }
 
+  // Traces at the device's highest stream priority, preparation at its
+  // lowest: when a slice's blocks retire, the block scheduler gives the SMs
+  // to the next slice before another request's grid build or zeroing.
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   for (Slot& sl : s->slots) {
     int rc = ffb_ctx_create(device, &sl.ctx);
+    cudaStream_t prep = nullptr;
+    if (rc >= 0 && (cudaStreamCreateWithPriority(&prep, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
+                    cudaStreamCreateWithPriority(&sl.trace, cudaStreamNonBlocking, prio_high) != cudaSuccess)) {
+      cudaGetLastError();
+      rc = ffb_set_error(FFB_ERR_CUDA, "ffb_server_create: stream creation failed");
+    }
+    if (rc >= 0)
+      rc = ffb_ctx_set_stream(sl.ctx, prep);
+    sl.prep = prep;
     if (rc < 0) {
-      for (Slot& o : s->slots)
+      for (Slot& o : s->slots) {
         ffb_ctx_destroy(o.ctx);
+        if (o.prep)
+          cudaStreamDestroy(o.prep);
+        if (o.trace)
+          cudaStreamDestroy(o.trace);
+      }
       cudaStreamDestroy(s->free_stream);
       delete s;
       return rc;
@@ -424,8 +445,11 @@ extern "C" void ffb_server_destroy(ffb_server* s)
       cudaFreeAsync(kv.second->counts, s->free_stream);
   cudaStreamSynchronize(s->free_stream);
   cudaStreamDestroy(s->free_stream);
-  for (Slot& sl : s->slots)
+  for (Slot& sl : s->slots) {
     ffb_ctx_destroy(sl.ctx);
+    cudaStreamDestroy(sl.prep);
+    cudaStreamDestroy(sl.trace);
+  }
   delete s;
 }
 

@@ -43,8 +43,13 @@ def test_reference_arm_prints_one_json_line():
 
 
 def test_issue_roofline_arithmetic():
+    d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    for shape in (0, 7, 5):
+        got = bench.issue_roofline(10.0, 1_000_000, 2000.0, 100, shape=shape)
+        ipr = d.get("warp_inst_per_ray_by_shape", {}).get(str(shape), d["k_form_factors_warp_inst_per_ray"])
+        assert got["warp_inst_per_ray"] == ipr
     got = bench.issue_roofline(10.0, 1_000_000, 2000.0, 100)
-    ipr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["k_form_factors_warp_inst_per_ray"]
+    ipr = d.get("warp_inst_per_ray_by_shape", {}).get("0", d["k_form_factors_warp_inst_per_ray"])
     achieved = ipr * 1_000_000 / 10e-3
     peak = 4 * 100 * 2000e6
     assert got["frac"] == pytest.approx(achieved / peak)
