@@ -2213,7 +2213,7 @@ extern "C" int ffb_trace_shape_get(int shape, ffb_trace_shape* out)
   if (shape < 0 || shape >= kNumShapes || !out)
     return fail(FFB_ERR_ARG, "shape %d outside [0, %d)", shape, kNumShapes);
   const TraceShape t = trace_shape(shape);
-  *out = ffb_trace_shape{t.adv, t.test, t.refill, t.blocks, t.coherent};
+  *out = ffb_trace_shape{t.adv, t.test, t.refill, t.blocks, t.coherent, t.lanes};
   return FFB_OK;
 }
 

@@ -196,21 +196,28 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 // the order of their directions (bins of an 8 x 8 Morton order on the Malley
 // disk) instead of in index order, so that lanes refilled together trace
 // rays of similar direction from the same face.
+// With `lanes` = K > 0, each lane keeps K rays in shared memory instead of
+// one in registers, and each iteration the warp runs ONE body -- the cell
+// advances or the triangle tests -- chosen by a vote of its lanes, each lane
+// working on one of its rays in that phase; `refill` is then the number of
+// lanes with a free ray slot that triggers a refill.
 struct TraceShape {
-  int adv, test, refill, blocks, coherent;
+  int adv, test, refill, blocks, coherent, lanes;
 };
-constexpr int kNumShapes = 9;
+constexpr int kNumShapes = 11;
 __host__ __device__ constexpr TraceShape trace_shape(int v)
 {
-  return v == 1 ? TraceShape{1, 1, 4, 8, 0}
-       : v == 2 ? TraceShape{2, 1, 6, 8, 0}
-       : v == 3 ? TraceShape{1, 2, 6, 8, 0}
-       : v == 4 ? TraceShape{3, 3, 6, 8, 0}
-       : v == 5 ? TraceShape{2, 2, 10, 8, 0}
-       : v == 6 ? TraceShape{2, 2, 6, 6, 0}
-       : v == 7 ? TraceShape{2, 2, 6, 8, 1}
-       : v == 8 ? TraceShape{2, 2, 10, 8, 1}
-                : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS, 0};
+  return v == 1 ? TraceShape{1, 1, 4, 8, 0, 0}
+       : v == 2 ? TraceShape{2, 1, 6, 8, 0, 0}
+       : v == 3 ? TraceShape{1, 2, 6, 8, 0, 0}
+       : v == 4 ? TraceShape{3, 3, 6, 8, 0, 0}
+       : v == 5 ? TraceShape{2, 2, 10, 8, 0, 0}
+       : v == 6 ? TraceShape{2, 2, 6, 6, 0, 0}
+       : v == 7 ? TraceShape{2, 2, 6, 8, 1, 0}
+       : v == 8 ? TraceShape{2, 2, 10, 8, 1, 0}
+       : v == 9 ? TraceShape{2, 2, 8, 8, 0, 2}
+       : v == 10 ? TraceShape{2, 2, 8, 8, 1, 2}
+                 : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS, 0, 0};
 }
 
 constexpr int kChunkRaysMax = 256;  // rays per chunk (the host's chunk size)
@@ -274,6 +281,70 @@ __device__ __forceinline__ void direction_order(uint32_t face, uint32_t j0, int 
   __syncwarp();
 }
 
+// Ray state of the shared-memory lanes (TraceShape::lanes): field f of the
+// ray in column c at R[f * kLaneRayCols + c], 32-bit words.  The cell
+// coordinates (each below 256) and the empty-space distance (below 128) share
+// one word; the direction signs are recomputed from the direction.
+enum {
+  kRayOx, kRayOy, kRayOz, kRayDx, kRayDy, kRayDz, kRayIx, kRayIy, kRayIz, kRayDlen, kRayBest, kRayBestRef, kRayI,
+  kRayEn, kRayCell, kRayRow, kRayFields
+};
+constexpr int kLaneRayCols = 2 * kTraceThreads;  // columns for K = 2 rays per lane
+
+__device__ __forceinline__ void lane_ray_load(const uint32_t* R, int c, Tracer& T)
+{
+  T.o = f3(__uint_as_float(R[kRayOx * kLaneRayCols + c]), __uint_as_float(R[kRayOy * kLaneRayCols + c]),
+           __uint_as_float(R[kRayOz * kLaneRayCols + c]));
+  T.dir = f3(__uint_as_float(R[kRayDx * kLaneRayCols + c]), __uint_as_float(R[kRayDy * kLaneRayCols + c]),
+             __uint_as_float(R[kRayDz * kLaneRayCols + c]));
+  T.inv = f3(__uint_as_float(R[kRayIx * kLaneRayCols + c]), __uint_as_float(R[kRayIy * kLaneRayCols + c]),
+             __uint_as_float(R[kRayIz * kLaneRayCols + c]));
+  T.dlen = __uint_as_float(R[kRayDlen * kLaneRayCols + c]);
+  T.best = __uint_as_float(R[kRayBest * kLaneRayCols + c]);
+  T.best_ref = (int)R[kRayBestRef * kLaneRayCols + c];
+  T.i = R[kRayI * kLaneRayCols + c];
+  T.en = R[kRayEn * kLaneRayCols + c];
+  const uint32_t cell = R[kRayCell * kLaneRayCols + c];
+  T.cx = (int)(cell & 0xFFu);
+  T.cy = (int)((cell >> 8) & 0xFFu);
+  T.cz = (int)((cell >> 16) & 0xFFu);
+  T.jump = (int)(cell >> 24);
+  T.sx = sgn(T.dir.x);
+  T.sy = sgn(T.dir.y);
+  T.sz = sgn(T.dir.z);
+}
+
+__device__ __forceinline__ void lane_ray_store_cell(uint32_t* R, int c, const Tracer& T)
+{
+  R[kRayI * kLaneRayCols + c] = T.i;
+  R[kRayEn * kLaneRayCols + c] = T.en;
+  R[kRayCell * kLaneRayCols + c] =
+      (uint32_t)T.cx | ((uint32_t)T.cy << 8) | ((uint32_t)T.cz << 16) | ((uint32_t)T.jump << 24);
+}
+
+__device__ __forceinline__ void lane_ray_store_test(uint32_t* R, int c, const Tracer& T)
+{
+  R[kRayBest * kLaneRayCols + c] = __float_as_uint(T.best);
+  R[kRayBestRef * kLaneRayCols + c] = (uint32_t)T.best_ref;
+  R[kRayI * kLaneRayCols + c] = T.i;
+}
+
+__device__ __forceinline__ void lane_ray_store(uint32_t* R, int c, const Tracer& T)
+{
+  R[kRayOx * kLaneRayCols + c] = __float_as_uint(T.o.x);
+  R[kRayOy * kLaneRayCols + c] = __float_as_uint(T.o.y);
+  R[kRayOz * kLaneRayCols + c] = __float_as_uint(T.o.z);
+  R[kRayDx * kLaneRayCols + c] = __float_as_uint(T.dir.x);
+  R[kRayDy * kLaneRayCols + c] = __float_as_uint(T.dir.y);
+  R[kRayDz * kLaneRayCols + c] = __float_as_uint(T.dir.z);
+  R[kRayIx * kLaneRayCols + c] = __float_as_uint(T.inv.x);
+  R[kRayIy * kLaneRayCols + c] = __float_as_uint(T.inv.y);
+  R[kRayIz * kLaneRayCols + c] = __float_as_uint(T.inv.z);
+  R[kRayDlen * kLaneRayCols + c] = __float_as_uint(T.dlen);
+  lane_ray_store_test(R, c, T);
+  lane_ray_store_cell(R, c, T);
+}
+
 template <bool kSkip, bool kStats, bool kHash, bool kPower = false, int kShape = 0>
 __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
     k_form_factors(const __grid_constant__ TraceParams p)
@@ -283,6 +354,8 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
   // coherent hand-out: per warp, direction-bin counters and the chunk's ray order
   __shared__ uint32_t s_bins[kS.coherent ? kWarpsPerBlock * kDirBins : 1];
   __shared__ uint8_t s_perm[kS.coherent ? kWarpsPerBlock * kChunkRaysMax : 1];
+  // K rays per lane: kRayFields fields of kTraceThreads * K slots
+  __shared__ uint32_t s_rays[kS.lanes ? kRayFields * kTraceThreads * kS.lanes : 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (p.span && threadIdx.x == 0)
     atomicMin(p.span, global_ns());
@@ -308,13 +381,149 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
     key1 = k.y;
   }
   bool exhausted = false;
+  uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0, n_jumps = 0;
+  if constexpr (kS.lanes > 0) {
+    // ---- K rays per lane in shared memory, one body per iteration ----
+    constexpr int K = kS.lanes;
+    static_assert(K * kTraceThreads <= kLaneRayCols, "lane ray columns");
+    uint32_t* const R = s_rays;
+    // the fields of slot k of this lane: column (warp * K + k) * 32 + lane,
+    // so that the 32 lanes of a warp always hit 32 different banks
+    const int col0 = warp * K * 32 + lane;
+    uint32_t ph = 0;  // 2 bits per slot: 0 free, 1 cell exhausted (advance), 2 references pending (test)
+    for (;;) {
+      bool has_free = false, has_adv = false, has_test = false;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const uint32_t s = (ph >> (2 * k)) & 3u;
+        has_free |= s == 0u;
+        has_adv |= s == 1u;
+        has_test |= s == 2u;
+      }
+      unsigned need = __ballot_sync(kFull, has_free);
+      const unsigned busy = __ballot_sync(kFull, has_adv || has_test);
+      if (__popc(need) < kS.refill && busy)
+        need = 0;
+      while (need && !exhausted) {
+        if (c_left == 0) {
+          int k = 0;
+          if (lane == 0)
+            k = (int)atomicAdd(p.chunk_cursor, 1u);
+          k = __shfl_sync(kFull, k, 0);
+          if (k >= p.n_chunks) {
+            exhausted = true;
+            break;
+          }
+          const Chunk ch = p.chunks[k];
+          c_face = ch.face;
+          c_j = ch.j0;
+          c_left = ch.count;
+          c_front = ch.front;
+          c_row = S.face_to_row ? __ldg(S.face_to_row + ch.face) : ch.face;
+          c_pos = 0;
+          if (kS.coherent)
+            direction_order((uint32_t)c_face, (uint32_t)c_j, c_left, key0, key1, epoch, s_bins + warp * kDirBins,
+                            s_perm + warp * kChunkRaysMax, lane);
+        }
+        const int take = min(__popc(need), c_left);
+        const int rank = __popc(need & lane_below);
+        const bool mine = ((need >> lane) & 1u) && rank < take;
+        if (mine) {
+          const int j = c_j + (kS.coherent ? (int)s_perm[warp * kChunkRaysMax + c_pos + rank] : c_pos + rank);
+          float3 o, e;
+          emit_ray(p.frames + 20 * ((size_t)S.face_base + c_face), (uint32_t)c_face, (uint32_t)j, c_front, key0,
+                   key1, epoch, o, e);
+          ++n_rays;
+          Tracer T;
+          if (tracer_begin<kSkip>(T, S.g, o, e, n_cells)) {
+            int k = 0;
+            while (k < K - 1 && ((ph >> (2 * k)) & 3u) != 0u)
+              ++k;
+            const int c = col0 + 32 * k;
+            lane_ray_store(R, c, T);
+            R[kRayRow * kLaneRayCols + c] = (uint32_t)(kPower ? 2 * c_face + (j >= c_front ? 1 : 0) : c_row);
+            ph |= (T.i < T.en ? 2u : 1u) << (2 * k);
+          }
+        }
+        need &= ~__ballot_sync(kFull, mine);
+        c_pos += take;
+        c_left -= take;
+      }
+      has_adv = has_test = false;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const uint32_t s = (ph >> (2 * k)) & 3u;
+        has_adv |= s == 1u;
+        has_test |= s == 2u;
+      }
+      const unsigned va = __ballot_sync(kFull, has_adv), vt = __ballot_sync(kFull, has_test);
+      if (exhausted && !(va | vt))
+        break;
+      const bool do_test = __popc(vt) >= __popc(va);
+      int hit = -1, row = 0;
+      if (do_test ? has_test : has_adv) {
+        const uint32_t want = do_test ? 2u : 1u;
+        int k = 0;
+        while (k < K - 1 && ((ph >> (2 * k)) & 3u) != want)
+          ++k;
+        const int c = col0 + 32 * k;
+        Tracer T;
+        lane_ray_load(R, c, T);
+        uint32_t s;
+        if (do_test) {
+#pragma unroll
+          for (int t = 0; t < kS.test; ++t)
+            if (T.i < T.en)
+              tracer_test(T, S.g, n_tests);
+          lane_ray_store_test(R, c, T);
+          s = T.i < T.en ? 2u : 1u;
+        } else {
+          bool live = true;
+#pragma unroll
+          for (int a = 0; a < kS.adv; ++a)
+            if (live && T.i >= T.en)
+              live = tracer_advance<kSkip>(T, S.g, n_cells, n_jumps);
+          if (!live) {
+            hit = tracer_result(T, S.g);
+            row = (int)R[kRayRow * kLaneRayCols + c];
+            s = 0u;
+          } else {
+            lane_ray_store_cell(R, c, T);
+            s = T.i < T.en ? 2u : 1u;
+          }
+        }
+        ph = (ph & ~(3u << (2 * k))) | (s << (2 * k));
+      }
+      bool fresh = false;
+      if (hit >= 0) {
+        ++n_hits;
+        const int hcol = S.face_to_row ? __ldg(S.face_to_row + hit) : hit;
+        if (kPower) {
+          atomicAdd(p.absorb + hcol, __ldg(p.power + row));
+        } else {
+          const uint32_t key = (uint32_t)row * (uint32_t)S.n_cols + (uint32_t)hcol;
+          if (kHash)
+            fresh = warp_hash_add(keys, vals, key, S.counts);
+          else
+            atomicAdd(S.counts + key, 1u);
+        }
+      }
+      if (kHash) {
+        fill += __popc(__ballot_sync(kFull, fresh));
+        if (fill > kWarpHash / 2) {
+          warp_hash_flush(keys, vals, S.counts, lane);
+          fill = 0;
+        }
+      }
+    }
+  } else {
   // lane state
   Tracer T;
   bool active = false;
   int my_row = 0;
-  uint32_t n_tests = 0, n_cells = 0, n_rays = 0, n_hits = 0, n_jumps = 0;
   for (;;) {
     unsigned need = __ballot_sync(kFull, !active);
+
     if (__popc(need) < kS.refill && need != kFull)
       need = 0;
     while (need && !exhausted) {
@@ -395,6 +604,7 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
       }
     }
   }
+  }  // one ray per lane in registers
   if (kHash)
     warp_hash_flush(keys, vals, S.counts, lane);
   if (kStats)

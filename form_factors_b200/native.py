@@ -98,7 +98,7 @@ def bounding_sphere(faces):
 
 class TraceShape(C.Structure):
     _fields_ = [("adv_per_iter", C.c_int), ("test_per_iter", C.c_int), ("refill_min", C.c_int),
-                ("blocks_per_sm", C.c_int), ("coherent", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("coherent", C.c_int), ("lanes", C.c_int)]
 
 
 class TuneResult(C.Structure):
@@ -229,7 +229,7 @@ def trace_shapes():
         t = TraceShape()
         _check(lib.ffb_trace_shape_get(v, C.byref(t)))
         out.append(dict(adv_per_iter=t.adv_per_iter, test_per_iter=t.test_per_iter, refill_min=t.refill_min,
-                        blocks_per_sm=t.blocks_per_sm, coherent=bool(t.coherent)))
+                        blocks_per_sm=t.blocks_per_sm, coherent=bool(t.coherent), lanes=t.lanes))
     return out
 
 

@@ -408,6 +408,8 @@ typedef struct {
   int refill_min;     /* idle lanes a warp waits for before it refills them */
   int blocks_per_sm;  /* resident 128-thread blocks per SM the kernel is built for */
   int coherent;       /* 1: a chunk's rays are handed out in direction order */
+  int lanes;          /* 0: one ray per lane in registers; K: K rays per lane in shared memory, one
+                         body (advances or tests) per iteration chosen by a vote of the lanes */
 } ffb_trace_shape;
 
 int ffb_trace_shape_count(void);
