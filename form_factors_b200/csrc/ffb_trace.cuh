@@ -204,7 +204,7 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 struct TraceShape {
   int adv, test, refill, blocks, coherent, lanes;
 };
-constexpr int kNumShapes = 11;
+constexpr int kNumShapes = 13;
 __host__ __device__ constexpr TraceShape trace_shape(int v)
 {
   return v == 1 ? TraceShape{1, 1, 4, 8, 0, 0}
@@ -217,6 +217,8 @@ __host__ __device__ constexpr TraceShape trace_shape(int v)
        : v == 8 ? TraceShape{2, 2, 10, 8, 1, 0}
        : v == 9 ? TraceShape{2, 2, 8, 8, 0, 2}
        : v == 10 ? TraceShape{2, 2, 8, 8, 1, 2}
+       : v == 11 ? TraceShape{2, 2, 8, 8, 0, 3}
+       : v == 12 ? TraceShape{2, 3, 8, 8, 0, 2}
                  : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS, 0, 0};
 }
 
@@ -282,29 +284,28 @@ __device__ __forceinline__ void direction_order(uint32_t face, uint32_t j0, int 
 }
 
 // Ray state of the shared-memory lanes (TraceShape::lanes): field f of the
-// ray in column c at R[f * kLaneRayCols + c], 32-bit words.  The cell
+// ray in column c at R[f * kCols + c], 32-bit words, kCols = K * 128.  The cell
 // coordinates (each below 256) and the empty-space distance (below 128) share
 // one word; the direction signs are recomputed from the direction.
 enum {
   kRayOx, kRayOy, kRayOz, kRayDx, kRayDy, kRayDz, kRayIx, kRayIy, kRayIz, kRayDlen, kRayBest, kRayBestRef, kRayI,
   kRayEn, kRayCell, kRayRow, kRayFields
 };
-constexpr int kLaneRayCols = 2 * kTraceThreads;  // columns for K = 2 rays per lane
-
+template <int kCols>
 __device__ __forceinline__ void lane_ray_load(const uint32_t* R, int c, Tracer& T)
 {
-  T.o = f3(__uint_as_float(R[kRayOx * kLaneRayCols + c]), __uint_as_float(R[kRayOy * kLaneRayCols + c]),
-           __uint_as_float(R[kRayOz * kLaneRayCols + c]));
-  T.dir = f3(__uint_as_float(R[kRayDx * kLaneRayCols + c]), __uint_as_float(R[kRayDy * kLaneRayCols + c]),
-             __uint_as_float(R[kRayDz * kLaneRayCols + c]));
-  T.inv = f3(__uint_as_float(R[kRayIx * kLaneRayCols + c]), __uint_as_float(R[kRayIy * kLaneRayCols + c]),
-             __uint_as_float(R[kRayIz * kLaneRayCols + c]));
-  T.dlen = __uint_as_float(R[kRayDlen * kLaneRayCols + c]);
-  T.best = __uint_as_float(R[kRayBest * kLaneRayCols + c]);
-  T.best_ref = (int)R[kRayBestRef * kLaneRayCols + c];
-  T.i = R[kRayI * kLaneRayCols + c];
-  T.en = R[kRayEn * kLaneRayCols + c];
-  const uint32_t cell = R[kRayCell * kLaneRayCols + c];
+  T.o = f3(__uint_as_float(R[kRayOx * kCols + c]), __uint_as_float(R[kRayOy * kCols + c]),
+           __uint_as_float(R[kRayOz * kCols + c]));
+  T.dir = f3(__uint_as_float(R[kRayDx * kCols + c]), __uint_as_float(R[kRayDy * kCols + c]),
+             __uint_as_float(R[kRayDz * kCols + c]));
+  T.inv = f3(__uint_as_float(R[kRayIx * kCols + c]), __uint_as_float(R[kRayIy * kCols + c]),
+             __uint_as_float(R[kRayIz * kCols + c]));
+  T.dlen = __uint_as_float(R[kRayDlen * kCols + c]);
+  T.best = __uint_as_float(R[kRayBest * kCols + c]);
+  T.best_ref = (int)R[kRayBestRef * kCols + c];
+  T.i = R[kRayI * kCols + c];
+  T.en = R[kRayEn * kCols + c];
+  const uint32_t cell = R[kRayCell * kCols + c];
   T.cx = (int)(cell & 0xFFu);
   T.cy = (int)((cell >> 8) & 0xFFu);
   T.cz = (int)((cell >> 16) & 0xFFu);
@@ -314,35 +315,38 @@ __device__ __forceinline__ void lane_ray_load(const uint32_t* R, int c, Tracer& 
   T.sz = sgn(T.dir.z);
 }
 
+template <int kCols>
 __device__ __forceinline__ void lane_ray_store_cell(uint32_t* R, int c, const Tracer& T)
 {
-  R[kRayI * kLaneRayCols + c] = T.i;
-  R[kRayEn * kLaneRayCols + c] = T.en;
-  R[kRayCell * kLaneRayCols + c] =
+  R[kRayI * kCols + c] = T.i;
+  R[kRayEn * kCols + c] = T.en;
+  R[kRayCell * kCols + c] =
       (uint32_t)T.cx | ((uint32_t)T.cy << 8) | ((uint32_t)T.cz << 16) | ((uint32_t)T.jump << 24);
 }
 
+template <int kCols>
 __device__ __forceinline__ void lane_ray_store_test(uint32_t* R, int c, const Tracer& T)
 {
-  R[kRayBest * kLaneRayCols + c] = __float_as_uint(T.best);
-  R[kRayBestRef * kLaneRayCols + c] = (uint32_t)T.best_ref;
-  R[kRayI * kLaneRayCols + c] = T.i;
+  R[kRayBest * kCols + c] = __float_as_uint(T.best);
+  R[kRayBestRef * kCols + c] = (uint32_t)T.best_ref;
+  R[kRayI * kCols + c] = T.i;
 }
 
+template <int kCols>
 __device__ __forceinline__ void lane_ray_store(uint32_t* R, int c, const Tracer& T)
 {
-  R[kRayOx * kLaneRayCols + c] = __float_as_uint(T.o.x);
-  R[kRayOy * kLaneRayCols + c] = __float_as_uint(T.o.y);
-  R[kRayOz * kLaneRayCols + c] = __float_as_uint(T.o.z);
-  R[kRayDx * kLaneRayCols + c] = __float_as_uint(T.dir.x);
-  R[kRayDy * kLaneRayCols + c] = __float_as_uint(T.dir.y);
-  R[kRayDz * kLaneRayCols + c] = __float_as_uint(T.dir.z);
-  R[kRayIx * kLaneRayCols + c] = __float_as_uint(T.inv.x);
-  R[kRayIy * kLaneRayCols + c] = __float_as_uint(T.inv.y);
-  R[kRayIz * kLaneRayCols + c] = __float_as_uint(T.inv.z);
-  R[kRayDlen * kLaneRayCols + c] = __float_as_uint(T.dlen);
-  lane_ray_store_test(R, c, T);
-  lane_ray_store_cell(R, c, T);
+  R[kRayOx * kCols + c] = __float_as_uint(T.o.x);
+  R[kRayOy * kCols + c] = __float_as_uint(T.o.y);
+  R[kRayOz * kCols + c] = __float_as_uint(T.o.z);
+  R[kRayDx * kCols + c] = __float_as_uint(T.dir.x);
+  R[kRayDy * kCols + c] = __float_as_uint(T.dir.y);
+  R[kRayDz * kCols + c] = __float_as_uint(T.dir.z);
+  R[kRayIx * kCols + c] = __float_as_uint(T.inv.x);
+  R[kRayIy * kCols + c] = __float_as_uint(T.inv.y);
+  R[kRayIz * kCols + c] = __float_as_uint(T.inv.z);
+  R[kRayDlen * kCols + c] = __float_as_uint(T.dlen);
+  lane_ray_store_test<kCols>(R, c, T);
+  lane_ray_store_cell<kCols>(R, c, T);
 }
 
 template <bool kSkip, bool kStats, bool kHash, bool kPower = false, int kShape = 0>
@@ -385,7 +389,7 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
   if constexpr (kS.lanes > 0) {
     // ---- K rays per lane in shared memory, one body per iteration ----
     constexpr int K = kS.lanes;
-    static_assert(K * kTraceThreads <= kLaneRayCols, "lane ray columns");
+    constexpr int kCols = K * kTraceThreads;
     uint32_t* const R = s_rays;
     // the fields of slot k of this lane: column (warp * K + k) * 32 + lane,
     // so that the 32 lanes of a warp always hit 32 different banks
@@ -440,8 +444,8 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
             while (k < K - 1 && ((ph >> (2 * k)) & 3u) != 0u)
               ++k;
             const int c = col0 + 32 * k;
-            lane_ray_store(R, c, T);
-            R[kRayRow * kLaneRayCols + c] = (uint32_t)(kPower ? 2 * c_face + (j >= c_front ? 1 : 0) : c_row);
+            lane_ray_store<kCols>(R, c, T);
+            R[kRayRow * kCols + c] = (uint32_t)(kPower ? 2 * c_face + (j >= c_front ? 1 : 0) : c_row);
             ph |= (T.i < T.en ? 2u : 1u) << (2 * k);
           }
         }
@@ -468,14 +472,14 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
           ++k;
         const int c = col0 + 32 * k;
         Tracer T;
-        lane_ray_load(R, c, T);
+        lane_ray_load<kCols>(R, c, T);
         uint32_t s;
         if (do_test) {
 #pragma unroll
           for (int t = 0; t < kS.test; ++t)
             if (T.i < T.en)
               tracer_test(T, S.g, n_tests);
-          lane_ray_store_test(R, c, T);
+          lane_ray_store_test<kCols>(R, c, T);
           s = T.i < T.en ? 2u : 1u;
         } else {
           bool live = true;
@@ -485,10 +489,10 @@ __global__ void __launch_bounds__(kTraceThreads, trace_shape(kShape).blocks)
               live = tracer_advance<kSkip>(T, S.g, n_cells, n_jumps);
           if (!live) {
             hit = tracer_result(T, S.g);
-            row = (int)R[kRayRow * kLaneRayCols + c];
+            row = (int)R[kRayRow * kCols + c];
             s = 0u;
           } else {
-            lane_ray_store_cell(R, c, T);
+            lane_ray_store_cell<kCols>(R, c, T);
             s = T.i < T.en ? 2u : 1u;
           }
         }
