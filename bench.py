@@ -70,6 +70,8 @@ def parse():
                          "(a small command for profiling the grid-build kernels)")
     ap.add_argument("--served-requests", type=int, default=256)
     ap.add_argument("--served-slots", type=int, default=16, help="requests prepared and traced at once")
+    ap.add_argument("--served-max-wait", type=float, default=30.0,
+                    help="age limit of the shortest-first served run, s (0: skip that run)")
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--served-sub-rate", type=float, default=0.5,
                     help="arrival rate of the sub-saturation run, requests/s (0: skip it)")
@@ -409,8 +411,10 @@ def served_section(args, ctx, stream):
     arrivals = np.cumsum(gaps)
     rays = sum(len(f) * r for f, r, _ in reqs)
 
-    def served(slots, arrivals, reqs):
+    def served(slots, arrivals, reqs, shortest_first=False):
         server = native.Server(0, budget_bytes=int(80e9), slots=slots)
+        if shortest_first:
+            server.set_admission(shortest_first=True, max_wait_s=args.served_max_wait)
         t0 = time.perf_counter()
         ids = []
         for (f, r, sd), at in zip(reqs, arrivals):
@@ -462,6 +466,14 @@ def served_section(args, ctx, stream):
     tune_s = time.perf_counter() - t0
     plain_wall, plain_lat, plain_trace = plain(arrivals, reqs)
     served_wall, lat, st, spans, slices = served(args.served_slots, arrivals, reqs)
+    sjf = None
+    if args.served_max_wait > 0:
+        sjf_wall, sjf_lat, _, _, _ = served(args.served_slots, arrivals, reqs, shortest_first=True)
+        sjf = {"admission": "least work first, the oldest first after %.0f s of waiting" % args.served_max_wait,
+               "scenes_per_s": n / sjf_wall, "speedup_scenes_per_s": plain_wall / sjf_wall,
+               "p50_latency_s": float(np.percentile(sjf_lat, 50)),
+               "p99_latency_s": float(np.percentile(sjf_lat, 99)),
+               "mean_latency_s": float(sjf_lat.mean()), "wall_s": sjf_wall}
     # device overlap: pairs of requests whose trace spans intersect
     ordered = sorted((a, b) for a, b in spans if b > a)
     overlaps = sum(1 for i in range(1, len(ordered)) if ordered[i][0] < max(e for _, e in ordered[:i]))
@@ -499,6 +511,8 @@ def served_section(args, ctx, stream):
             "peak_tracing": int(st.peak_tracing), "trace_slices": int(sum(slices)),
             "requests_overlapping_on_device": int(overlaps),
             "note": "offered load far above capacity: latency is queueing under saturation",
+            "mean_latency_s": float(lat.mean()), "plain_mean_latency_s": float(plain_lat.mean()),
+            "shortest_first": sjf,
             "autotune_warmup_s": tune_s,
             "sub_saturation": sub}
 
@@ -974,6 +988,10 @@ def ours(args):
             summary["served_p50_s"] = served["p50_latency_s"]
             summary["served_p99_s"] = served["p99_latency_s"]
             summary["served_ceiling"] = served.get("ceiling")
+            if served.get("shortest_first"):
+                summary["served_shortest_first_p50_s"] = served["shortest_first"]["p50_latency_s"]
+                summary["served_shortest_first_vs_plain"] = served["shortest_first"]["speedup_scenes_per_s"]
+            summary["plain_p50_s"] = served["plain_p50_latency_s"]
         line["summary"] = summary
         print(json.dumps(line))
     ctx.close()

@@ -121,6 +121,8 @@ struct ffb_server {
   int peak_tracing = 0;  // most requests in the trace rotation at once
   long long slice_chunks = kSliceRays / kChunkRays;
   int window = kWindow;
+  int policy = FFB_ADMIT_FIFO;  // admission order (ffb_server_set_admission)
+  double max_wait_s = 0.0;      // FFB_ADMIT_SHORTEST: age past which the oldest request goes first
   // frees of released matrices, off every slot's stream: a synchronous
   // cudaFree would wait for the whole device and drain the slice pipeline
   cudaStream_t free_stream = nullptr;
@@ -136,6 +138,34 @@ unsigned long long estimate_bytes(int n_faces, bool tuned)
 {
   const unsigned long long n = (unsigned long long)n_faces;
   return 4ull * n * n + (tuned ? 10240ull : 1536ull) * n + (8ull << 20);
+}
+
+// Position in the queue of the request to admit next, or -1 when none may
+// enter yet.  FIFO: the oldest, once its reservation fits the budget (no
+// overtaking, so a large request cannot be starved by a stream of small
+// ones).  Shortest first: the request with the least work (faces x rays per
+// face), unless the oldest has waited longer than max_wait_s, which then
+// goes first: starvation is bounded by the age limit.
+long admission_pick(const ffb_server* s)
+{
+  if (s->queue.empty())
+    return -1;
+  size_t idx = 0;
+  if (s->policy == FFB_ADMIT_SHORTEST && secs(s->queue.front()->t_submit, Clock::now()) <= s->max_wait_s) {
+    unsigned long long best = ~0ull;
+    for (size_t i = 0; i < s->queue.size(); ++i) {
+      const Request& q = *s->queue[i];
+      const unsigned long long work = (unsigned long long)q.n_faces * (unsigned long long)q.rays_per_face;
+      if (work < best) {
+        best = work;
+        idx = i;
+      }
+    }
+  }
+  const Request& r = *s->queue[idx];
+  if (s->budget && s->reserved + r.reserve > s->budget)
+    return -1;
+  return (long)idx;
 }
 
 // The worker's part of a request before its trace: scene, grid, matrix,
@@ -214,17 +244,12 @@ void worker_main(ffb_server* s, int slot)
     std::shared_ptr<Request> r;
     {
       std::unique_lock<std::mutex> lock(s->mu);
-      // admission in arrival order: the oldest queued request enters as soon
-      // as its reservation fits the budget (no overtaking, so a large request
-      // cannot be starved by a stream of small ones)
-      s->cv_work.wait(lock, [&] {
-        return s->stopping ||
-               (!s->queue.empty() && (s->budget == 0 || s->reserved + s->queue.front()->reserve <= s->budget));
-      });
+      long pick = -1;
+      s->cv_work.wait(lock, [&] { return s->stopping || (pick = admission_pick(s)) >= 0; });
       if (s->stopping)
         break;
-      r = s->queue.front();
-      s->queue.pop_front();
+      r = s->queue[(size_t)pick];
+      s->queue.erase(s->queue.begin() + pick);
       s->reserved += r->reserve;
       r->state = FFB_REQ_RUNNING;
       r->t_admit = Clock::now();
@@ -580,6 +605,19 @@ extern "C" int ffb_server_set_slicing(ffb_server* s, long long slice_rays, int w
   std::lock_guard<std::mutex> lock(s->mu);
   s->slice_chunks = slice_rays / kChunkRays;
   s->window = window;
+  return FFB_OK;
+}
+
+extern "C" int ffb_server_set_admission(ffb_server* s, int policy, double max_wait_s)
+{
+  if (!s || (policy != FFB_ADMIT_FIFO && policy != FFB_ADMIT_SHORTEST) || !(max_wait_s >= 0.0))
+    return ffb_set_error(FFB_ERR_ARG, "ffb_server_set_admission: FFB_ADMIT_FIFO or FFB_ADMIT_SHORTEST, max_wait_s >= 0");
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->policy = policy;
+    s->max_wait_s = max_wait_s;
+  }
+  s->cv_work.notify_all();
   return FFB_OK;
 }
 

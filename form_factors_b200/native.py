@@ -193,6 +193,7 @@ def load(path=LIB_PATH):
         "ffb_server_release": (i32, [vp, C.c_longlong]),
         "ffb_server_stats": (i32, [vp, C.POINTER(ServerInfo)]),
         "ffb_server_set_slicing": (i32, [vp, C.c_longlong, i32]),
+        "ffb_server_set_admission": (i32, [vp, i32, C.c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -701,6 +702,12 @@ class Server:
     def set_slicing(self, slice_rays, window=2):
         """Rays per trace slice and slices in flight (ffb_server_set_slicing)."""
         _check(self._lib.ffb_server_set_slicing(self._h, int(slice_rays), int(window)))
+
+    def set_admission(self, shortest_first=False, max_wait_s=0.0):
+        """Admission order (ffb_server_set_admission): arrival order, or the
+        least work first with the oldest request first once it has waited
+        max_wait_s."""
+        _check(self._lib.ffb_server_set_admission(self._h, 1 if shortest_first else 0, float(max_wait_s)))
 
     def release(self, rid):
         _check(self._lib.ffb_server_release(self._h, int(rid)))

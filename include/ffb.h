@@ -258,6 +258,13 @@ int ffb_server_stats(ffb_server* server, ffb_server_info* out);
  * 64 Mi, rounded down to whole 256-ray chunks) and `window` slices in flight
  * (default 2, at most 8).  Applies to the slices launched after the call. */
 int ffb_server_set_slicing(ffb_server* server, long long slice_rays, int window);
+/* Admission order.  FFB_ADMIT_FIFO (default): arrival order, no overtaking.
+ * FFB_ADMIT_SHORTEST: the queued request with the least work (faces x rays
+ * per face) first, unless the oldest queued request has waited longer than
+ * max_wait_s, which then goes first (starvation bounded by the age limit). */
+#define FFB_ADMIT_FIFO 0
+#define FFB_ADMIT_SHORTEST 1
+int ffb_server_set_admission(ffb_server* server, int policy, double max_wait_s);
 
 /* One step of the radiance equation (thermal_equation/radiance_cpu.cpp:96-190)
  * on the resident scene and grid: every face emits front[f] + rear[f] Malley

@@ -84,3 +84,33 @@ def test_traces_of_requests_overlap_on_the_device(ctx):
         assert np.array_equal(server.result(rid, n), want)
         server.release(rid)
     server.close()
+
+
+def test_shortest_first_admission_and_its_age_limit(ctx):
+    """One slot; a large request, a second large one, then two small ones.
+    Shortest-first admits the small ones before the second large request;
+    with an age limit of zero the oldest request always goes first, which is
+    arrival order.  Results are those of the same solve alone."""
+    big = scenes.icosphere(4, 1.0, inward=True)  # 5 120 faces
+    small = scenes.parallel_plates(4, 1.0)       # 32 faces
+    for shortest, limit in ((True, 600.0), (True, 0.0), (False, 0.0)):
+        server = native.Server(0, budget_bytes=0, slots=1)
+        server.set_admission(shortest_first=shortest, max_wait_s=limit)
+        ids = [server.submit(big, 2000, 1), server.submit(big, 2000, 2), server.submit(small, 100, 3),
+               server.submit(small, 100, 4)]
+        infos = [server.wait(i, timeout_s=300) for i in ids]
+        assert all(inf.state == 2 for inf in infos)
+        q = [inf.queue_s for inf in infos]
+        if shortest and limit > 0:
+            assert q[2] < q[1] and q[3] < q[1], q  # the small requests overtake the second large one
+        else:
+            assert q[1] < q[2] < q[3], q           # arrival order
+        got = server.result(ids[2], len(small))
+        ctx.scene_set(small)
+        ctx.grid_build(cells_per_face=32)
+        want = ctx.form_factor_counts(np.full(len(small), 100, np.int32), np.zeros(len(small), np.int32), seed=3,
+                                      epoch=0)
+        assert np.array_equal(got, want)
+        for i in ids:
+            server.release(i)
+        server.close()
