@@ -540,6 +540,39 @@ extern "C" int ffb_server_wait(ffb_server* s, long long id, double timeout_s, ff
   return done() ? FFB_OK : ffb_set_error(FFB_ERR_TIMEOUT, "request not finished before the timeout");
 }
 
+extern "C" int ffb_server_wait_any(ffb_server* s, const long long* ids, int n, double timeout_s, long long* done_id,
+                                   ffb_request_info* info)
+{
+  if (!s || !ids || n <= 0 || !done_id)
+    return ffb_set_error(FFB_ERR_ARG, "ffb_server_wait_any: bad arguments");
+  long long found = -1;
+  {
+    std::unique_lock<std::mutex> lock(s->mu);
+    for (int k = 0; k < n; ++k)
+      if (s->all.find(ids[k]) == s->all.end())
+        return ffb_set_error(FFB_ERR_ARG, "ffb_server_wait_any: unknown request");
+    auto any_done = [&] {
+      for (int k = 0; k < n; ++k) {
+        auto it = s->all.find(ids[k]);
+        // a request released meanwhile ends the wait (ffb_server_wait then reports it unknown)
+        if (it == s->all.end() || it->second->state == FFB_REQ_DONE || it->second->state == FFB_REQ_FAILED) {
+          found = ids[k];
+          return true;
+        }
+      }
+      return false;
+    };
+    if (timeout_s < 0)
+      s->cv_done.wait(lock, any_done);
+    else
+      s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), any_done);
+  }
+  if (found < 0)
+    return ffb_set_error(FFB_ERR_TIMEOUT, "no request finished before the timeout");
+  *done_id = found;
+  return ffb_server_wait(s, found, 0.0, info);
+}
+
 extern "C" int ffb_server_result(ffb_server* s, long long id, uint32_t* counts)
 {
   if (!s || !counts)

@@ -194,6 +194,7 @@ def load(path=LIB_PATH):
         "ffb_server_stats": (i32, [vp, C.POINTER(ServerInfo)]),
         "ffb_server_set_slicing": (i32, [vp, C.c_longlong, i32]),
         "ffb_server_set_admission": (i32, [vp, i32, C.c_double]),
+        "ffb_server_wait_any": (i32, [vp, vp, i32, C.c_double, C.POINTER(C.c_longlong), C.POINTER(RequestInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -692,6 +693,15 @@ class Server:
         info = RequestInfo()
         _check(self._lib.ffb_server_wait(self._h, int(rid), float(timeout_s), C.byref(info)))
         return info
+
+    def wait_any(self, rids, timeout_s=-1.0):
+        """(request id, RequestInfo) of the first of `rids` to finish."""
+        arr = np.ascontiguousarray(rids, np.int64)
+        done = C.c_longlong()
+        info = RequestInfo()
+        _check(self._lib.ffb_server_wait_any(self._h, _ptr(arr), len(arr), float(timeout_s), C.byref(done),
+                                             C.byref(info)))
+        return done.value, info
 
     def result(self, rid, n_faces, out=None):
         if out is None:

@@ -249,6 +249,15 @@ int ffb_server_submit(ffb_server* server, const float* faces9, int n_faces, int 
 /* Waits for a request (timeout_s < 0: no limit); FFB_ERR_TIMEOUT if it is
  * still queued or running when the time is up. */
 int ffb_server_wait(ffb_server* server, long long request_id, double timeout_s, ffb_request_info* info);
+/* Waits until one of the n requests `ids` has finished (timeout_s < 0: no
+ * limit) and reports it in *done_id and *info, as ffb_server_wait does.  A
+ * client that consumes results in completion order -- and releases each --
+ * keeps the budget free for the requests still queued: a finished result
+ * keeps its reservation until released, so a client that holds finished
+ * results while it waits for a request that has not been admitted can leave
+ * that request no room. */
+int ffb_server_wait_any(ffb_server* server, const long long* ids, int n, double timeout_s, long long* done_id,
+                        ffb_request_info* info);
 /* Copies a finished request's counts (host or device, N*N uint32). */
 int ffb_server_result(ffb_server* server, long long request_id, uint32_t* counts);
 /* Frees a finished request's resident matrix and its budget reservation. */

@@ -98,9 +98,21 @@ def test_shortest_first_admission_and_its_age_limit(ctx):
         server.set_admission(shortest_first=shortest, max_wait_s=limit)
         ids = [server.submit(big, 2000, 1), server.submit(big, 2000, 2), server.submit(small, 100, 3),
                server.submit(small, 100, 4)]
-        infos = [server.wait(i, timeout_s=300) for i in ids]
+        # collected in completion order (ffb_server_wait_any)
+        order, infos_by = [], {}
+        pending = list(ids)
+        while pending:
+            rid, inf = server.wait_any(pending, timeout_s=300)
+            order.append(rid)
+            infos_by[rid] = inf
+            pending.remove(rid)
+        infos = [infos_by[i] for i in ids]
         assert all(inf.state == 2 for inf in infos)
         q = [inf.queue_s for inf in infos]
+        if shortest and limit > 0:
+            assert order.index(ids[2]) < order.index(ids[1]) and order.index(ids[3]) < order.index(ids[1]), order
+        else:
+            assert order == ids, order
         if shortest and limit > 0:
             assert q[2] < q[1] and q[3] < q[1], q  # the small requests overtake the second large one
         else:
