@@ -517,8 +517,8 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
     k_empty_init<<<grid_blocks(n_cells, 256), 256, 0, c->stream>>>(dptr<uint32_t>(s.cell_start), (int)n_cells, d);
     const long long lines[3] = {(long long)I.ny * I.nz, (long long)I.nx * I.nz, (long long)I.nx * I.ny};
     for (int axis = 0; axis < 3; ++axis)
-      k_empty_pass_warp<<<dim3(grid_blocks(lines[axis], kEmptyWarps), 1u << axis), 32 * kEmptyWarps, 0,
-                          c->stream>>>(d, n_cells, I.nx, I.ny, I.nz, axis);
+      k_empty_pass<<<dim3(grid_blocks(lines[axis], 128), 1u << axis), 128, 0, c->stream>>>(d, n_cells, I.nx, I.ny,
+                                                                                         I.nz, axis);
     FFB_CUDA(cudaGetLastError());
   }
   FFB_TRY(ensure(c, s.cell_rec, sizeof(uint2) * (size_t)n_cells));
@@ -1789,7 +1789,7 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
                                 (int)csv::write_smem(csv::kTileBytes)));
   src.n_entries = (long long)src.n * src.n;
   const long long n_tiles = (src.n_entries + csv::kTile - 1) / csv::kTile;
-  const long long n_fused = (src.n_entries + csv::kWarpTile - 1) / csv::kWarpTile;  // one warp per tile
+  const long long n_fused = (src.n_entries + csv::kFusedTile - 1) / csv::kFusedTile;
   FFB_TRY(ensure(c, c->csv_tile_len, sizeof(unsigned long long) * (size_t)std::max(n_tiles, n_fused)));
   FFB_TRY(ensure(c, c->csv_tile_off, sizeof(unsigned long long) * (size_t)(n_tiles + 2)));
   auto* tile_len = dptr<unsigned long long>(c->csv_tile_len);
@@ -1797,9 +1797,11 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
   bool text_dev = false;
   FFB_TRY(ptr_kind(c, text, &text_dev));
   if (text_dev) {
-    // one pass, one warp per 512-entry tile: the tile-length buffer holds
-    // the look-back status words; the first two words of the offset buffer
-    // the ticket and error bits, then the total
+    // one pass: the tile-length buffer holds the look-back status words; the
+    // first two words of the offset buffer the ticket and error bits, then
+    // the total
+    FFB_CUDA(cudaFuncSetAttribute(csv::k_csv_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)csv::kFusedSmem));
     FFB_CUDA(cudaMemsetAsync(tile_len, 0, sizeof(unsigned long long) * (size_t)n_fused, c->stream));
     FFB_CUDA(cudaMemsetAsync(tile_off, 0, 2 * sizeof(unsigned long long), c->stream));
     csv::FusedSink sink;
@@ -1810,8 +1812,7 @@ int csv_run(ffb_ctx* c, csv::Source src, char* text, unsigned long long cap, FIL
     sink.err = reinterpret_cast<unsigned int*>(tile_off) + 1;
     sink.total = tile_off + 1;
     sink.n_tiles = n_fused;
-    csv::k_csv_warp<<<(unsigned)((n_fused + csv::kWarpTileWarps - 1) / csv::kWarpTileWarps), csv::kWarpTileThreads,
-                      0, c->stream>>>(src, sink);
+    csv::k_csv_fused<<<(unsigned)n_fused, csv::kFusedThreads, csv::kFusedSmem, c->stream>>>(src, sink);
     FFB_CUDA(cudaGetLastError());
     unsigned long long aux[2] = {0, 0};  // {ticket | err << 32, total}
     FFB_CUDA(cudaMemcpyAsync(aux, tile_off, sizeof aux, cudaMemcpyDeviceToHost, c->stream));

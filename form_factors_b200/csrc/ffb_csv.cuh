@@ -891,202 +891,6 @@ __global__ void __launch_bounds__(kFusedThreads, FFB_CSV_BLOCKS) k_csv_fused(Sou
   for (uint32_t i = head + 16u * body + threadIdx.x; i < total; i += kFusedThreads)
     dst[i] = (char)sbuf[i];
 }
-
-// Value and column of entry o of a warp tile (queue work, one division).
-__device__ __forceinline__ float fused_warp_value(const Source& s, long long tile, int o, int* col)
-{
-  const long long e = tile * (32 * 16) + o;
-  const int row = (int)(e / s.n);
-  *col = (int)(e - (long long)row * s.n);
-  return entry_value(s, e, row_ratio(s, row));
-}
-
-// Writes a warp tile's text to `base` (the warp's stage in shared memory, or
-// the buffer itself): each lane its run's +0 entries, then the nonzero
-// entries of the queue formatted by all lanes.  `before` is the lane's run
-// offset; run_len its entry lengths, four per word.
-template <class Area>
-__device__ __forceinline__ void warp_tile_text(const Source& s, long long tile, unsigned char* base, const Area& W,
-                                               int lane, uint32_t before, uint32_t zero_mask, uint32_t end_mask,
-                                               const uint32_t* run_len, uint32_t n_q)
-{
-  __syncwarp();  // every lane's run offset (W.toff) is in place
-  uint32_t pos = before;
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    if ((zero_mask >> k) & 1u) {
-      base[pos] = '0';
-      base[pos + 1] = ((end_mask >> k) & 1u) ? '\n' : ';';
-    }
-    pos += (run_len[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-  }
-  for (uint32_t q = lane; q < n_q; q += 32) {
-    const int o = W.queue[q];
-    const int t = o >> 4;
-    uint32_t at = W.toff[t];
-    for (int j = t * 16; j < o; ++j)
-      at += W.len[j];
-    int c;
-    const float v = fused_warp_value(s, tile, o, &c);
-    PtrOut w{reinterpret_cast<char*>(base + at), 0};
-    format_g6_to(v, w);
-    w.put(c == s.n - 1 ? '\n' : ';');
-  }
-  __syncwarp();
-}
-
-// ---------------------------------------------------------------------------
-// Single pass into a device buffer, one warp per tile (k_csv_warp).  The
-// same text as k_csv_fused, with the tile cut to one warp's 512 entries so
-// that no phase waits at a block barrier: lane t holds entries
-// [16t, 16t + 16) of the tile; the nonzero entries go to a warp queue
-// (ballots) and are measured and formatted by all lanes together; a warp scan
-// of the 16-entry run lengths gives each run's offset; the tile publishes its
-// length, stages its text in the warp's shared memory (when it fits
-// kWarpStage bytes, as every tile of a sparse matrix does) and finds its
-// place by decoupled look-back over the tiles before it (bounded polls; a
-// timeout sets kFusedTimeout).  A tile whose text does not fit the stage
-// writes it straight to the buffer once its offset is known.  Tiles are
-// taken by ticket, so a warp waits only for tiles already running.
-// ---------------------------------------------------------------------------
-constexpr int kWarpRun = 16;                      // consecutive entries per lane
-constexpr int kWarpTile = 32 * kWarpRun;          // entries per warp tile
-constexpr int kWarpStage = kWarpTile * 5;         // staged text per warp (5 B per entry on average)
-constexpr int kWarpTileWarps = 4;                 // warps per block
-constexpr int kWarpTileThreads = 32 * kWarpTileWarps;
-struct WarpTileSmem {
-  unsigned char text[kWarpStage + 16];  // + one word read past the end by the copy
-  uint8_t len[kWarpTile];               // entry lengths with separator, run by run
-  uint16_t queue[kWarpTile];            // nonzero entries
-  uint32_t toff[32];                    // staged offset of each lane's run
-};
-static_assert(sizeof(WarpTileSmem) % 16 == 0, "16-byte aligned per-warp areas");
-
-__global__ void __launch_bounds__(kWarpTileThreads, 8) k_csv_warp(Source s, FusedSink out)
-{
-  __shared__ __align__(16) WarpTileSmem area[kWarpTileWarps];
-  const int lane = threadIdx.x & 31;
-  WarpTileSmem& W = area[threadIdx.x >> 5];
-  const unsigned below = (1u << lane) - 1u;
-  long long tile = 0;
-  if (lane == 0)
-    tile = (long long)atomicAdd(out.ticket, 1u);
-  tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-  if (tile >= out.n_tiles)
-    return;
-  // 1. the lane's run: values, +0 / row-end flags, +0 lengths, the queue
-  const int o0 = kWarpRun * lane;
-  const long long e0 = tile * kWarpTile + o0;
-  const uint32_t* words = s.ff ? reinterpret_cast<const uint32_t*>(s.ff) : s.counts;
-  uint32_t raw[kWarpRun];
-  if (e0 + kWarpRun <= s.n_entries && ((uintptr_t)(words + e0) & 15u) == 0) {
-    const uint4* p = reinterpret_cast<const uint4*>(words + e0);
-#pragma unroll
-    for (int j = 0; j < kWarpRun / 4; ++j) {
-      const uint4 w = __ldg(p + j);
-      raw[4 * j] = w.x;
-      raw[4 * j + 1] = w.y;
-      raw[4 * j + 2] = w.z;
-      raw[4 * j + 3] = w.w;
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < kWarpRun; ++k)
-      raw[k] = e0 + k < s.n_entries ? __ldg(words + e0 + k) : 0u;
-  }
-  int row = (int)(e0 / s.n), col = (int)(e0 - (long long)row * s.n);
-  float ratio = (!s.ff && row < s.n) ? row_ratio(s, row) : 1.f;
-  uint32_t zero_mask = 0, end_mask = 0, valid_mask = 0, lens[kWarpRun / 4] = {0u, 0u, 0u, 0u};
-  uint32_t n_q = 0;
-#pragma unroll
-  for (int k = 0; k < kWarpRun; ++k) {
-    const bool valid = e0 + k < s.n_entries;
-    const float v = s.ff ? __uint_as_float(raw[k]) : (float)raw[k] * ratio;
-    const bool zero = valid && __float_as_uint(v) == 0u;
-    valid_mask |= valid ? 1u << k : 0u;
-    zero_mask |= zero ? 1u << k : 0u;
-    end_mask |= col == s.n - 1 ? 1u << k : 0u;
-    lens[k >> 2] |= zero ? 2u << (8 * (k & 3)) : 0u;
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, valid && !zero);
-    if (valid && !zero)
-      W.queue[n_q + __popc(m & below)] = (uint16_t)(o0 + k);
-    n_q += __popc(m);
-    if (++col == s.n) {
-      col = 0;
-      ++row;
-      if (!s.ff && row < s.n)
-        ratio = row_ratio(s, row);
-    }
-  }
-  *reinterpret_cast<uint4*>(W.len + o0) = make_uint4(lens[0], lens[1], lens[2], lens[3]);
-  __syncwarp();
-  for (uint32_t q = lane; q < n_q; q += 32) {
-    const int o = W.queue[q];
-    int c;
-    W.len[o] = (uint8_t)(format_g6_len(fused_warp_value(s, tile, o, &c)) + 1);
-  }
-  __syncwarp();
-  // 2. run lengths, the tile's length and each run's offset in the tile
-  const uint4 lw = *reinterpret_cast<const uint4*>(W.len + o0);
-  const uint32_t run_len[4] = {lw.x, lw.y, lw.z, lw.w};
-  const uint32_t mine = __dp4a(lw.x, 0x01010101u, __dp4a(lw.y, 0x01010101u, __dp4a(lw.z, 0x01010101u,
-                                                                                  __dp4a(lw.w, 0x01010101u, 0u))));
-  uint32_t incl = mine;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-    if (lane >= d)
-      incl += y;
-  }
-  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  const uint32_t before = incl - mine;
-  W.toff[lane] = before;
-  // 3. publish the tile's length; stage its text while the tiles before it finish
-  if (lane == 0)
-    st_relaxed(out.status + tile, (tile == 0 ? kTilePrefix : kTileAgg) | total);
-  const bool staged = total <= (uint32_t)kWarpStage;
-  if (staged)
-    warp_tile_text(s, tile, W.text, W, lane, before, zero_mask, end_mask, run_len, n_q);
-  // 4. the tile's place in the text
-  unsigned long long excl = 0;
-  if (tile > 0) {
-    excl = look_back(out, tile, lane);
-    if (lane == 0)
-      st_relaxed(out.status + tile, kTilePrefix | (excl + total));
-  }
-  if (lane == 0 && tile == out.n_tiles - 1)
-    *out.total = excl + total;
-  if (excl + total > out.cap) {
-    if (lane == 0)
-      atomicOr(out.err, kFusedOverflow);
-    return;
-  }
-  char* dst = out.text + excl;
-  if (!staged) {
-    // a dense tile: its text goes straight to the buffer
-    warp_tile_text(s, tile, reinterpret_cast<unsigned char*>(dst), W, lane, before, zero_mask, end_mask, run_len,
-                   n_q);
-    return;
-  }
-  // 5. copy the staged text: bytes up to the first 16-byte boundary, then
-  // 16-byte stores assembled from 32-bit shared words, then the tail
-  const uint32_t head = min(total, (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u));
-  const uint32_t body = (total - head) >> 4;
-  for (uint32_t i = lane; i < head; i += 32)
-    dst[i] = (char)W.text[i];
-  const uint32_t r8 = 8u * (head & 3u);
-  const uint32_t* sw = reinterpret_cast<const uint32_t*>(W.text) + (head >> 2);
-  uint4* dv = reinterpret_cast<uint4*>(dst + head);
-  for (uint32_t i = lane; i < body; i += 32) {
-    const uint32_t* w = sw + 4 * i;
-    const uint32_t a0 = w[0], a1 = w[1], a2 = w[2], a3 = w[3], a4 = w[4];
-    dv[i] = make_uint4(__funnelshift_r(a0, a1, r8), __funnelshift_r(a1, a2, r8), __funnelshift_r(a2, a3, r8),
-                       __funnelshift_r(a3, a4, r8));
-  }
-  for (uint32_t i = head + 16u * body + lane; i < total; i += 32)
-    dst[i] = (char)W.text[i];
-}
-
 #endif  // __CUDACC__
 
 }  // namespace csv

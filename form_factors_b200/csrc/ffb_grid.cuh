@@ -466,52 +466,6 @@ __global__ void k_empty_pass(uint8_t* __restrict__ d, long long n_cells, int nx,
   }
 }
 
-// The same pass with one warp per line: the line is read once into the
-// warp's shared memory, then each lane computes its cells straight from the
-// definition, new[i] = min_{r >= 0} max(r, old[i + r*s]) (positions past the
-// end of the line count as empty), scanning r only while r is below the best
-// value found: at most kEmptyCap steps per cell, and far fewer next to
-// occupied cells.  The result equals k_empty_pass's; this form keeps every
-// SM busy where one thread per line leaves most of the GPU idle (26 244
-// threads for an x pass at 162^3).
-constexpr int kEmptyWarps = 4;  // lines per block
-
-__global__ void __launch_bounds__(32 * kEmptyWarps) k_empty_pass_warp(uint8_t* __restrict__ d, long long n_cells,
-                                                                       int nx, int ny, int nz, int axis)
-{
-  __shared__ uint8_t s_line[kEmptyWarps][kMaxDim];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t = blockIdx.x * kEmptyWarps + w;
-  int n_len, stride, base;
-  if (axis == 0) {
-    if (t >= ny * nz) return;
-    n_len = nx; stride = 1; base = t * nx;
-  } else if (axis == 1) {
-    if (t >= nx * nz) return;
-    const int i = t % nx, k = t / nx;
-    n_len = ny; stride = nx; base = k * nx * ny + i;
-  } else {
-    if (t >= nx * ny) return;
-    n_len = nz; stride = nx * ny; base = t;
-  }
-  uint8_t* in = d + (size_t)blockIdx.y * n_cells;
-  uint8_t* neg = d + (size_t)(blockIdx.y | (1u << axis)) * n_cells;
-  uint8_t* line = s_line[w];
-  for (int i = lane; i < n_len; i += 32)
-    line[i] = in[base + i * stride];
-  __syncwarp();
-  for (int i = lane; i < n_len; i += 32) {
-    // positive direction (written in place) and negative direction
-    int gp = line[i], gn = gp;
-    for (int r = 1; r < gp && i + r < n_len; ++r)
-      gp = min(gp, max(r, (int)line[i + r]));
-    for (int r = 1; r < gn && i - r >= 0; ++r)
-      gn = min(gn, max(r, (int)line[i - r]));
-    in[base + i * stride] = (uint8_t)gp;
-    neg[base + i * stride] = (uint8_t)gn;
-  }
-}
-
 // Packs the cell records: occupied {start, end}; empty {octants 0-3, flag |
 // octants 4-7}, one byte per octant (octant o in byte o & 3).  Without a
 // distance map every octant distance is 1 (single DDA steps).
