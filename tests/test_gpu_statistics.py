@@ -136,16 +136,18 @@ def test_enclosure_rows_sum_to_one(ctx):
 
 def test_config3_clutter_bit_exact_with_autotuned_grid(ctx, oracle):
     """2000 random equilateral triangles (edge 0.05) in a 2028-triangle unit
-    cube, the grid chosen by the autotuner among 32^3..128^3 and cells per
-    face; the counts stay bit-identical to the oracle whatever it picks."""
+    cube, the grid (32^3..128^3) and the kernel's launch shape chosen by the
+    autotuner; the counts stay bit-identical to the oracle whatever it
+    picks."""
     faces = scenes.clutter(2000, 0.05, seed=1, enclosure_cells=13)
     n = len(faces)
     front, rear = emission.front_only(n, 12)
     ctx.scene_set(faces)
-    best = ctx.autotune_grid(front, rear, seed=3,
-                             candidates=[dict(dims=(d, d, d)) for d in (32, 64, 96, 128)], sample_every=4)
-    assert best["dims"][0] in (32, 64, 96, 128)
+    best = ctx.autotune(front, rear, seed=3, candidates=[dict(dims=(d, d, d)) for d in (32, 64, 96, 128)],
+                        sample_every=4, force=True)
+    assert best["dims"][0] in (32, 64, 96, 128) and ctx.trace_shape() == best["shape"]
     got = ctx.form_factor_counts(front, rear, seed=3)
     oracle.set_threads(0)
     want = oracle.form_factor_counts(faces, front, rear, seed=3)
+    ctx.set_trace_shape(0)
     assert np.array_equal(got, want)
