@@ -221,7 +221,8 @@ void finish(ffb_server* s, Slot& sl, const std::shared_ptr<Request>& r, int err,
       r->error = err;
       r->message = msg;
       if (r->counts) {
-        cudaFreeAsync(r->counts, s->free_stream);
+        // after whatever the failed preparation left queued on the slot's stream
+        cudaFreeAsync(r->counts, (cudaStream_t)ffb_ctx_stream(sl.ctx));
         r->counts = nullptr;
       }
       s->reserved -= r->reserve;
