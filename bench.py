@@ -896,6 +896,15 @@ def ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         k_ms = float(t.item())
     tests, cells, hits, jumps = [float(x) for x in work.tolist()]
+    # the zeroing of the count rows alone: a counts call in which no face
+    # emits does only that (its stats time brackets the memset)
+    no_rays = np.zeros_like(front)
+    zms = []
+    for _ in range(3):
+        ctx.form_factor_counts_rows(no_rays, no_rays, SEED, row_b, row_e, epoch=0, out=counts)
+        zms.append(ctx.stats().kernel_ms)
+    zero_ms = statistics.median(zms)
+    zero_bytes = 4 * rows * n
     tests_per_launch = tests
     achieved = tests_per_launch * FLOPS_PER_TEST / (k_ms * 1e-3)
     peak = fp32_peak(local)
@@ -982,6 +991,9 @@ def ours(args):
                          "issue": issue_roofline(k_ms, rays_per_step / world, clk.get("sm_mhz"), shape=timed_shape,
                                                  n_sm=
                                                  torch.cuda.get_device_properties(local).multi_processor_count)},
+            "zeroing": {"ms": zero_ms, "bytes": zero_bytes, "gbs": zero_bytes / (zero_ms * 1e-3) / 1e9,
+                        "frac": zero_bytes / (zero_ms * 1e-3) / 1e9 / measured_hbm_gbs(),
+                        "note": "cudaMemsetAsync of the step's count rows before the trace, CUDA events"},
             "tests_per_ray": tests / rays_per_step, "cells_per_ray": cells / rays_per_step,
             "jumps_per_ray": jumps / rays_per_step,
             "hit_fraction": hits / rays_per_step,

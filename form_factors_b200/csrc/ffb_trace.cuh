@@ -204,7 +204,7 @@ constexpr int kRefillMin = FFB_REFILL_MIN;
 struct TraceShape {
   int adv, test, refill, blocks, coherent, lanes;
 };
-constexpr int kNumShapes = 15;
+constexpr int kNumShapes = 14;
 __host__ __device__ constexpr TraceShape trace_shape(int v)
 {
   return v == 1 ? TraceShape{1, 1, 4, 8, 0, 0}
@@ -219,8 +219,7 @@ __host__ __device__ constexpr TraceShape trace_shape(int v)
        : v == 10 ? TraceShape{2, 2, 8, 8, 1, 2}
        : v == 11 ? TraceShape{2, 2, 8, 8, 0, 3}
        : v == 12 ? TraceShape{2, 3, 8, 8, 0, 2}
-       : v == 13 ? TraceShape{2, 2, 8, 7, 0, 4}
-       : v == 14 ? TraceShape{2, 3, 8, 8, 0, 3}
+       : v == 13 ? TraceShape{2, 3, 8, 8, 0, 3}
                  : TraceShape{FFB_ADV_PER_ITER, FFB_TEST_PER_ITER, FFB_REFILL_MIN, FFB_MIN_BLOCKS, 0, 0};
 }
 
