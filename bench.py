@@ -816,11 +816,13 @@ def ours(args):
     dims = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
     tune = None
     if dims is None and args.cells_per_face <= 0:
-        # grid and launch shape chosen by the autotuner on a ~4 Mi-ray sample
-        # (rank 0's choice on every rank)
+        # grid and launch shape chosen by the autotuner, timed on the whole
+        # step (every face emits: the launch tails weigh as in the real run;
+        # rank 0's choice on every rank)
         t0 = time.perf_counter()
         tune = ctx.autotune(front, rear, SEED, candidates=[dict(cells_per_face=c, skip_empty=not args.no_skip)
-                                                           for c in (128.0, 192.0, 256.0)], force=True)
+                                                           for c in (128.0, 192.0, 256.0)], sample_every=1,
+                            force=True)
         tune["tuning_s"] = time.perf_counter() - t0
         if world > 1:
             pick = torch.tensor([tune["cells_per_face"], float(tune["shape"])], device="cuda")
