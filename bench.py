@@ -92,16 +92,67 @@ def workload(rays_per_face):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
+    """SM clock and clock-event reasons sampled while the timed region runs.
+    NVML is polled from a thread every 2 ms (read-only queries), so a timed
+    region of a tenth of a second still gets tens of samples; without NVML,
+    nvidia-smi -lms 200 is the fallback."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, device):
         self.device = device
         self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
         self.proc = None
+        self.nvml = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is not None:
+            pci = "%08x:%02x:%02x.0" % (getattr(props, "pci_domain_id", 0), bus, getattr(props, "pci_device_id", 0))
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(pci)
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+
+    def _sample(self):
+        nv, h = self.nvml
+        return (nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+
+    def _poll(self):
+        while not self.stop_flag.is_set():
+            try:
+                self.rows.append(self._sample())
+            except Exception:  # a failed query ends sampling, not the run
+                return
+            self.stop_flag.wait(0.002)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            # the first queries after nvmlInit pay NVML's own set-up: take
+            # them here, before the timed region, and keep their latency
+            t0 = time.perf_counter()
+            self._sample()
+            self.first_query_ms = (time.perf_counter() - t0) * 1e3
+            t0 = time.perf_counter()
+            self._sample()
+            self.query_ms = (time.perf_counter() - t0) * 1e3
+        except Exception:
+            self.nvml = None
+        if self.nvml:
+            import threading
+            self.stop_flag = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -110,6 +161,19 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread:
+            self.stop_flag.set()
+            self.thread.join(2)
+            rows, self.thread = self.rows, None
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            sm = [float(r[0]) for r in rows]
+            loaded = [s for s in sm if s > 0.5 * max(sm)]
+            reasons = sorted({name for r in rows for name, bit in self.REASON_BITS if r[2] & bit})
+            return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(max(r[1] for r in rows)),
+                    "sm_min_mhz": min(sm), "reasons": reasons, "samples": len(rows),
+                    "source": "nvml polled every 2 ms (one query round %.2f ms; the first after init %.1f ms, "
+                              "taken before the timed region)" % (self.query_ms, self.first_query_ms)}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -550,6 +614,7 @@ def csv_section(ctx, stream, counts, front, rear, n):
     from oracle_lib import Reference
     outgoing = (front.astype(np.int64) + rear).astype(np.int32)
     d_out = torch.from_numpy(outgoing).cuda()
+    nonzero = int(torch.count_nonzero(counts).item())
     n_text = ctx.csv_length(counts=counts, outgoing=d_out)
     text = torch.empty(n_text, dtype=torch.uint8, device="cuda")
     ctx.csv_format(counts=counts, outgoing=d_out, out=text)  # warm-up
@@ -593,7 +658,7 @@ def csv_section(ctx, stream, counts, front, rear, n):
                              "to the same file system" % (k, k)}
     return {
         "workload": "CSV text of the %dx%d matrix of this step (csv_export::export_csv format)" % (n, n),
-        "entries": entries, "text_bytes": int(n_text),
+        "entries": entries, "nonzero_entries": nonzero, "text_bytes": int(n_text),
         "format_ms": fmt_s * 1e3, "format_entries_per_s": entries / fmt_s,
         "roofline": {"bound": "hbm", "achieved": alg_bytes / fmt_s / 1e9, "peak": measured_hbm_gbs(),
                      "peak_source": hbm_peak()[1], "unit": "GB/s",
@@ -859,7 +924,8 @@ def ours(args):
         dist.barrier()
     clocks = Clocks(local)
     clocks.start()
-    time.sleep(0.2)
+    if not clocks.thread:
+        time.sleep(0.2)  # nvidia-smi's first sample
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -907,6 +973,7 @@ def ours(args):
         zms.append(ctx.stats().kernel_ms)
     zero_ms = statistics.median(zms)
     zero_bytes = 4 * rows * n
+    step(10_004)  # counts of a real step again: the sections below format and gather them
     tests_per_launch = tests
     achieved = tests_per_launch * FLOPS_PER_TEST / (k_ms * 1e-3)
     peak = fp32_peak(local)
