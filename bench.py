@@ -989,15 +989,29 @@ def ours(args):
     for i in range(e2e_steps):
         step(20_001 + i, out=host_counts)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
+    d2h_rank = ctx.stats().d2h_bytes  # the last step's device -> host bytes
+    # the same steps with every row block copied dense (no host threads)
+    host_threads = ctx.host_threads()
+    ctx.set_host_threads(0)
     if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        step(20_001 + i, out=host_counts)
+    e2e_dense_s = (time.perf_counter() - t0) / e2e_steps
+    ctx.set_host_threads(-1)
+    t = torch.tensor([e2e_s, e2e_dense_s], device="cuda")
+    d2h_t = torch.tensor([d2h_rank], dtype=torch.float64, device="cuda")
+    if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        dist.all_reduce(d2h_t)
+    e2e_s, e2e_dense_s = [float(x) for x in t.tolist()]
     # host -> device per step (all ranks): one 16-byte record per emitting
     # face (face, its ray counts, its first work chunk), the chunks built on
-    # the GPU; device -> host: every rank's row block, the whole matrix
+    # the GPU; device -> host: every rank's row blocks as the (column, count)
+    # pairs of their nonzero entries plus a header per block
     h2d = 16 * int(np.count_nonzero(front.astype(np.int64) + rear))
-    d2h = 4 * n * n
+    d2h = int(d2h_t.item())
     gather = None
     if world > 1:
         # the full matrix on every rank: one NCCL all_gather of the row
@@ -1044,7 +1058,14 @@ def ours(args):
                        "gather": gather,
                        "l2": "flushed each step by zeroing the 1.95 GB count matrix"},
             "e2e": {"value": world * rays_per_step / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3, "host_threads": host_threads,
+                    "output": "the N x N uint32 counts in pinned host memory, every step",
+                    "transfer": "each row block packed on the device to (column, count) pairs of its nonzero "
+                                "entries; the pairs cross PCIe and host threads expand them into the host "
+                                "matrix with streaming stores while the next block traces",
+                    "dense_copy": {"value": world * rays_per_step / e2e_dense_s, "ms_per_step": e2e_dense_s * 1e3,
+                                   "d2h_bytes_per_step": 4 * n * n,
+                                   "note": "the same steps with every row block copied dense (host threads 0)"}},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "GFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic_per_launch(),

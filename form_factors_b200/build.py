@@ -18,7 +18,7 @@ LIB = os.path.join(PKG, "libffb200.so")
 PROBE_LIB = os.path.join(PKG, "libffb200_probe.so")
 
 CUDA_SOURCES = ["ffb_api.cu", "ffb_static.cu"]
-CXX_SOURCES = ["ffb_systems.cpp", "ffb_server.cpp", "ffb_thermal.cpp"]
+CXX_SOURCES = ["ffb_systems.cpp", "ffb_server.cpp", "ffb_thermal.cpp", "ffb_host_rows.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

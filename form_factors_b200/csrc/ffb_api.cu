@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <map>
@@ -26,6 +27,7 @@
 #include "ffb_csv.cuh"
 #include "ffb_internal.h"
 #include "ffb_obj.cuh"
+#include "ffb_pack.cuh"
 #include "ffb_trace.cuh"
 
 using namespace ffb;
@@ -151,7 +153,19 @@ struct ffb_ctx {
   // event per row block (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t block_done[kMaxPipeBlocks] = {};
+  cudaEvent_t block_copied[kMaxPipeBlocks] = {};
   cudaEvent_t copies_done = nullptr;
+  // the same output moved as (column, count) pairs: device packs of the row
+  // blocks and their headers, pinned copies of them, and the host threads
+  // that expand them into the caller's rows
+  DevBuf pack_hdr, pack_pairs;
+  uint32_t* pack_hdr_host = nullptr;
+  size_t pack_hdr_host_cap = 0;
+  uint32_t* pack_stage[2] = {nullptr, nullptr};
+  size_t pack_stage_cap = 0;
+  int host_threads = -1;  // -1: the default, min(8, hardware threads)
+  ffb_host_pool* host_pool = nullptr;
+  unsigned long long last_d2h = 0;  // device->host bytes of the last counts call
 };
 
 namespace {
@@ -334,13 +348,25 @@ int ensure_pipeline(ffb_ctx* c)
   if (c->copy_stream)
     return FFB_OK;
   cudaError_t e = cudaEventCreateWithFlags(&c->copies_done, cudaEventDisableTiming);
-  for (int b = 0; b < kMaxPipeBlocks && e == cudaSuccess; ++b)
+  for (int b = 0; b < kMaxPipeBlocks && e == cudaSuccess; ++b) {
     e = cudaEventCreateWithFlags(&c->block_done[b], cudaEventDisableTiming);
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&c->block_copied[b], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess)
     e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess)
     return fail(FFB_ERR_CUDA, "copy stream/event creation: %s", cudaGetErrorString(e));
   return FFB_OK;
+}
+
+// Host threads that expand packed host outputs (0: dense copies only).
+int host_threads(const ffb_ctx* c)
+{
+  if (c->host_threads >= 0)
+    return c->host_threads;
+  const unsigned hw = std::thread::hardware_concurrency();
+  return (int)std::min(8u, std::max(hw, 1u));
 }
 
 int ensure_batch_streams(ffb_ctx* c)
@@ -717,7 +743,8 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
                     &c->scan_sums, &c->chunks,      &c->chunk_src,    &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
                     &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
-                    &c->power_tab, &c->absorb, &c->span, &c->obj_text, &c->obj_chunk, &c->obj_chunk_off,
+                    &c->power_tab, &c->absorb, &c->span, &c->pack_hdr, &c->pack_pairs, &c->obj_text,
+                    &c->obj_chunk, &c->obj_chunk_off,
                     &c->obj_starts, &c->obj_flags, &c->obj_ords, &c->obj_vertices, &c->obj_face_idx,
                     &c->obj_face_line, &c->obj_special, &c->obj_ranges, &c->obj_faces, &c->obj_err};
   for (DevBuf* b : bufs)
@@ -737,6 +764,12 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
   if (c->copies_done) cudaEventDestroy(c->copies_done);
   for (cudaEvent_t e : c->block_done)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->block_copied)
+    if (e) cudaEventDestroy(e);
+  ffb_host_pool_destroy(c->host_pool);
+  if (c->pack_hdr_host) cudaFreeHost(c->pack_hdr_host);
+  for (uint32_t* p : c->pack_stage)
+    if (p) cudaFreeHost(p);
   if (c->pinned_free) cudaEventDestroy(c->pinned_free);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -777,6 +810,18 @@ extern "C" int ffb_ctx_set_budget(ffb_ctx* c, unsigned long long bytes)
 }
 
 extern "C" unsigned long long ffb_ctx_bytes(ffb_ctx* c) { return c ? c->bytes : 0; }
+
+extern "C" int ffb_ctx_set_host_threads(ffb_ctx* c, int n)
+{
+  if (!c)
+    return fail(FFB_ERR_ARG, "null context");
+  if (n < -1 || n > 256)
+    return fail(FFB_ERR_ARG, "host threads %d outside [-1, 256]", n);
+  c->host_threads = n;
+  return FFB_OK;
+}
+
+extern "C" int ffb_ctx_host_threads(ffb_ctx* c) { return c ? host_threads(c) : 0; }
 
 extern "C" int ffb_ctx_set_stats(ffb_ctx* c, int on)
 {
@@ -975,6 +1020,80 @@ extern "C" int ffb_emit(ffb_ctx* c, const int32_t* front, const int32_t* rear, u
   return FFB_OK;
 }
 
+namespace {
+
+// Pinned host memory of at least `bytes` in *p (capacity *cap), kept and
+// grown by doubling.
+int ensure_pinned(uint32_t** p, size_t* cap, size_t bytes)
+{
+  if (bytes <= *cap)
+    return FFB_OK;
+  if (*p)
+    cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t want = std::max(bytes, (size_t)8 << 20);
+  FFB_CUDA(cudaMallocHost((void**)p, want));
+  *cap = want;
+  return FFB_OK;
+}
+
+// A host output of several row blocks moved as (column, count) pairs: called
+// after every block's trace and pack are queued on the context stream
+// (block_done[b] recorded after block b's pack).  Every device-to-host copy
+// goes on the copy stream, issued once its block is done: block b's header,
+// then its pairs (or, when they would not fit its cap of a quarter of its
+// entries, its dense rows).  A copy queued early on the context stream would
+// hold the copy engine's queue until that stream reached it.  Host threads
+// expand block b while block b + 1's copies run.
+int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int n_rows, const uint32_t* d_counts,
+                 uint32_t* counts, const std::vector<size_t>& hdr_off, const std::vector<size_t>& pair_off,
+                 const std::vector<uint32_t>& cap)
+{
+  const int n_blocks = (int)bounds.size() - 1;
+  std::vector<char> dense((size_t)n_blocks, 0);
+  auto fetch = [&](int b) -> int {
+    const int rows = bounds[b + 1] - bounds[b];
+    FFB_CUDA(cudaStreamWaitEvent(c->copy_stream, c->block_done[b], 0));
+    FFB_CUDA(cudaMemcpyAsync(c->pack_hdr_host + hdr_off[b], dptr<uint32_t>(c->pack_hdr) + hdr_off[b],
+                             sizeof(uint32_t) * pack_header_words(rows), cudaMemcpyDeviceToHost, c->copy_stream));
+    FFB_CUDA(cudaStreamSynchronize(c->copy_stream));
+    const uint32_t total = c->pack_hdr_host[hdr_off[b]];
+    const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
+    const size_t n_words = (size_t)rows * n_rows;
+    c->last_d2h += sizeof(uint32_t) * pack_header_words(rows);
+    if (total > cap[b]) {
+      dense[b] = 1;
+      FFB_CUDA(cudaMemcpyAsync(counts + off, d_counts + off, sizeof(uint32_t) * n_words, cudaMemcpyDeviceToHost,
+                               c->copy_stream));
+      c->last_d2h += sizeof(uint32_t) * n_words;
+    } else if (total > 0) {
+      FFB_CUDA(cudaMemcpyAsync(c->pack_stage[b & 1], dptr<uint2>(c->pack_pairs) + pair_off[b],
+                               sizeof(uint2) * (size_t)total, cudaMemcpyDeviceToHost, c->copy_stream));
+      c->last_d2h += sizeof(uint2) * (size_t)total;
+    }
+    FFB_CUDA(cudaEventRecord(c->block_copied[b], c->copy_stream));
+    return FFB_OK;
+  };
+  FFB_TRY(fetch(0));
+  for (int b = 0; b < n_blocks; ++b) {
+    FFB_CUDA(cudaEventSynchronize(c->block_copied[b]));
+    const int rows = bounds[b + 1] - bounds[b];
+    const uint32_t* h = c->pack_hdr_host + hdr_off[b];
+    if (!dense[b])
+      ffb_host_expand_start(c->host_pool, counts + (size_t)(bounds[b] - row_begin) * n_rows, rows, n_rows, h + 2,
+                            h + 2 + rows, c->pack_stage[b & 1]);
+    // the next block's pairs go to the other stage, which block b - 1 used
+    const int rc = b + 1 < n_blocks ? fetch(b + 1) : FFB_OK;
+    if (!dense[b])
+      ffb_host_expand_join(c->host_pool);
+    FFB_TRY(rc);
+  }
+  return FFB_OK;
+}
+
+}  // namespace
+
 extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
                                            uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
                                            int row_begin, int row_end, uint32_t* counts)
@@ -1053,6 +1172,40 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   FFB_TRY(ensure(c, c->cursor, sizeof(uint32_t) * kMaxPipeBlocks));
   if (n_blocks > 1)
     FFB_TRY(ensure_pipeline(c));
+  // A pipelined host output moves as (column, count) pairs when host threads
+  // are enabled: per block a header (pack_header_words) and at most a
+  // quarter of its entries as pairs (2 bytes per entry instead of 4).
+  const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0;
+  std::vector<size_t> hdr_off, pair_off;
+  std::vector<uint32_t> cap;
+  size_t hdr_words = 0;
+  c->last_d2h = 0;
+  if (packed) {
+    size_t& hw = hdr_words;
+    size_t pw = 0, max_cap = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+      const int rows = bounds[b + 1] - bounds[b];
+      hdr_off.push_back(hw);
+      pair_off.push_back(pw);
+      cap.push_back((uint32_t)std::min<size_t>((size_t)rows * n_rows / 4, UINT32_MAX));
+      hw += pack_header_words(rows);
+      pw += cap.back();
+      max_cap = std::max<size_t>(max_cap, cap.back());
+    }
+    FFB_TRY(ensure(c, c->pack_hdr, sizeof(uint32_t) * hw));
+    FFB_TRY(ensure(c, c->pack_pairs, sizeof(uint2) * std::max<size_t>(pw, 1)));
+    FFB_TRY(ensure_pinned(&c->pack_hdr_host, &c->pack_hdr_host_cap, sizeof(uint32_t) * hw));
+    size_t stage_cap = c->pack_stage_cap;
+    for (uint32_t*& st : c->pack_stage) {
+      stage_cap = c->pack_stage_cap;  // both stages have the same capacity
+      FFB_TRY(ensure_pinned(&st, &stage_cap, sizeof(uint2) * std::max<size_t>(max_cap, 1)));
+    }
+    c->pack_stage_cap = stage_cap;
+    if (!c->host_pool || ffb_host_pool_threads(c->host_pool) != host_threads(c)) {
+      ffb_host_pool_destroy(c->host_pool);
+      c->host_pool = ffb_host_pool_create(host_threads(c));
+    }
+  }
   TraceParams p;
   p.frames = dptr<float>(c->frames);
   p.key0 = (uint32_t)seed;
@@ -1073,29 +1226,58 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   p.scene.face_base = 0;
   p.scene.n_cols = n_rows;
   FFB_CUDA(cudaMemsetAsync(c->cursor.ptr, 0, sizeof(uint32_t) * n_blocks, c->stream));
+  if (packed)  // the blocks' pair cursors (header word 0) start at zero
+    FFB_CUDA(cudaMemsetAsync(c->pack_hdr.ptr, 0, sizeof(uint32_t) * hdr_words, c->stream));
   timing_begin(c);
+  // Row blocks alternate between two side streams, so that one block's
+  // launch tail (a block holds a few chunks per warp) overlaps the next
+  // block's launch; blocks share nothing they write (rows, cursor, pairs).
+  constexpr int kBlockStreams = 2;
+  if (n_blocks > 1) {
+    FFB_TRY(ensure_batch_streams(c));
+    FFB_CUDA(cudaEventRecord(c->batch_fork, c->stream));
+    for (int k = 0; k < kBlockStreams; ++k)
+      FFB_CUDA(cudaStreamWaitEvent(c->batch_streams[k], c->batch_fork, 0));
+  }
   for (int b = 0; b < n_blocks; ++b) {
+    cudaStream_t st = n_blocks > 1 ? c->batch_streams[b % kBlockStreams] : c->stream;
     const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
     const size_t n_words = (size_t)(bounds[b + 1] - bounds[b]) * n_rows;
-    FFB_CUDA(cudaMemsetAsync((uint32_t*)d_counts + off, 0, sizeof(uint32_t) * n_words, c->stream));
+    FFB_CUDA(cudaMemsetAsync((uint32_t*)d_counts + off, 0, sizeof(uint32_t) * n_words, st));
     if (first[b + 1] > first[b]) {
       p.chunks = dptr<Chunk>(c->chunks) + first[b];
       p.n_chunks = first[b + 1] - first[b];
       p.chunk_cursor = dptr<uint32_t>(c->cursor) + b;
       if (s.info.skip_empty)
-        FFB_TRY((launch_fused<true>(c, p, false)));
+        FFB_TRY((launch_fused<true>(c, p, false, st)));
       else
-        FFB_TRY((launch_fused<false>(c, p, false)));
+        FFB_TRY((launch_fused<false>(c, p, false, st)));
+    }
+    if (packed) {
+      const int rows = bounds[b + 1] - bounds[b];
+      k_rows_pack<<<std::min(rows, c->n_sm * 8), kPackThreads, 0, st>>>(
+          (const uint32_t*)d_counts + off, rows, n_rows, dptr<uint32_t>(c->pack_hdr) + hdr_off[b], cap[b],
+          dptr<uint2>(c->pack_pairs) + pair_off[b]);
+      FFB_CUDA(cudaGetLastError());
     }
     if (n_blocks > 1)
-      FFB_CUDA(cudaEventRecord(c->block_done[b], c->stream));
+      FFB_CUDA(cudaEventRecord(c->block_done[b], st));
   }
+  if (n_blocks > 1)  // the context stream continues after every block
+    for (int k = 0; k < kBlockStreams; ++k) {
+      FFB_CUDA(cudaEventRecord(c->batch_join[k], c->batch_streams[k]));
+      FFB_CUDA(cudaStreamWaitEvent(c->stream, c->batch_join[k], 0));
+    }
   timing_end(c);
   if (!host_out)
     return FFB_OK;
-  if (n_blocks == 1) {
+  if (packed) {
+    FFB_TRY(fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off, cap));
+  } else if (n_blocks == 1) {
+    c->last_d2h = sizeof(uint32_t) * words;
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
   } else {
+    c->last_d2h = sizeof(uint32_t) * words;
     // all launches are queued before the first copy: a copy to pageable
     // memory holds the host until it ends
     for (int b = 0; b < n_blocks; ++b) {
@@ -2434,6 +2616,7 @@ extern "C" int ffb_stats_get(ffb_ctx* c, ffb_stats* out)
     out->hits = s[kStatHits];
     out->jumps = s[kStatJumps];
   }
+  out->d2h_bytes = c->last_d2h;
   if (c->timed)
     cudaEventElapsedTime(&out->kernel_ms, c->ev0, c->ev1);
   return FFB_OK;

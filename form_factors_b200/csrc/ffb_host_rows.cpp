@@ -1,0 +1,205 @@
+// ffb_host_rows.cpp -- host threads that write count-matrix rows into a
+// caller's host buffer from the (column, count) pairs of their nonzero
+// entries (ffb_internal.h).
+//
+// A form-factor count matrix is mostly zeros (the closed 22 080-face
+// enclosure at 1000 rays per face fills 4 % of its entries), so a host
+// output is cheaper to move as the pairs of its nonzeros: the device packs
+// each finished row block, the pairs cross PCIe, and these threads expand
+// them into the dense rows.  A thread writes a row front to back, segment by
+// segment, with non-temporal stores (no read-for-ownership of the
+// destination lines): the destination is written once, in full, at the
+// host's streaming-store bandwidth.
+#include <immintrin.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "ffb_internal.h"
+
+struct ffb_host_pool {
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable wake, idle;
+  uint64_t generation = 0;
+  bool stop = false;
+  int busy = 0;  // workers still on the current job
+  std::function<void(int, int)> task;  // (task, worker)
+  int n_tasks = 0;
+  std::atomic<int> next{0};
+  std::vector<uint32_t*> seg;  // one zeroed 64-byte aligned scratch segment per worker
+  bool avx2 = false;
+};
+
+namespace {
+
+void worker_main(ffb_host_pool* p, int id)
+{
+  uint64_t seen = 0;
+  for (;;) {
+    std::function<void(int, int)> task;
+    {
+      std::unique_lock<std::mutex> lk(p->mu);
+      p->wake.wait(lk, [&] { return p->stop || p->generation != seen; });
+      if (p->stop)
+        return;
+      seen = p->generation;
+      task = p->task;
+    }
+    for (int t = p->next.fetch_add(1); t < p->n_tasks; t = p->next.fetch_add(1))
+      task(t, id);
+    _mm_sfence();  // the streaming stores are globally visible before the job counts as done
+    std::lock_guard<std::mutex> lk(p->mu);
+    if (--p->busy == 0)
+      p->idle.notify_all();
+  }
+}
+
+// Row r of the block from its pairs, which come in ascending column order.
+// The row is built in segments of kSeg words in a zeroed scratch segment of
+// the thread's (16 KB, L1 resident): the segment's few pairs are stored
+// into it, the segment is streamed to the destination with non-temporal
+// stores, and the stored words are cleared again.  Words before the
+// destination's first 32-byte boundary are written with plain stores, so
+// the streaming stores are aligned; so is the tail after the last whole
+// vector.
+constexpr int kSeg = 4096;
+
+template <bool kAvx2>
+void expand_row(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
+                uint32_t* __restrict__ seg);
+
+template <>
+void expand_row<false>(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
+                       uint32_t* __restrict__ seg)
+{
+  uint32_t k = 0;
+  int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
+  head = std::min(head, n_cols);
+  for (int i = 0; i < head; ++i)
+    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? pairs[2 * k++ + 1] : 0u;
+  for (int i0 = head; i0 < n_cols; i0 += kSeg) {
+    const int len = std::min(kSeg, n_cols - i0);
+    const uint32_t k0 = k;
+    while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
+      seg[pairs[2 * k] - (uint32_t)i0] = pairs[2 * k + 1];
+      ++k;
+    }
+    uint32_t* d = dst + i0;
+    int j = 0;
+    for (; j + 8 <= len; j += 8) {
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + j), _mm_load_si128(reinterpret_cast<const __m128i*>(seg + j)));
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + j + 4),
+                       _mm_load_si128(reinterpret_cast<const __m128i*>(seg + j + 4)));
+    }
+    for (; j < len; ++j)
+      d[j] = seg[j];
+    for (uint32_t q = k0; q < k; ++q)
+      seg[pairs[2 * q] - (uint32_t)i0] = 0u;
+  }
+}
+
+template <>
+__attribute__((target("avx2"))) void expand_row<true>(uint32_t* __restrict__ dst, int n_cols,
+                                                      const uint32_t* __restrict__ pairs, uint32_t n,
+                                                      uint32_t* __restrict__ seg)
+{
+  uint32_t k = 0;
+  int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
+  head = std::min(head, n_cols);
+  for (int i = 0; i < head; ++i)
+    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? pairs[2 * k++ + 1] : 0u;
+  for (int i0 = head; i0 < n_cols; i0 += kSeg) {
+    const int len = std::min(kSeg, n_cols - i0);
+    const uint32_t k0 = k;
+    while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
+      seg[pairs[2 * k] - (uint32_t)i0] = pairs[2 * k + 1];
+      ++k;
+    }
+    uint32_t* d = dst + i0;
+    int j = 0;
+    for (; j + 16 <= len; j += 16) {
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(d + j),
+                          _mm256_load_si256(reinterpret_cast<const __m256i*>(seg + j)));
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(d + j + 8),
+                          _mm256_load_si256(reinterpret_cast<const __m256i*>(seg + j + 8)));
+    }
+    for (; j < len; ++j)
+      d[j] = seg[j];
+    for (uint32_t q = k0; q < k; ++q)
+      seg[pairs[2 * q] - (uint32_t)i0] = 0u;
+  }
+}
+
+}  // namespace
+
+ffb_host_pool* ffb_host_pool_create(int threads)
+{
+  ffb_host_pool* p = new ffb_host_pool;
+  threads = std::max(threads, 1);
+  p->avx2 = __builtin_cpu_supports("avx2");
+  for (int i = 0; i < threads; ++i) {
+    uint32_t* sg = static_cast<uint32_t*>(std::aligned_alloc(64, sizeof(uint32_t) * kSeg));
+    std::memset(sg, 0, sizeof(uint32_t) * kSeg);
+    p->seg.push_back(sg);
+  }
+  for (int i = 0; i < threads; ++i)
+    p->workers.emplace_back(worker_main, p, i);
+  return p;
+}
+
+void ffb_host_pool_destroy(ffb_host_pool* p)
+{
+  if (!p)
+    return;
+  {
+    std::lock_guard<std::mutex> lk(p->mu);
+    p->stop = true;
+  }
+  p->wake.notify_all();
+  for (std::thread& t : p->workers)
+    t.join();
+  for (uint32_t* sg : p->seg)
+    std::free(sg);
+  delete p;
+}
+
+int ffb_host_pool_threads(const ffb_host_pool* p) { return p ? (int)p->workers.size() : 0; }
+
+void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
+                           const uint32_t* count, const uint32_t* pairs)
+{
+  // tasks of 8 rows: a few hundred KB of destination each
+  constexpr int kRowsPerTask = 8;
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->task = [p, dst, rows, n_cols, first, count, pairs](int t, int w) {
+    uint32_t* sg = p->seg[(size_t)w];
+    const int r1 = std::min(rows, (t + 1) * kRowsPerTask);
+    for (int r = t * kRowsPerTask; r < r1; ++r) {
+      uint32_t* d = dst + (size_t)r * (size_t)n_cols;
+      if (p->avx2)
+        expand_row<true>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg);
+      else
+        expand_row<false>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg);
+    }
+  };
+  p->n_tasks = (rows + kRowsPerTask - 1) / kRowsPerTask;
+  p->next.store(0);
+  p->busy = (int)p->workers.size();
+  ++p->generation;
+  p->wake.notify_all();
+}
+
+void ffb_host_expand_join(ffb_host_pool* p)
+{
+  std::unique_lock<std::mutex> lk(p->mu);
+  p->idle.wait(lk, [&] { return p->busy == 0; });
+}

@@ -28,3 +28,19 @@ int ffb_trace_prepare(ffb_ctx* c, const int32_t* front, const int32_t* rear, uin
                       uint32_t* counts, long long* n_chunks);
 int ffb_trace_slice(ffb_ctx* c, long long first, long long count, void* stream);
 int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long* end_ns);
+
+// Host threads that write count-matrix rows into a host buffer from the
+// (column, count) pairs of their nonzero entries (ffb_host_rows.cpp).
+// ffb_host_expand_start hands rows [0, rows) to the pool and returns: row r
+// of the n_cols-wide uint32 matrix at dst gets the count[r] pairs at
+// pairs + 2 * first[r] (column, count; columns ascending and below n_cols)
+// and zeros elsewhere; every entry of the rows is written.  ffb_host_expand_join waits until the rows are
+// written (and their streaming stores are visible).  One job at a time per
+// pool; the buffers must stay valid until the join.
+struct ffb_host_pool;
+ffb_host_pool* ffb_host_pool_create(int threads);
+void ffb_host_pool_destroy(ffb_host_pool* p);
+int ffb_host_pool_threads(const ffb_host_pool* p);
+void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
+                           const uint32_t* count, const uint32_t* pairs);
+void ffb_host_expand_join(ffb_host_pool* p);

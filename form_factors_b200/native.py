@@ -46,7 +46,8 @@ class GridInfo(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("tests", C.c_ulonglong), ("cells", C.c_ulonglong), ("rays", C.c_ulonglong),
-                ("hits", C.c_ulonglong), ("kernel_ms", C.c_float), ("jumps", C.c_ulonglong)]
+                ("hits", C.c_ulonglong), ("kernel_ms", C.c_float), ("jumps", C.c_ulonglong),
+                ("d2h_bytes", C.c_ulonglong)]
 
 
 class DiscSource(C.Structure):
@@ -145,6 +146,8 @@ def load(path=LIB_PATH):
         "ffb_ctx_synchronize": (i32, [vp]),
         "ffb_ctx_set_budget": (i32, [vp, C.c_ulonglong]),
         "ffb_ctx_set_stats": (i32, [vp, i32]),
+        "ffb_ctx_set_host_threads": (i32, [vp, i32]),
+        "ffb_ctx_host_threads": (i32, [vp]),
         "ffb_ctx_bytes": (C.c_ulonglong, [vp]),
         "ffb_last_error": (C.c_char_p, []),
         "ffb_scene_set": (i32, [vp, vp, i32]),
@@ -300,6 +303,14 @@ class Context:
     def set_stats(self, on):
         """Counters in the fused kernel on or off (on by default)."""
         _check(self._lib.ffb_ctx_set_stats(self._h, 1 if on else 0))
+
+    def set_host_threads(self, n):
+        """Host threads that expand packed host outputs of the count matrix
+        (-1: default, 0: dense copies only)."""
+        _check(self._lib.ffb_ctx_set_host_threads(self._h, int(n)))
+
+    def host_threads(self):
+        return _check(self._lib.ffb_ctx_host_threads(self._h))
 
     def device_bytes(self):
         return int(self._lib.ffb_ctx_bytes(self._h))

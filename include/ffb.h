@@ -71,6 +71,8 @@ typedef struct {
   unsigned long long hits;  /* rays that hit a face */
   float kernel_ms;          /* device time of the trace kernel (CUDA events) */
   unsigned long long jumps; /* empty-space jumps among the cells visited */
+  unsigned long long d2h_bytes; /* device-to-host bytes of the last counts call with a host output (0 for a
+                                   device output) */
 } ffb_stats;
 
 /* Context: one device, one stream, resident scene and grid.
@@ -95,6 +97,16 @@ unsigned long long ffb_ctx_bytes(ffb_ctx* ctx);
  * counts (kernel_ms stays).  No reference counterpart: the reference keeps no
  * such counters. */
 int ffb_ctx_set_stats(ffb_ctx* ctx, int on);
+/* Host threads of the context (-1: the default, min(8, hardware threads);
+ * 0 to 256).  A count matrix written to a host buffer in row blocks (64 MB
+ * or more, ffb_form_factor_counts(_rows)) crosses PCIe as the (column, count)
+ * pairs of each block's nonzero entries, packed on the device, and these
+ * threads expand them into the caller's rows with streaming stores while the
+ * next block traces; a block denser than a quarter of its entries is copied
+ * dense.  0: every block is copied dense.  The result is the same either
+ * way.  No reference counterpart (the reference's matrix is on the host). */
+int ffb_ctx_set_host_threads(ffb_ctx* ctx, int n);
+int ffb_ctx_host_threads(ffb_ctx* ctx);
 const char* ffb_last_error(void);
 
 /* Scene upload and per-face precompute (host or device faces9).

@@ -1,0 +1,139 @@
+"""Count matrices written to host buffers in row blocks (64 MB and more).
+
+Each finished row block is packed on the device to the (column, count) pairs
+of its nonzero entries; the pairs cross PCIe and host threads expand them
+into the caller's rows with streaming stores, while the next block traces.
+A block with more nonzeros than a quarter of its entries is copied dense.
+Whatever the path, the host matrix must equal the device-resident output
+of the same call bit for bit: pageable and pinned buffers, a destination
+that is not 16-byte aligned, a row width that is not a multiple of four,
+blocks without emitting faces, dense blocks, one host thread or several,
+and host threads 0 (every block copied dense).  The device output itself is
+pinned to the oracle by the parity tests.
+"""
+import numpy as np
+import pytest
+
+from form_factors_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+SEED = 77
+
+
+def _device(ctx, front, rear, epoch, rows=None, face_to_row=None, n_rows=None):
+    import torch
+    n = n_rows or ctx.n_faces
+    b, e = rows if rows else (0, n)
+    out = torch.empty((e - b, n), dtype=torch.int32, device="cuda")
+    ctx.form_factor_counts_rows(front, rear, SEED, b, e, epoch=epoch, face_to_row=face_to_row, n_rows=n, out=out)
+    ctx.synchronize()
+    assert ctx.stats().d2h_bytes == 0
+    return out.cpu().numpy().view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def scene():
+    faces = scenes.enclosure(4, 12)  # 5120 + 576 = 5696 faces: rows of 22 784 bytes
+    return faces
+
+
+@pytest.mark.parametrize("threads", [-1, 1, 3, 0])
+def test_packed_output_equals_device_output(ctx, scene, threads):
+    import torch
+    n = len(scene)
+    assert 4 * n * n >= 64 << 20
+    ctx.scene_set(scene)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    front = np.full(n, 30, np.int32)
+    rear = np.zeros(n, np.int32)
+    want = _device(ctx, front, rear, epoch=4)
+    assert want.any()
+    ctx.set_host_threads(threads)
+    try:
+        pageable = np.full((n, n), 0xDEADBEEF, np.uint32)
+        ctx.form_factor_counts(front, rear, SEED, epoch=4, out=pageable)
+        d2h = ctx.stats().d2h_bytes
+        assert np.array_equal(pageable, want)
+        pinned = torch.full((n, n), -1, dtype=torch.int32, pin_memory=True)
+        ctx.form_factor_counts(front, rear, SEED, epoch=4, out=pinned)
+        assert np.array_equal(pinned.numpy().view(np.uint32), want)
+    finally:
+        ctx.set_host_threads(-1)
+    if threads == 0:
+        assert d2h == 4 * n * n
+    else:
+        nnz = int(np.count_nonzero(want))
+        assert 8 * nnz < d2h < 8 * nnz + 16 * n + 4096, "pairs plus block headers"
+
+
+def test_unaligned_destination_and_odd_width(ctx):
+    """A destination 4 bytes past a 16-byte boundary, and a row width that is
+    not a multiple of four (head and tail words of every row)."""
+    import torch
+    faces = scenes.enclosure(4, 11)  # 5120 + 484 = 5604 faces
+    faces = faces[:-1]               # 5603: odd width
+    n = len(faces)
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    front = np.full(n, 25, np.int32)
+    rear = np.full(n, 2, np.int32)
+    want = _device(ctx, front, rear, epoch=6)
+    raw = torch.full((n * n + 3,), -1, dtype=torch.int32, pin_memory=True)
+    for shift in (1, 2, 3):
+        view = raw[shift:shift + n * n]
+        assert view.data_ptr() % 16 != 0
+        ctx.form_factor_counts(front, rear, SEED, epoch=6, out=view)
+        assert np.array_equal(view.numpy().view(np.uint32).reshape(n, n), want), shift
+
+
+def test_blocks_without_emitters_and_row_ranges(ctx, scene):
+    """Row ranges whose blocks include ones where no face emits (all-zero
+    rows written by the host threads), and sparse emitters."""
+    n = len(scene)
+    ctx.scene_set(scene)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    front = np.zeros(n, np.int32)
+    front[:1500] = 40  # only the first rows emit: the second of the two row blocks has no emitting face
+    rear = np.zeros(n, np.int32)
+    want = _device(ctx, front, rear, epoch=8)
+    got = np.full((n, n), 0xDEADBEEF, np.uint32)
+    ctx.form_factor_counts(front, rear, SEED, epoch=8, out=got)
+    assert np.array_equal(got, want)
+    assert not got[1500:].any()
+    front[4000:4003] = 500  # a few dense rows among empty ones
+    want = _device(ctx, front, rear, epoch=8)
+    part = ctx.form_factor_counts_rows(front, rear, SEED, 700, n, epoch=8)
+    assert np.array_equal(part, want[700:])
+
+
+def test_dense_blocks_fall_back_to_dense_copies(ctx):
+    """A small closed scene traced with many rays per face fills most of its
+    entries: its blocks exceed the pair cap and are copied dense, and the
+    result is unchanged."""
+    faces = scenes.icosphere(4, 1.0, inward=True)  # 5120 faces, 105 MB matrix
+    n = len(faces)
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=32, skip_empty=True)
+    front = np.full(n, 12000, np.int32)
+    rear = np.zeros(n, np.int32)
+    want = _device(ctx, front, rear, epoch=1)
+    assert np.count_nonzero(want) > n * n / 4, "dense enough to pass the cap"
+    got = ctx.form_factor_counts(front, rear, SEED, epoch=1)
+    assert np.array_equal(got, want)
+    assert ctx.stats().d2h_bytes >= 4 * n * n
+
+
+def test_mesh_rows_host_output(ctx, scene):
+    """Rows as meshes (face_to_row): several faces add into one row."""
+    n = len(scene)
+    ctx.scene_set(scene)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    rng = np.random.default_rng(3)
+    m = 4200
+    face_to_row = rng.integers(0, m, n).astype(np.int32)
+    front = np.full(n, 20, np.int32)
+    rear = np.zeros(n, np.int32)
+    want = _device(ctx, front, rear, epoch=2, face_to_row=face_to_row, n_rows=m)
+    got = ctx.form_factor_counts(front, rear, SEED, epoch=2, face_to_row=face_to_row, n_rows=m)
+    assert np.array_equal(got, want)
