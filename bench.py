@@ -17,8 +17,10 @@ step's lines in L2.
   value  rays/s with the scene, grid and matrix resident (CUDA events on the
          context stream around K steps, max over ranks)
   e2e    rays/s through the C ABI with host buffers: host ray counts in, the
-         count matrix copied to pinned host memory every step (in row blocks
-         whose copies overlap the next block's trace)
+         count matrix in pinned host memory every step (row blocks packed on
+         the device to the (column, count) pairs of their nonzero entries,
+         which cross PCIe and are expanded into the host rows by host threads
+         while the next block traces)
   --impl reference  the reference's own CPU path (zgrid_cpu caster + malley_cpu
          emission, compiled from its sources into oracle/_ref) on a bounded
          sample of the same workload, all host cores
@@ -123,8 +125,7 @@ class Clocks:
 
     def _sample(self):
         nv, h = self.nvml
-        return (nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
-                nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+        return (nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetCurrentClocksEventReasons(h))
 
     def _poll(self):
         while not self.stop_flag.is_set():
@@ -145,6 +146,8 @@ class Clocks:
             t0 = time.perf_counter()
             self._sample()
             self.query_ms = (time.perf_counter() - t0) * 1e3
+            nv, h = self.nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
             self.nvml = None
         if self.nvml:
@@ -169,8 +172,8 @@ class Clocks:
                 return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
             sm = [float(r[0]) for r in rows]
             loaded = [s for s in sm if s > 0.5 * max(sm)]
-            reasons = sorted({name for r in rows for name, bit in self.REASON_BITS if r[2] & bit})
-            return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(max(r[1] for r in rows)),
+            reasons = sorted({name for r in rows for name, bit in self.REASON_BITS if r[1] & bit})
+            return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.max_mhz,
                     "sm_min_mhz": min(sm), "reasons": reasons, "samples": len(rows),
                     "source": "nvml polled every 2 ms (one query round %.2f ms; the first after init %.1f ms, "
                               "taken before the timed region)" % (self.query_ms, self.first_query_ms)}

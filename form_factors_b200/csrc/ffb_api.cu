@@ -163,7 +163,7 @@ struct ffb_ctx {
   size_t pack_hdr_host_cap = 0;
   uint32_t* pack_stage[2] = {nullptr, nullptr};
   size_t pack_stage_cap = 0;
-  int host_threads = -1;  // -1: the default, min(8, hardware threads)
+  int host_threads = -1;  // -1: the default, min(12, hardware threads)
   ffb_host_pool* host_pool = nullptr;
   unsigned long long last_d2h = 0;  // device->host bytes of the last counts call
 };
@@ -366,7 +366,7 @@ int host_threads(const ffb_ctx* c)
   if (c->host_threads >= 0)
     return c->host_threads;
   const unsigned hw = std::thread::hardware_concurrency();
-  return (int)std::min(8u, std::max(hw, 1u));
+  return (int)std::min(12u, std::max(hw, 1u));
 }
 
 int ensure_batch_streams(ffb_ctx* c)

@@ -97,7 +97,7 @@ unsigned long long ffb_ctx_bytes(ffb_ctx* ctx);
  * counts (kernel_ms stays).  No reference counterpart: the reference keeps no
  * such counters. */
 int ffb_ctx_set_stats(ffb_ctx* ctx, int on);
-/* Host threads of the context (-1: the default, min(8, hardware threads);
+/* Host threads of the context (-1: the default, min(12, hardware threads);
  * 0 to 256).  A count matrix written to a host buffer in row blocks (64 MB
  * or more, ffb_form_factor_counts(_rows)) crosses PCIe as the (column, count)
  * pairs of each block's nonzero entries, packed on the device, and these
