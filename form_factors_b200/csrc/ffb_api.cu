@@ -1046,9 +1046,20 @@ int ensure_pinned(uint32_t** p, size_t* cap, size_t bytes)
 // entries, its dense rows).  A copy queued early on the context stream would
 // hold the copy engine's queue until that stream reached it.  Host threads
 // expand block b while block b + 1's copies run.
+// A host output written as the normalised form factors instead of the
+// counts (ffb_form_factors): ff the host matrix, inv[m] = 1.f /
+// (float)outgoing[m] for every row, outgoing the same on the device and
+// scratch a device float block (dense blocks are normalised there first).
+struct FloatSink {
+  float* ff;
+  const float* inv;
+  const int32_t* outgoing;
+  float* scratch;
+};
+
 int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int n_rows, const uint32_t* d_counts,
                  uint32_t* counts, const std::vector<size_t>& hdr_off, const std::vector<size_t>& pair_off,
-                 const std::vector<uint32_t>& cap)
+                 const std::vector<uint32_t>& cap, const FloatSink* fs)
 {
   const int n_blocks = (int)bounds.size() - 1;
   std::vector<char> dense((size_t)n_blocks, 0);
@@ -1062,7 +1073,15 @@ int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int 
     const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
     const size_t n_words = (size_t)rows * n_rows;
     c->last_d2h += sizeof(uint32_t) * pack_header_words(rows);
-    if (total > cap[b]) {
+    if (total > cap[b] && fs) {
+      dense[b] = 1;
+      k_normalise<<<grid_blocks((long long)n_words, 256, c->n_sm * 16), 256, 0, c->copy_stream>>>(
+          d_counts + off, fs->outgoing + bounds[b], rows, n_rows, fs->scratch);
+      FFB_CUDA(cudaGetLastError());
+      FFB_CUDA(cudaMemcpyAsync(fs->ff + off, fs->scratch, sizeof(float) * n_words, cudaMemcpyDeviceToHost,
+                               c->copy_stream));
+      c->last_d2h += sizeof(float) * n_words;
+    } else if (total > cap[b]) {
       dense[b] = 1;
       FFB_CUDA(cudaMemcpyAsync(counts + off, d_counts + off, sizeof(uint32_t) * n_words, cudaMemcpyDeviceToHost,
                                c->copy_stream));
@@ -1080,9 +1099,12 @@ int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int 
     FFB_CUDA(cudaEventSynchronize(c->block_copied[b]));
     const int rows = bounds[b + 1] - bounds[b];
     const uint32_t* h = c->pack_hdr_host + hdr_off[b];
-    if (!dense[b])
-      ffb_host_expand_start(c->host_pool, counts + (size_t)(bounds[b] - row_begin) * n_rows, rows, n_rows, h + 2,
-                            h + 2 + rows, c->pack_stage[b & 1]);
+    const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
+    if (!dense[b] && fs)
+      ffb_host_expand_norm_start(c->host_pool, fs->ff + off, rows, n_rows, h + 2, h + 2 + rows, c->pack_stage[b & 1],
+                                 fs->inv + bounds[b]);
+    else if (!dense[b])
+      ffb_host_expand_start(c->host_pool, counts + off, rows, n_rows, h + 2, h + 2 + rows, c->pack_stage[b & 1]);
     // the next block's pairs go to the other stage, which block b - 1 used
     const int rc = b + 1 < n_blocks ? fetch(b + 1) : FFB_OK;
     if (!dense[b])
@@ -1094,9 +1116,14 @@ int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int 
 
 }  // namespace
 
-extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
-                                           uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
-                                           int row_begin, int row_end, uint32_t* counts)
+namespace {
+
+// ffb_form_factor_counts_rows; with fs, the output is fs's host float
+// matrix of normalised form factors instead of `counts` (a packed host
+// output: the caller checks that it is one).
+int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed, uint32_t epoch, int flags,
+                     const int32_t* face_to_row, int n_rows, int row_begin, int row_end, uint32_t* counts,
+                     const FloatSink* fs)
 {
   FFB_TRY(check_ctx(c));
   SceneData& s = c->main;
@@ -1106,7 +1133,7 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
     return fail(FFB_ERR_NO_GRID, "form factors before ffb_grid_build");
   long long total = 0;
   FFB_TRY(check_counts(s.n_faces, front, rear, &total));
-  if (!counts)
+  if (!counts && !fs)
     return fail(FFB_ERR_ARG, "null counts");
   if (!face_to_row && n_rows != s.n_faces)
     return fail(FFB_ERR_ARG, "identity rows need n_rows == n_faces (%d != %d)", n_rows, s.n_faces);
@@ -1124,8 +1151,13 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   FFB_TRY(ensure_frames(c, flags));
   const size_t words = (size_t)(row_end - row_begin) * n_rows;
   void* d_counts;
-  bool host_out;
-  FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * words, c->tmp_out, &d_counts, &host_out));
+  bool host_out = true;
+  if (fs) {
+    FFB_TRY(ensure(c, c->tmp_out, sizeof(uint32_t) * words));
+    d_counts = c->tmp_out.ptr;
+  } else {
+    FFB_TRY(output_ptr(c, counts, sizeof(uint32_t) * words, c->tmp_out, &d_counts, &host_out));
+  }
   // Row blocks: one launch each.  A host output of FFB_PIPELINE_MIN_BYTES or
   // more is split so that each finished block goes to the host on the copy
   // stream while the next block traces.
@@ -1176,6 +1208,8 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   // are enabled: per block a header (pack_header_words) and at most a
   // quarter of its entries as pairs (2 bytes per entry instead of 4).
   const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0;
+  if (fs && !packed)
+    return fail(FFB_ERR_ARG, "normalised host output without a packed transfer");
   std::vector<size_t> hdr_off, pair_off;
   std::vector<uint32_t> cap;
   size_t hdr_words = 0;
@@ -1272,7 +1306,17 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   if (!host_out)
     return FFB_OK;
   if (packed) {
-    FFB_TRY(fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off, cap));
+    FloatSink sink;
+    if (fs) {  // dense blocks are normalised into a device block before their copy
+      size_t max_words = 0;
+      for (int b = 0; b < n_blocks; ++b)
+        max_words = std::max(max_words, (size_t)(bounds[b + 1] - bounds[b]) * n_rows);
+      FFB_TRY(ensure(c, c->tmp_out2, sizeof(float) * max_words));
+      sink = *fs;
+      sink.scratch = dptr<float>(c->tmp_out2);
+    }
+    FFB_TRY(fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off, cap,
+                         fs ? &sink : nullptr));
   } else if (n_blocks == 1) {
     c->last_d2h = sizeof(uint32_t) * words;
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
@@ -1294,6 +1338,16 @@ extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, con
   }
   FFB_CUDA(cudaStreamSynchronize(c->stream));
   return FFB_OK;
+}
+
+}  // namespace
+
+extern "C" int ffb_form_factor_counts_rows(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint64_t seed,
+                                           uint32_t epoch, int flags, const int32_t* face_to_row, int n_rows,
+                                           int row_begin, int row_end, uint32_t* counts)
+{
+  return counts_rows_impl(c, front, rear, seed, epoch, flags, face_to_row, n_rows, row_begin, row_end, counts,
+                          nullptr);
 }
 
 // ===========================================================================
@@ -1410,7 +1464,7 @@ extern "C" int ffb_normalise(ffb_ctx* c, const uint32_t* counts, const int32_t* 
   FFB_TRY(upload(c, c->front_dev, outgoing, sizeof(int32_t) * (size_t)n_rows));
   FFB_TRY(output_ptr(c, ff, sizeof(float) * mat, c->tmp_out2, &d_ff, &host_out));
   k_normalise<<<grid_blocks((long long)mat, 256, c->n_sm * 16), 256, 0, c->stream>>>(
-      (const uint32_t*)d_counts, dptr<int32_t>(c->front_dev), n_rows, (float*)d_ff);
+      (const uint32_t*)d_counts, dptr<int32_t>(c->front_dev), n_rows, n_rows, (float*)d_ff);
   FFB_CUDA(cudaGetLastError());
   if (host_out) {
     FFB_TRY(finish_output(c, ff, d_ff, sizeof(float) * mat));
@@ -1428,6 +1482,19 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   if (n_rows > kMaxRows)
     return fail(FFB_ERR_TOO_LARGE, "n_rows %d above %d", n_rows, kMaxRows);
   const size_t mat = (size_t)n_rows * n_rows;
+  bool ff_dev = false;
+  FFB_TRY(ptr_kind(c, ff, &ff_dev));
+  if (!ff_dev && sizeof(float) * mat >= FFB_PIPELINE_MIN_BYTES && host_threads(c) > 0) {
+    // a large host matrix: traced in row blocks whose nonzero counts cross
+    // PCIe packed and are normalised into the rows by the host threads, with
+    // the device's operations: (float)count * (1.f / (float)outgoing[m])
+    std::vector<float> inv((size_t)n_rows);
+    for (int m = 0; m < n_rows; ++m)
+      inv[(size_t)m] = 1.f / (float)outgoing[m];
+    FFB_TRY(upload(c, c->front_dev, outgoing, sizeof(int32_t) * (size_t)n_rows));
+    FloatSink fs{ff, inv.data(), dptr<int32_t>(c->front_dev), nullptr};
+    return counts_rows_impl(c, front, rear, seed, epoch, flags, face_to_row, n_rows, 0, n_rows, nullptr, &fs);
+  }
   FFB_TRY(ensure(c, c->ff_counts, sizeof(uint32_t) * mat));
   FFB_TRY(ffb_form_factor_counts(c, front, rear, seed, epoch, flags, face_to_row, n_rows,
                                  dptr<uint32_t>(c->ff_counts)));

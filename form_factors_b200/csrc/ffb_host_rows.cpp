@@ -70,27 +70,50 @@ void worker_main(ffb_host_pool* p, int id)
 // stores, and the stored words are cleared again.  Words before the
 // destination's first 32-byte boundary are written with plain stores, so
 // the streaming stores are aligned; so is the tail after the last whole
-// vector.
+// vector.  With kNorm the row holds floats, count * inv as
+// (float)count * inv (one rounding each, the device normalisation's
+// operations); its zeros are 0.f * inv, all-zero bits unless inv is not
+// finite or negative, which rows take word by word.
 constexpr int kSeg = 4096;
 
-template <bool kAvx2>
-void expand_row(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
-                uint32_t* __restrict__ seg);
-
-template <>
-void expand_row<false>(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
-                       uint32_t* __restrict__ seg)
+inline uint32_t bits_of(float x)
 {
+  uint32_t u;
+  std::memcpy(&u, &x, sizeof u);
+  return u;
+}
+
+template <bool kNorm>
+inline uint32_t entry_bits(uint32_t count, float inv)
+{
+  return kNorm ? bits_of((float)count * inv) : count;
+}
+
+template <bool kNorm>
+void expand_row_words(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n, float inv)
+{
+  const uint32_t zero = entry_bits<kNorm>(0u, inv);
+  uint32_t k = 0;
+  for (int i = 0; i < n_cols; ++i)
+    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : zero;
+}
+
+template <bool kNorm>
+void expand_row_sse2(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
+                     uint32_t* __restrict__ seg, float inv)
+{
+  if (kNorm && entry_bits<true>(0u, inv) != 0u)
+    return expand_row_words<kNorm>(dst, n_cols, pairs, n, inv);
   uint32_t k = 0;
   int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
   head = std::min(head, n_cols);
   for (int i = 0; i < head; ++i)
-    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? pairs[2 * k++ + 1] : 0u;
+    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : 0u;
   for (int i0 = head; i0 < n_cols; i0 += kSeg) {
     const int len = std::min(kSeg, n_cols - i0);
     const uint32_t k0 = k;
     while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
-      seg[pairs[2 * k] - (uint32_t)i0] = pairs[2 * k + 1];
+      seg[pairs[2 * k] - (uint32_t)i0] = entry_bits<kNorm>(pairs[2 * k + 1], inv);
       ++k;
     }
     uint32_t* d = dst + i0;
@@ -107,21 +130,23 @@ void expand_row<false>(uint32_t* __restrict__ dst, int n_cols, const uint32_t* _
   }
 }
 
-template <>
-__attribute__((target("avx2"))) void expand_row<true>(uint32_t* __restrict__ dst, int n_cols,
-                                                      const uint32_t* __restrict__ pairs, uint32_t n,
-                                                      uint32_t* __restrict__ seg)
+template <bool kNorm>
+__attribute__((target("avx2"))) void expand_row_avx2(uint32_t* __restrict__ dst, int n_cols,
+                                                     const uint32_t* __restrict__ pairs, uint32_t n,
+                                                     uint32_t* __restrict__ seg, float inv)
 {
+  if (kNorm && entry_bits<true>(0u, inv) != 0u)
+    return expand_row_words<kNorm>(dst, n_cols, pairs, n, inv);
   uint32_t k = 0;
   int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
   head = std::min(head, n_cols);
   for (int i = 0; i < head; ++i)
-    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? pairs[2 * k++ + 1] : 0u;
+    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : 0u;
   for (int i0 = head; i0 < n_cols; i0 += kSeg) {
     const int len = std::min(kSeg, n_cols - i0);
     const uint32_t k0 = k;
     while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
-      seg[pairs[2 * k] - (uint32_t)i0] = pairs[2 * k + 1];
+      seg[pairs[2 * k] - (uint32_t)i0] = entry_bits<kNorm>(pairs[2 * k + 1], inv);
       ++k;
     }
     uint32_t* d = dst + i0;
@@ -174,21 +199,26 @@ void ffb_host_pool_destroy(ffb_host_pool* p)
 
 int ffb_host_pool_threads(const ffb_host_pool* p) { return p ? (int)p->workers.size() : 0; }
 
-void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
-                           const uint32_t* count, const uint32_t* pairs)
+namespace {
+
+// Hands rows [0, rows) to the pool; inv: one factor per row (kNorm), or null.
+template <bool kNorm>
+void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first, const uint32_t* count,
+                  const uint32_t* pairs, const float* inv)
 {
   // tasks of 8 rows: a few hundred KB of destination each
   constexpr int kRowsPerTask = 8;
   std::lock_guard<std::mutex> lk(p->mu);
-  p->task = [p, dst, rows, n_cols, first, count, pairs](int t, int w) {
+  p->task = [p, dst, rows, n_cols, first, count, pairs, inv](int t, int w) {
     uint32_t* sg = p->seg[(size_t)w];
     const int r1 = std::min(rows, (t + 1) * kRowsPerTask);
     for (int r = t * kRowsPerTask; r < r1; ++r) {
       uint32_t* d = dst + (size_t)r * (size_t)n_cols;
+      const float f = kNorm ? inv[r] : 0.f;
       if (p->avx2)
-        expand_row<true>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg);
+        expand_row_avx2<kNorm>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg, f);
       else
-        expand_row<false>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg);
+        expand_row_sse2<kNorm>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg, f);
     }
   };
   p->n_tasks = (rows + kRowsPerTask - 1) / kRowsPerTask;
@@ -196,6 +226,20 @@ void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols
   p->busy = (int)p->workers.size();
   ++p->generation;
   p->wake.notify_all();
+}
+
+}  // namespace
+
+void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
+                           const uint32_t* count, const uint32_t* pairs)
+{
+  expand_start<false>(p, dst, rows, n_cols, first, count, pairs, nullptr);
+}
+
+void ffb_host_expand_norm_start(ffb_host_pool* p, float* dst, int rows, int n_cols, const uint32_t* first,
+                                const uint32_t* count, const uint32_t* pairs, const float* inv)
+{
+  expand_start<true>(p, reinterpret_cast<uint32_t*>(dst), rows, n_cols, first, count, pairs, inv);
 }
 
 void ffb_host_expand_join(ffb_host_pool* p)

@@ -43,4 +43,8 @@ void ffb_host_pool_destroy(ffb_host_pool* p);
 int ffb_host_pool_threads(const ffb_host_pool* p);
 void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
                            const uint32_t* count, const uint32_t* pairs);
+// The same rows as floats (float)count * inv[r] -- zeros as 0.f * inv[r] --
+// for a normalised form-factor matrix (inv[r] = 1.f / (float)outgoing[r]).
+void ffb_host_expand_norm_start(ffb_host_pool* p, float* dst, int rows, int n_cols, const uint32_t* first,
+                                const uint32_t* count, const uint32_t* pairs, const float* inv);
 void ffb_host_expand_join(ffb_host_pool* p);

@@ -870,13 +870,14 @@ __global__ void k_emit(const float* __restrict__ frames, const long long* __rest
 }
 
 // Per-mesh normalisation of the counts (cpuFactorsCalculator/cpu_system.cpp
-// :193-195): ff[m][j] = (float)count[m][j] * (1.f / (float)outgoing[m]).
-__global__ void k_normalise(const uint32_t* __restrict__ counts, const int32_t* __restrict__ outgoing, int n_rows,
-                            float* __restrict__ ff)
+// :193-195): ff[m][j] = (float)count[m][j] * (1.f / (float)outgoing[m]) for
+// `rows` rows of n_cols entries (outgoing indexed from the first of them).
+__global__ void k_normalise(const uint32_t* __restrict__ counts, const int32_t* __restrict__ outgoing, int rows,
+                            int n_cols, float* __restrict__ ff)
 {
-  const size_t n = (size_t)n_rows * n_rows;
+  const size_t n = (size_t)rows * n_cols;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int m = (int)(i / n_rows);
+    const int m = (int)(i / n_cols);
     const float ratio = 1.f / (float)outgoing[m];
     ff[i] = (float)counts[i] * ratio;
   }

@@ -3,10 +3,13 @@
 // construction: random sparse rows (ascending columns, some empty, some
 // full), row widths 1..300 and a few thousand, destinations at every 4-byte
 // offset from a 64-byte boundary, 1 to 5 threads, jobs back to back on one
-// pool.  Exits non-zero on the first difference.
+// pool; counts as they are, and normalised to floats (float)count * inv with
+// finite, infinite and negative factors.  Exits non-zero on the first
+// difference (bit for bit).
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <random>
 #include <vector>
 
@@ -40,12 +43,31 @@ int main()
           }
         count[r] = (uint32_t)(pairs.size() / 2) - first[r];
       }
+      // the normalised form on every other case: one factor per row, among
+      // them the non-finite and negative ones (zeros become NaN or -0)
+      const bool norm = rep % 2 == 1;
+      std::vector<float> inv(rows);
+      if (norm) {
+        for (int r = 0; r < rows; ++r) {
+          const int pick = (int)(rng() % 8);
+          const int32_t outgoing = pick == 0 ? 0 : pick == 1 ? -3 : 1 + (int32_t)(rng() % 100000);
+          inv[r] = 1.f / (float)outgoing;
+          for (int c = 0; c < n_cols; ++c) {
+            const float v = (float)want[(size_t)r * n_cols + c] * inv[r];
+            std::memcpy(&want[(size_t)r * n_cols + c], &v, sizeof v);
+          }
+        }
+      }
       std::vector<uint32_t> mem((size_t)rows * n_cols + 64, 0xDEADBEEFu);
       uint32_t* base = mem.data();
       while ((uintptr_t)base & 63u)
         ++base;
       uint32_t* dst = base + shift;
-      ffb_host_expand_start(pool, dst, rows, n_cols, first.data(), count.data(), pairs.data());
+      if (norm)
+        ffb_host_expand_norm_start(pool, reinterpret_cast<float*>(dst), rows, n_cols, first.data(), count.data(),
+                                   pairs.data(), inv.data());
+      else
+        ffb_host_expand_start(pool, dst, rows, n_cols, first.data(), count.data(), pairs.data());
       ffb_host_expand_join(pool);
       for (size_t i = 0; i < want.size(); ++i)
         if (dst[i] != want[i]) {

@@ -137,3 +137,75 @@ def test_mesh_rows_host_output(ctx, scene):
     want = _device(ctx, front, rear, epoch=2, face_to_row=face_to_row, n_rows=m)
     got = ctx.form_factor_counts(front, rear, SEED, epoch=2, face_to_row=face_to_row, n_rows=m)
     assert np.array_equal(got, want)
+
+
+def _same_floats(got, want):
+    """Bit-identical floats, except that a NaN may have any NaN's bits (the
+    device's 0 * inf and the host's differ in sign and payload)."""
+    nan = np.isnan(want)
+    assert np.array_equal(np.isnan(got), nan)
+    assert np.array_equal(got[~nan].view(np.uint32), want[~nan].view(np.uint32))
+
+
+@pytest.mark.parametrize("threads", [-1, 0])
+def test_normalised_host_output(ctx, scene, threads):
+    """ffb_form_factors into a host float matrix: the nonzero counts cross
+    PCIe packed and host threads write (float)count * (1.f / outgoing[m]),
+    the device normalisation's operations; rows without outgoing rays are
+    0 * inf = NaN on both paths."""
+    import torch
+    n = len(scene)
+    ctx.scene_set(scene)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    front = np.full(n, 30, np.int32)
+    front[::97] = 0  # rows with no outgoing rays
+    rear = np.zeros(n, np.int32)
+    outgoing = (front + rear).astype(np.int32)
+    dev = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    ctx.form_factors(front, rear, SEED, epoch=5, outgoing=outgoing, out=dev)
+    ctx.synchronize()
+    want = dev.cpu().numpy()
+    assert np.isnan(want[0]).all() and not np.isnan(want[1]).any()
+    ctx.set_host_threads(threads)
+    try:
+        got = np.full((n, n), 7.0, np.float32)
+        ctx.form_factors(front, rear, SEED, epoch=5, outgoing=outgoing, out=got)
+        d2h = ctx.stats().d2h_bytes
+    finally:
+        ctx.set_host_threads(-1)
+    _same_floats(got, want)
+    if threads != 0:
+        assert d2h < n * n, "pairs, not the dense matrix"
+
+
+def test_normalised_host_output_dense_blocks_and_meshes(ctx, scene):
+    """Dense blocks of a normalised host output are normalised on the device
+    and copied dense; mesh rows (face_to_row) take the packed path."""
+    faces = scenes.icosphere(4, 1.0, inward=True)
+    n = len(faces)
+    ctx.scene_set(faces)
+    ctx.grid_build(cells_per_face=32, skip_empty=True)
+    front = np.full(n, 12000, np.int32)
+    rear = np.zeros(n, np.int32)
+    want = ctx.form_factors(front, rear, SEED, epoch=1, out=_device_floats(n))
+    ctx.synchronize()
+    got = ctx.form_factors(front, rear, SEED, epoch=1)
+    _same_floats(got, want.cpu().numpy())
+    assert ctx.stats().d2h_bytes >= 4 * n * n
+    n = len(scene)
+    ctx.scene_set(scene)
+    ctx.grid_build(cells_per_face=64, skip_empty=True)
+    rng = np.random.default_rng(9)
+    m = 4300
+    face_to_row = rng.integers(0, m, n).astype(np.int32)
+    front = np.full(n, 25, np.int32)
+    rear = np.full(n, 3, np.int32)
+    want = ctx.form_factors(front, rear, SEED, epoch=3, face_to_row=face_to_row, n_rows=m, out=_device_floats(m))
+    ctx.synchronize()
+    got = ctx.form_factors(front, rear, SEED, epoch=3, face_to_row=face_to_row, n_rows=m)
+    _same_floats(got, want.cpu().numpy())
+
+
+def _device_floats(n):
+    import torch
+    return torch.empty((n, n), dtype=torch.float32, device="cuda")
