@@ -213,6 +213,13 @@ void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const u
     uint32_t* sg = p->seg[(size_t)w];
     const int r1 = std::min(rows, (t + 1) * kRowsPerTask);
     for (int r = t * kRowsPerTask; r < r1; ++r) {
+      // the next row's pairs lie elsewhere (rows reserve their pairs in any
+      // order): fetch them into the cache while this row is written
+      if (r + 1 < rows) {
+        const char* q = reinterpret_cast<const char*>(pairs + 2 * (size_t)first[r + 1]);
+        for (size_t b = 0; b < 8 * (size_t)count[r + 1]; b += 64)
+          _mm_prefetch(q + b, _MM_HINT_T0);
+      }
       uint32_t* d = dst + (size_t)r * (size_t)n_cols;
       const float f = kNorm ? inv[r] : 0.f;
       if (p->avx2)
