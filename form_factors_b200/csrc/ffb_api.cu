@@ -1167,9 +1167,15 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
     const size_t want = (sizeof(uint32_t) * words + FFB_PIPELINE_BLOCK_BYTES - 1) / FFB_PIPELINE_BLOCK_BYTES;
     n_blocks = (int)std::min<size_t>(std::max<size_t>(want, 2), (size_t)std::min(kMaxPipeBlocks, span));
   }
+  // Equal blocks, except that the first of several has half the rows (when
+  // every block keeps one): the host's side of a pipelined output starts
+  // once it is done.
   std::vector<int> bounds(n_blocks + 1);
+  const bool half_first = n_blocks > 1 && span >= 2 * n_blocks;
   for (int b = 0; b <= n_blocks; ++b)
-    bounds[b] = row_begin + (int)((long long)span * b / n_blocks);
+    bounds[b] = b == 0 ? row_begin
+                : half_first ? row_begin + (int)((long long)span * (2 * b - 1) / (2 * n_blocks - 1))
+                             : row_begin + (int)((long long)span * b / n_blocks);
   // the chunks of each block, block after block; faces outside
   // [row_begin, row_end) do not emit
   std::vector<int> face_block(s.n_faces, -1);
@@ -1287,7 +1293,7 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
       else
         FFB_TRY((launch_fused<false>(c, p, false, st)));
     }
-    if (packed) {
+    if (packed && bounds[b + 1] > bounds[b]) {
       const int rows = bounds[b + 1] - bounds[b];
       k_rows_pack<<<std::min(rows, c->n_sm * 8), kPackThreads, 0, st>>>(
           (const uint32_t*)d_counts + off, rows, n_rows, dptr<uint32_t>(c->pack_hdr) + hdr_off[b], cap[b],
