@@ -1059,8 +1059,9 @@ struct FloatSink {
 
 int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int n_rows, const uint32_t* d_counts,
                  uint32_t* counts, const std::vector<size_t>& hdr_off, const std::vector<size_t>& pair_off,
-                 const std::vector<uint32_t>& cap, const FloatSink* fs)
+                 const std::vector<uint32_t>& cap, bool narrow, const FloatSink* fs)
 {
+  const size_t pair_bytes = narrow ? sizeof(uint32_t) : sizeof(uint2);
   const int n_blocks = (int)bounds.size() - 1;
   std::vector<char> dense((size_t)n_blocks, 0);
   auto fetch = [&](int b) -> int {
@@ -1087,9 +1088,9 @@ int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int 
                                c->copy_stream));
       c->last_d2h += sizeof(uint32_t) * n_words;
     } else if (total > 0) {
-      FFB_CUDA(cudaMemcpyAsync(c->pack_stage[b & 1], dptr<uint2>(c->pack_pairs) + pair_off[b],
-                               sizeof(uint2) * (size_t)total, cudaMemcpyDeviceToHost, c->copy_stream));
-      c->last_d2h += sizeof(uint2) * (size_t)total;
+      FFB_CUDA(cudaMemcpyAsync(c->pack_stage[b & 1], dptr<unsigned char>(c->pack_pairs) + pair_bytes * pair_off[b],
+                               pair_bytes * (size_t)total, cudaMemcpyDeviceToHost, c->copy_stream));
+      c->last_d2h += pair_bytes * (size_t)total;
     }
     FFB_CUDA(cudaEventRecord(c->block_copied[b], c->copy_stream));
     return FFB_OK;
@@ -1102,9 +1103,10 @@ int fetch_packed(ffb_ctx* c, const std::vector<int>& bounds, int row_begin, int 
     const size_t off = (size_t)(bounds[b] - row_begin) * n_rows;
     if (!dense[b] && fs)
       ffb_host_expand_norm_start(c->host_pool, fs->ff + off, rows, n_rows, h + 2, h + 2 + rows, c->pack_stage[b & 1],
-                                 fs->inv + bounds[b]);
+                                 narrow, fs->inv + bounds[b]);
     else if (!dense[b])
-      ffb_host_expand_start(c->host_pool, counts + off, rows, n_rows, h + 2, h + 2 + rows, c->pack_stage[b & 1]);
+      ffb_host_expand_start(c->host_pool, counts + off, rows, n_rows, h + 2, h + 2 + rows, c->pack_stage[b & 1],
+                            narrow);
     // the next block's pairs go to the other stage, which block b - 1 used
     const int rc = b + 1 < n_blocks ? fetch(b + 1) : FFB_OK;
     if (!dense[b])
@@ -1216,6 +1218,22 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
   const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0;
   if (fs && !packed)
     return fail(FFB_ERR_ARG, "normalised host output without a packed transfer");
+  // One word per pair (column | count << 16) when no column and no count
+  // reaches 2^16: a count is at most its row's rays.
+  bool narrow = false;
+  if (packed && n_rows <= 65536) {
+    std::vector<long long> row_rays(face_to_row ? (size_t)n_rows : 0, 0);
+    long long most = 0;
+    for (int f = 0; f < s.n_faces; ++f) {
+      const long long r = (long long)front[f] + rear[f];
+      if (face_to_row)
+        most = std::max(most, row_rays[(size_t)face_to_row[f]] += r);
+      else
+        most = std::max(most, r);
+    }
+    narrow = most < 65536;
+  }
+  const size_t pair_bytes = narrow ? sizeof(uint32_t) : sizeof(uint2);
   std::vector<size_t> hdr_off, pair_off;
   std::vector<uint32_t> cap;
   size_t hdr_words = 0;
@@ -1233,7 +1251,7 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
       max_cap = std::max<size_t>(max_cap, cap.back());
     }
     FFB_TRY(ensure(c, c->pack_hdr, sizeof(uint32_t) * hw));
-    FFB_TRY(ensure(c, c->pack_pairs, sizeof(uint2) * std::max<size_t>(pw, 1)));
+    FFB_TRY(ensure(c, c->pack_pairs, pair_bytes * std::max<size_t>(pw, 1)));
     FFB_TRY(ensure_pinned(&c->pack_hdr_host, &c->pack_hdr_host_cap, sizeof(uint32_t) * hw));
     size_t stage_cap = c->pack_stage_cap;
     for (uint32_t*& st : c->pack_stage) {
@@ -1295,9 +1313,9 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
     }
     if (packed && bounds[b + 1] > bounds[b]) {
       const int rows = bounds[b + 1] - bounds[b];
-      k_rows_pack<<<std::min(rows, c->n_sm * 8), kPackThreads, 0, st>>>(
+      (narrow ? k_rows_pack<true> : k_rows_pack<false>)<<<std::min(rows, c->n_sm * 8), kPackThreads, 0, st>>>(
           (const uint32_t*)d_counts + off, rows, n_rows, dptr<uint32_t>(c->pack_hdr) + hdr_off[b], cap[b],
-          dptr<uint2>(c->pack_pairs) + pair_off[b]);
+          dptr<unsigned char>(c->pack_pairs) + pair_bytes * pair_off[b]);
       FFB_CUDA(cudaGetLastError());
     }
     if (n_blocks > 1)
@@ -1322,7 +1340,7 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
       sink.scratch = dptr<float>(c->tmp_out2);
     }
     FFB_TRY(fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off, cap,
-                         fs ? &sink : nullptr));
+                         narrow, fs ? &sink : nullptr));
   } else if (n_blocks == 1) {
     c->last_d2h = sizeof(uint32_t) * words;
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));

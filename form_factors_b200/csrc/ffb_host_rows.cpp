@@ -89,31 +89,44 @@ inline uint32_t entry_bits(uint32_t count, float inv)
   return kNorm ? bits_of((float)count * inv) : count;
 }
 
-template <bool kNorm>
+// Pair k of a row: two words (column, count), or with kNarrow one word
+// column | count << 16.
+template <bool kNarrow>
+inline uint32_t pair_col(const uint32_t* pairs, uint32_t k)
+{
+  return kNarrow ? pairs[k] & 0xFFFFu : pairs[2 * k];
+}
+template <bool kNarrow>
+inline uint32_t pair_val(const uint32_t* pairs, uint32_t k)
+{
+  return kNarrow ? pairs[k] >> 16 : pairs[2 * k + 1];
+}
+
+template <bool kNorm, bool kNarrow>
 void expand_row_words(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n, float inv)
 {
   const uint32_t zero = entry_bits<kNorm>(0u, inv);
   uint32_t k = 0;
   for (int i = 0; i < n_cols; ++i)
-    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : zero;
+    dst[i] = (k < n && pair_col<kNarrow>(pairs, k) == (uint32_t)i) ? entry_bits<kNorm>(pair_val<kNarrow>(pairs, k++), inv) : zero;
 }
 
-template <bool kNorm>
+template <bool kNorm, bool kNarrow>
 void expand_row_sse2(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __restrict__ pairs, uint32_t n,
                      uint32_t* __restrict__ seg, float inv)
 {
   if (kNorm && entry_bits<true>(0u, inv) != 0u)
-    return expand_row_words<kNorm>(dst, n_cols, pairs, n, inv);
+    return expand_row_words<kNorm, kNarrow>(dst, n_cols, pairs, n, inv);
   uint32_t k = 0;
   int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
   head = std::min(head, n_cols);
   for (int i = 0; i < head; ++i)
-    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : 0u;
+    dst[i] = (k < n && pair_col<kNarrow>(pairs, k) == (uint32_t)i) ? entry_bits<kNorm>(pair_val<kNarrow>(pairs, k++), inv) : 0u;
   for (int i0 = head; i0 < n_cols; i0 += kSeg) {
     const int len = std::min(kSeg, n_cols - i0);
     const uint32_t k0 = k;
-    while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
-      seg[pairs[2 * k] - (uint32_t)i0] = entry_bits<kNorm>(pairs[2 * k + 1], inv);
+    while (k < n && pair_col<kNarrow>(pairs, k) < (uint32_t)(i0 + len)) {
+      seg[pair_col<kNarrow>(pairs, k) - (uint32_t)i0] = entry_bits<kNorm>(pair_val<kNarrow>(pairs, k), inv);
       ++k;
     }
     uint32_t* d = dst + i0;
@@ -126,27 +139,27 @@ void expand_row_sse2(uint32_t* __restrict__ dst, int n_cols, const uint32_t* __r
     for (; j < len; ++j)
       d[j] = seg[j];
     for (uint32_t q = k0; q < k; ++q)
-      seg[pairs[2 * q] - (uint32_t)i0] = 0u;
+      seg[pair_col<kNarrow>(pairs, q) - (uint32_t)i0] = 0u;
   }
 }
 
-template <bool kNorm>
+template <bool kNorm, bool kNarrow>
 __attribute__((target("avx2"))) void expand_row_avx2(uint32_t* __restrict__ dst, int n_cols,
                                                      const uint32_t* __restrict__ pairs, uint32_t n,
                                                      uint32_t* __restrict__ seg, float inv)
 {
   if (kNorm && entry_bits<true>(0u, inv) != 0u)
-    return expand_row_words<kNorm>(dst, n_cols, pairs, n, inv);
+    return expand_row_words<kNorm, kNarrow>(dst, n_cols, pairs, n, inv);
   uint32_t k = 0;
   int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
   head = std::min(head, n_cols);
   for (int i = 0; i < head; ++i)
-    dst[i] = (k < n && pairs[2 * k] == (uint32_t)i) ? entry_bits<kNorm>(pairs[2 * k++ + 1], inv) : 0u;
+    dst[i] = (k < n && pair_col<kNarrow>(pairs, k) == (uint32_t)i) ? entry_bits<kNorm>(pair_val<kNarrow>(pairs, k++), inv) : 0u;
   for (int i0 = head; i0 < n_cols; i0 += kSeg) {
     const int len = std::min(kSeg, n_cols - i0);
     const uint32_t k0 = k;
-    while (k < n && pairs[2 * k] < (uint32_t)(i0 + len)) {
-      seg[pairs[2 * k] - (uint32_t)i0] = entry_bits<kNorm>(pairs[2 * k + 1], inv);
+    while (k < n && pair_col<kNarrow>(pairs, k) < (uint32_t)(i0 + len)) {
+      seg[pair_col<kNarrow>(pairs, k) - (uint32_t)i0] = entry_bits<kNorm>(pair_val<kNarrow>(pairs, k), inv);
       ++k;
     }
     uint32_t* d = dst + i0;
@@ -160,7 +173,7 @@ __attribute__((target("avx2"))) void expand_row_avx2(uint32_t* __restrict__ dst,
     for (; j < len; ++j)
       d[j] = seg[j];
     for (uint32_t q = k0; q < k; ++q)
-      seg[pairs[2 * q] - (uint32_t)i0] = 0u;
+      seg[pair_col<kNarrow>(pairs, q) - (uint32_t)i0] = 0u;
   }
 }
 
@@ -202,12 +215,13 @@ int ffb_host_pool_threads(const ffb_host_pool* p) { return p ? (int)p->workers.s
 namespace {
 
 // Hands rows [0, rows) to the pool; inv: one factor per row (kNorm), or null.
-template <bool kNorm>
+template <bool kNorm, bool kNarrow>
 void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first, const uint32_t* count,
                   const uint32_t* pairs, const float* inv)
 {
   // tasks of 8 rows: a few hundred KB of destination each
   constexpr int kRowsPerTask = 8;
+  constexpr size_t kWords = kNarrow ? 1 : 2;  // words per pair
   std::lock_guard<std::mutex> lk(p->mu);
   p->task = [p, dst, rows, n_cols, first, count, pairs, inv](int t, int w) {
     uint32_t* sg = p->seg[(size_t)w];
@@ -216,16 +230,17 @@ void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const u
       // the next row's pairs lie elsewhere (rows reserve their pairs in any
       // order): fetch them into the cache while this row is written
       if (r + 1 < rows) {
-        const char* q = reinterpret_cast<const char*>(pairs + 2 * (size_t)first[r + 1]);
-        for (size_t b = 0; b < 8 * (size_t)count[r + 1]; b += 64)
+        const char* q = reinterpret_cast<const char*>(pairs + kWords * first[r + 1]);
+        for (size_t b = 0; b < 4 * kWords * count[r + 1]; b += 64)
           _mm_prefetch(q + b, _MM_HINT_T0);
       }
       uint32_t* d = dst + (size_t)r * (size_t)n_cols;
       const float f = kNorm ? inv[r] : 0.f;
+      const uint32_t* pr = pairs + kWords * first[r];
       if (p->avx2)
-        expand_row_avx2<kNorm>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg, f);
+        expand_row_avx2<kNorm, kNarrow>(d, n_cols, pr, count[r], sg, f);
       else
-        expand_row_sse2<kNorm>(d, n_cols, pairs + 2 * (size_t)first[r], count[r], sg, f);
+        expand_row_sse2<kNorm, kNarrow>(d, n_cols, pr, count[r], sg, f);
     }
   };
   p->n_tasks = (rows + kRowsPerTask - 1) / kRowsPerTask;
@@ -238,15 +253,22 @@ void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const u
 }  // namespace
 
 void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
-                           const uint32_t* count, const uint32_t* pairs)
+                           const uint32_t* count, const uint32_t* pairs, int narrow)
 {
-  expand_start<false>(p, dst, rows, n_cols, first, count, pairs, nullptr);
+  if (narrow)
+    expand_start<false, true>(p, dst, rows, n_cols, first, count, pairs, nullptr);
+  else
+    expand_start<false, false>(p, dst, rows, n_cols, first, count, pairs, nullptr);
 }
 
 void ffb_host_expand_norm_start(ffb_host_pool* p, float* dst, int rows, int n_cols, const uint32_t* first,
-                                const uint32_t* count, const uint32_t* pairs, const float* inv)
+                                const uint32_t* count, const uint32_t* pairs, int narrow, const float* inv)
 {
-  expand_start<true>(p, reinterpret_cast<uint32_t*>(dst), rows, n_cols, first, count, pairs, inv);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  if (narrow)
+    expand_start<true, true>(p, d, rows, n_cols, first, count, pairs, inv);
+  else
+    expand_start<true, false>(p, d, rows, n_cols, first, count, pairs, inv);
 }
 
 void ffb_host_expand_join(ffb_host_pool* p)

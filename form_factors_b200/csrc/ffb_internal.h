@@ -32,19 +32,21 @@ int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long*
 // Host threads that write count-matrix rows into a host buffer from the
 // (column, count) pairs of their nonzero entries (ffb_host_rows.cpp).
 // ffb_host_expand_start hands rows [0, rows) to the pool and returns: row r
-// of the n_cols-wide uint32 matrix at dst gets the count[r] pairs at
-// pairs + 2 * first[r] (column, count; columns ascending and below n_cols)
-// and zeros elsewhere; every entry of the rows is written.  ffb_host_expand_join waits until the rows are
-// written (and their streaming stores are visible).  One job at a time per
-// pool; the buffers must stay valid until the join.
+// of the n_cols-wide uint32 matrix at dst gets the count[r] pairs from pair
+// first[r] on (columns ascending and below n_cols) and zeros elsewhere;
+// every entry of the rows is written.  A pair is two words (column, count),
+// or with `narrow` one word column | count << 16.  ffb_host_expand_join
+// waits until the rows are written (and their streaming stores are
+// visible).  One job at a time per pool; the buffers must stay valid until
+// the join.
 struct ffb_host_pool;
 ffb_host_pool* ffb_host_pool_create(int threads);
 void ffb_host_pool_destroy(ffb_host_pool* p);
 int ffb_host_pool_threads(const ffb_host_pool* p);
 void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
-                           const uint32_t* count, const uint32_t* pairs);
+                           const uint32_t* count, const uint32_t* pairs, int narrow);
 // The same rows as floats (float)count * inv[r] -- zeros as 0.f * inv[r] --
 // for a normalised form-factor matrix (inv[r] = 1.f / (float)outgoing[r]).
 void ffb_host_expand_norm_start(ffb_host_pool* p, float* dst, int rows, int n_cols, const uint32_t* first,
-                                const uint32_t* count, const uint32_t* pairs, const float* inv);
+                                const uint32_t* count, const uint32_t* pairs, int narrow, const float* inv);
 void ffb_host_expand_join(ffb_host_pool* p);

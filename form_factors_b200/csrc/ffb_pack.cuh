@@ -14,6 +14,17 @@ __host__ __device__ constexpr size_t pack_header_words(int rows) { return 2 + 2 
 
 constexpr int kPackThreads = 256;
 
+// A pair is two words (column, count), or with kNarrow one word
+// column | count << 16, when columns and counts are below 2^16.
+template <bool kNarrow>
+__device__ __forceinline__ void pack_pair_store(void* pairs, uint32_t k, uint32_t col, uint32_t v)
+{
+  if (kNarrow)
+    static_cast<uint32_t*>(pairs)[k] = col | (v << 16);
+  else
+    static_cast<uint2*>(pairs)[k] = make_uint2(col, v);
+}
+
 // One CTA per row (grid-stride over rows).  Pass 1 counts the row's nonzero
 // entries (16-byte loads when the row is 16-byte aligned), one atomic on
 // hdr[0] reserves that many pairs, and (first, count) goes to the header.
@@ -23,9 +34,10 @@ constexpr int kPackThreads = 256;
 // column order.  A row whose pairs would pass `cap` writes none: the host
 // sees hdr[0] > cap and copies the block dense.  hdr[0] is zero before the
 // launch.
+template <bool kNarrow>
 __global__ void __launch_bounds__(kPackThreads) k_rows_pack(const uint32_t* __restrict__ counts, int rows,
                                                             int n_cols, uint32_t* __restrict__ hdr, uint32_t cap,
-                                                            uint2* __restrict__ pairs)
+                                                            void* __restrict__ pairs)
 {
   constexpr int kWarps = kPackThreads / 32;
   constexpr uint32_t kSkip = 0xFFFFFFFFu;
@@ -93,7 +105,7 @@ __global__ void __launch_bounds__(kPackThreads) k_rows_pack(const uint32_t* __re
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (v[j] != 0u)
-            pairs[q++] = make_uint2((uint32_t)(i0 + j), v[j]);
+            pack_pair_store<kNarrow>(pairs, q++, (uint32_t)(i0 + j), v[j]);
         pos += tile;
       }
     }

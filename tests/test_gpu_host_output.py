@@ -38,14 +38,18 @@ def scene():
     return faces
 
 
-@pytest.mark.parametrize("threads", [-1, 1, 3, 0])
-def test_packed_output_equals_device_output(ctx, scene, threads):
+@pytest.mark.parametrize("threads,wide", [(-1, False), (1, False), (3, False), (0, False), (-1, True)])
+def test_packed_output_equals_device_output(ctx, scene, threads, wide):
+    """wide: one row emits 70 000 rays, so a count may pass 2^16 and pairs
+    take two words (column, count) instead of one."""
     import torch
     n = len(scene)
     assert 4 * n * n >= 64 << 20
     ctx.scene_set(scene)
     ctx.grid_build(cells_per_face=64, skip_empty=True)
     front = np.full(n, 30, np.int32)
+    if wide:
+        front[17] = 70000
     rear = np.zeros(n, np.int32)
     want = _device(ctx, front, rear, epoch=4)
     assert want.any()
@@ -64,7 +68,8 @@ def test_packed_output_equals_device_output(ctx, scene, threads):
         assert d2h == 4 * n * n
     else:
         nnz = int(np.count_nonzero(want))
-        assert 8 * nnz < d2h < 8 * nnz + 16 * n + 4096, "pairs plus block headers"
+        pair = 8 if wide else 4
+        assert pair * nnz < d2h < pair * nnz + 16 * n + 4096, "pairs plus block headers"
 
 
 def test_unaligned_destination_and_odd_width(ctx):
