@@ -434,6 +434,14 @@ def batched_section(ctx, stream, args):
     torch.cuda.empty_cache()
     # plain through the reference-facing call: a host float matrix per scene
     host = torch.empty(int(sizes.max()) ** 2, dtype=torch.float32, pin_memory=True)
+    # warm-up: the eight largest scenes once, untimed, so that the call's
+    # scratch buffers have reached their sizes before the timed pass
+    for i in np.argsort(sizes)[-8:]:
+        n = len(sl[i])
+        ctx.scene_set(sl[i])
+        grid(i)
+        ctx.form_factors(fronts[i], rears[i], int(seeds[i]), epoch=1, n_rows=n,
+                         out=host[:n * n].numpy().reshape(n, n))
     t0 = time.perf_counter()
     for i, f in enumerate(sl):
         n = len(f)

@@ -1022,17 +1022,42 @@ extern "C" int ffb_emit(ffb_ctx* c, const int32_t* front, const int32_t* rear, u
 
 namespace {
 
+// Whether rows [row_begin, row_end) of the count matrix are sparse enough
+// for the packed transfer: a row holds at most min(its rays, n_rows)
+// nonzero entries, and the bound summed over the rows must fit the pair
+// caps (a quarter of the entries).  Denser matrices go dense as a whole.
+bool face_rows_ok(int n_faces, const int32_t* face_to_row, int n_rows)
+{
+  for (int f = 0; f < n_faces; ++f)
+    if (face_to_row[f] < 0 || face_to_row[f] >= n_rows)
+      return false;
+  return true;
+}
+
+bool sparse_enough(int n_faces, const int32_t* front, const int32_t* rear, const int32_t* face_to_row, int n_rows,
+                   int row_begin, int row_end)
+{
+  std::vector<long long> rays((size_t)n_rows, 0);
+  for (int f = 0; f < n_faces; ++f)
+    rays[(size_t)(face_to_row ? face_to_row[f] : f)] += (long long)front[f] + rear[f];
+  long long bound = 0;
+  for (int r = row_begin; r < row_end; ++r)
+    bound += std::min<long long>(rays[(size_t)r], n_rows);
+  return bound <= (long long)(row_end - row_begin) * n_rows / 4;
+}
+
 // Pinned host memory of at least `bytes` in *p (capacity *cap), kept and
-// grown by doubling.
+// grown by doubling (page-locking costs tens of ms per hundred MB, so a
+// run of growing requests must not pay it each time).
 int ensure_pinned(uint32_t** p, size_t* cap, size_t bytes)
 {
   if (bytes <= *cap)
     return FFB_OK;
+  const size_t want = std::max(std::max(bytes, 2 * *cap), (size_t)8 << 20);
   if (*p)
     cudaFreeHost(*p);
   *p = nullptr;
   *cap = 0;
-  const size_t want = std::max(bytes, (size_t)8 << 20);
   FFB_CUDA(cudaMallocHost((void**)p, want));
   *cap = want;
   return FFB_OK;
@@ -1215,7 +1240,8 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
   // A pipelined host output moves as (column, count) pairs when host threads
   // are enabled: per block a header (pack_header_words) and at most a
   // quarter of its entries as pairs (2 bytes per entry instead of 4).
-  const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0;
+  const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0 &&
+                      sparse_enough(s.n_faces, front, rear, face_to_row, n_rows, row_begin, row_end);
   if (fs && !packed)
     return fail(FFB_ERR_ARG, "normalised host output without a packed transfer");
   // One word per pair (column | count << 16) when no column and no count
@@ -1253,10 +1279,14 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
     FFB_TRY(ensure(c, c->pack_hdr, sizeof(uint32_t) * hw));
     FFB_TRY(ensure(c, c->pack_pairs, pair_bytes * std::max<size_t>(pw, 1)));
     FFB_TRY(ensure_pinned(&c->pack_hdr_host, &c->pack_hdr_host_cap, sizeof(uint32_t) * hw));
+    // both stages hold a block's pairs; sized at once for blocks of up to
+    // FFB_PIPELINE_BLOCK_BYTES (the blocks of every matrix below 16 of them)
+    const size_t stage_bytes = std::max(pair_bytes * std::max<size_t>(max_cap, 1),
+                                        (size_t)FFB_PIPELINE_BLOCK_BYTES / 2);
     size_t stage_cap = c->pack_stage_cap;
     for (uint32_t*& st : c->pack_stage) {
       stage_cap = c->pack_stage_cap;  // both stages have the same capacity
-      FFB_TRY(ensure_pinned(&st, &stage_cap, sizeof(uint2) * std::max<size_t>(max_cap, 1)));
+      FFB_TRY(ensure_pinned(&st, &stage_cap, stage_bytes));
     }
     c->pack_stage_cap = stage_cap;
     if (!c->host_pool || ffb_host_pool_threads(c->host_pool) != host_threads(c)) {
@@ -1508,7 +1538,9 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   const size_t mat = (size_t)n_rows * n_rows;
   bool ff_dev = false;
   FFB_TRY(ptr_kind(c, ff, &ff_dev));
-  if (!ff_dev && sizeof(float) * mat >= FFB_PIPELINE_MIN_BYTES && host_threads(c) > 0) {
+  if (!ff_dev && sizeof(float) * mat >= FFB_PIPELINE_MIN_BYTES && host_threads(c) > 0 && c->main.n_faces > 0 &&
+      front && rear && (!face_to_row || face_rows_ok(c->main.n_faces, face_to_row, n_rows)) &&
+      sparse_enough(c->main.n_faces, front, rear, face_to_row, n_rows, 0, n_rows)) {
     // a large host matrix: traced in row blocks whose nonzero counts cross
     // PCIe packed and are normalised into the rows by the host threads, with
     // the device's operations: (float)count * (1.f / (float)outgoing[m])

@@ -112,10 +112,10 @@ def test_blocks_without_emitters_and_row_ranges(ctx, scene):
     assert np.array_equal(part, want[700:])
 
 
-def test_dense_blocks_fall_back_to_dense_copies(ctx):
-    """A small closed scene traced with many rays per face fills most of its
-    entries: its blocks exceed the pair cap and are copied dense, and the
-    result is unchanged."""
+def test_dense_matrices_and_dense_blocks(ctx):
+    """A matrix whose rays could fill more than a quarter of its entries is
+    copied dense as a whole; when only some rows are dense, a block whose
+    pairs pass its cap is copied dense and the others come packed."""
     faces = scenes.icosphere(4, 1.0, inward=True)  # 5120 faces, 105 MB matrix
     n = len(faces)
     ctx.scene_set(faces)
@@ -123,10 +123,19 @@ def test_dense_blocks_fall_back_to_dense_copies(ctx):
     front = np.full(n, 12000, np.int32)
     rear = np.zeros(n, np.int32)
     want = _device(ctx, front, rear, epoch=1)
-    assert np.count_nonzero(want) > n * n / 4, "dense enough to pass the cap"
+    assert np.count_nonzero(want) > n * n / 4
     got = ctx.form_factor_counts(front, rear, SEED, epoch=1)
     assert np.array_equal(got, want)
-    assert ctx.stats().d2h_bytes >= 4 * n * n
+    assert ctx.stats().d2h_bytes == 4 * n * n
+    # 1000 dense rows: within the global bound, but the first block (1 706
+    # rows, half-size) holds them all and passes its own cap
+    front[:] = 0
+    front[:1000] = 12000
+    want = _device(ctx, front, rear, epoch=2)
+    got = ctx.form_factor_counts(front, rear, SEED, epoch=2)
+    assert np.array_equal(got, want)
+    d2h = ctx.stats().d2h_bytes
+    assert 4 * 1706 * n <= d2h < 4 * 1706 * n + 16 * n + 4096, "block 0 dense, block 1 empty pairs"
 
 
 def test_mesh_rows_host_output(ctx, scene):
@@ -184,19 +193,23 @@ def test_normalised_host_output(ctx, scene, threads):
 
 
 def test_normalised_host_output_dense_blocks_and_meshes(ctx, scene):
-    """Dense blocks of a normalised host output are normalised on the device
-    and copied dense; mesh rows (face_to_row) take the packed path."""
+    """A block of a normalised host output whose pairs pass its cap is
+    normalised on the device and copied dense; mesh rows (face_to_row) take
+    the packed path."""
     faces = scenes.icosphere(4, 1.0, inward=True)
     n = len(faces)
     ctx.scene_set(faces)
     ctx.grid_build(cells_per_face=32, skip_empty=True)
-    front = np.full(n, 12000, np.int32)
+    front = np.zeros(n, np.int32)
+    front[:1000] = 12000
+    front[3000:] = 40
     rear = np.zeros(n, np.int32)
     want = ctx.form_factors(front, rear, SEED, epoch=1, out=_device_floats(n))
     ctx.synchronize()
     got = ctx.form_factors(front, rear, SEED, epoch=1)
     _same_floats(got, want.cpu().numpy())
-    assert ctx.stats().d2h_bytes >= 4 * n * n
+    d2h = ctx.stats().d2h_bytes
+    assert 4 * 1706 * n <= d2h < 4 * n * n, "block 0 (1 706 rows) dense, block 1 as pairs"
     n = len(scene)
     ctx.scene_set(scene)
     ctx.grid_build(cells_per_face=64, skip_empty=True)
