@@ -72,6 +72,8 @@ def parse():
                          "(a small command for profiling the grid-build kernels)")
     ap.add_argument("--served-requests", type=int, default=256)
     ap.add_argument("--served-slots", type=int, default=16, help="requests prepared and traced at once")
+    ap.add_argument("--served-slice-rays", type=int, default=0,
+                    help="rays per trace slice of the serving loop (0: the library default, 64 Mi)")
     ap.add_argument("--served-max-wait", type=float, default=30.0,
                     help="age limit of the shortest-first served run, s (0: skip that run)")
     ap.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
@@ -503,6 +505,8 @@ def served_section(args, ctx, stream):
 
     def served(slots, arrivals, reqs, shortest_first=False):
         server = native.Server(0, budget_bytes=int(80e9), slots=slots)
+        if args.served_slice_rays > 0:
+            server.set_slicing(args.served_slice_rays)
         if shortest_first:
             server.set_admission(shortest_first=True, max_wait_s=args.served_max_wait)
         t0 = time.perf_counter()
