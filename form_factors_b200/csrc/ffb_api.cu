@@ -1026,6 +1026,17 @@ namespace {
 // for the packed transfer: a row holds at most min(its rays, n_rows)
 // nonzero entries, and the bound summed over the rows must fit the pair
 // caps (a quarter of the entries).  Denser matrices go dense as a whole.
+// The context's host threads, started (or restarted with a new count) on
+// first use; false when they cannot be started.
+bool ensure_host_pool(ffb_ctx* c)
+{
+  if (c->host_pool && ffb_host_pool_threads(c->host_pool) == host_threads(c))
+    return true;
+  ffb_host_pool_destroy(c->host_pool);
+  c->host_pool = ffb_host_pool_create(host_threads(c));
+  return c->host_pool != nullptr;
+}
+
 bool face_rows_ok(int n_faces, const int32_t* face_to_row, int n_rows)
 {
   for (int f = 0; f < n_faces; ++f)
@@ -1240,8 +1251,9 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
   // A pipelined host output moves as (column, count) pairs when host threads
   // are enabled: per block a header (pack_header_words) and at most a
   // quarter of its entries as pairs (2 bytes per entry instead of 4).
-  const bool packed = host_out && n_blocks > 1 && host_threads(c) > 0 &&
-                      sparse_enough(s.n_faces, front, rear, face_to_row, n_rows, row_begin, row_end);
+  bool packed = host_out && n_blocks > 1 && host_threads(c) > 0 &&
+                sparse_enough(s.n_faces, front, rear, face_to_row, n_rows, row_begin, row_end);
+  packed = packed && ensure_host_pool(c);  // without host threads the blocks are copied dense
   if (fs && !packed)
     return fail(FFB_ERR_ARG, "normalised host output without a packed transfer");
   // One word per pair (column | count << 16) when no column and no count
@@ -1289,10 +1301,6 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
       FFB_TRY(ensure_pinned(&st, &stage_cap, stage_bytes));
     }
     c->pack_stage_cap = stage_cap;
-    if (!c->host_pool || ffb_host_pool_threads(c->host_pool) != host_threads(c)) {
-      ffb_host_pool_destroy(c->host_pool);
-      c->host_pool = ffb_host_pool_create(host_threads(c));
-    }
   }
   TraceParams p;
   p.frames = dptr<float>(c->frames);
@@ -1369,8 +1377,14 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
       sink = *fs;
       sink.scratch = dptr<float>(c->tmp_out2);
     }
-    FFB_TRY(fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off, cap,
-                         narrow, fs ? &sink : nullptr));
+    const int rc = fetch_packed(c, bounds, row_begin, n_rows, (const uint32_t*)d_counts, counts, hdr_off, pair_off,
+                                cap, narrow, fs ? &sink : nullptr);
+    if (rc != FFB_OK) {  // nothing may still write into the caller's buffer once the call returns
+      cudaStreamSynchronize(c->copy_stream);
+      cudaStreamSynchronize(c->stream);
+      cudaGetLastError();
+      return rc;
+    }
   } else if (n_blocks == 1) {
     c->last_d2h = sizeof(uint32_t) * words;
     FFB_TRY(finish_output(c, counts, d_counts, sizeof(uint32_t) * words));
@@ -1540,7 +1554,7 @@ extern "C" int ffb_form_factors(ffb_ctx* c, const int32_t* front, const int32_t*
   FFB_TRY(ptr_kind(c, ff, &ff_dev));
   if (!ff_dev && sizeof(float) * mat >= FFB_PIPELINE_MIN_BYTES && host_threads(c) > 0 && c->main.n_faces > 0 &&
       front && rear && (!face_to_row || face_rows_ok(c->main.n_faces, face_to_row, n_rows)) &&
-      sparse_enough(c->main.n_faces, front, rear, face_to_row, n_rows, 0, n_rows)) {
+      sparse_enough(c->main.n_faces, front, rear, face_to_row, n_rows, 0, n_rows) && ensure_host_pool(c)) {
     // a large host matrix: traced in row blocks whose nonzero counts cross
     // PCIe packed and are normalised into the rows by the host threads, with
     // the device's operations: (float)count * (1.f / (float)outgoing[m])

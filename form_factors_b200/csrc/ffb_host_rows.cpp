@@ -20,6 +20,7 @@
 #include <cstring>
 #include <functional>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -181,16 +182,27 @@ __attribute__((target("avx2"))) void expand_row_avx2(uint32_t* __restrict__ dst,
 
 ffb_host_pool* ffb_host_pool_create(int threads)
 {
-  ffb_host_pool* p = new ffb_host_pool;
+  ffb_host_pool* p = new (std::nothrow) ffb_host_pool;
+  if (!p)
+    return nullptr;
   threads = std::max(threads, 1);
   p->avx2 = __builtin_cpu_supports("avx2");
   for (int i = 0; i < threads; ++i) {
     uint32_t* sg = static_cast<uint32_t*>(std::aligned_alloc(64, sizeof(uint32_t) * kSeg));
+    if (!sg) {
+      ffb_host_pool_destroy(p);
+      return nullptr;
+    }
     std::memset(sg, 0, sizeof(uint32_t) * kSeg);
     p->seg.push_back(sg);
   }
-  for (int i = 0; i < threads; ++i)
-    p->workers.emplace_back(worker_main, p, i);
+  try {
+    for (int i = 0; i < threads; ++i)
+      p->workers.emplace_back(worker_main, p, i);
+  } catch (...) {  // no more threads: the threads started so far are stopped
+    ffb_host_pool_destroy(p);
+    return nullptr;
+  }
   return p;
 }
 

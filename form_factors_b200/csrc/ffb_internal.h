@@ -40,7 +40,7 @@ int ffb_trace_span(ffb_ctx* c, unsigned long long* start_ns, unsigned long long*
 // visible).  One job at a time per pool; the buffers must stay valid until
 // the join.
 struct ffb_host_pool;
-ffb_host_pool* ffb_host_pool_create(int threads);
+ffb_host_pool* ffb_host_pool_create(int threads);  // null when threads or memory run out
 void ffb_host_pool_destroy(ffb_host_pool* p);
 int ffb_host_pool_threads(const ffb_host_pool* p);
 void ffb_host_expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const uint32_t* first,
