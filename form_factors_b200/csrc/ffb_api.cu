@@ -133,6 +133,7 @@ struct ffb_ctx {
   DevBuf csv_tile_len, csv_tile_off, csv_text;  // CSV formatting
   DevBuf power_tab, absorb;                     // radiance sink
   DevBuf span;                                  // sliced traces: earliest start / latest end (globaltimer ns)
+  DevBuf live_count;                            // grid build: faces with a non-empty binning box
   TraceParams slice_params{};                   // sliced traces: the prepared launch
   bool slice_ready = false;
   long long slice_chunks = 0;
@@ -519,9 +520,17 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
                                           s.n_faces, dptr<uint32_t>(s.cell_fill));
   FFB_CUDA(cudaGetLastError());
   FFB_TRY(scan(c, dptr<uint32_t>(s.cell_fill), (int)n_cells, dptr<uint32_t>(s.cell_start)));
-  uint32_t total = 0;
+  // the live faces (non-empty binning boxes), counted on the device and read
+  // with the reference total
+  FFB_TRY(ensure(c, c->live_count, sizeof(uint32_t)));
+  FFB_CUDA(cudaMemsetAsync(c->live_count.ptr, 0, sizeof(uint32_t), c->stream));
+  k_count_live<<<grid_blocks(s.n_faces, 256), 256, 0, c->stream>>>(dptr<float4>(s.box_lo), dptr<float4>(s.box_hi),
+                                                                  s.n_faces, dptr<uint32_t>(c->live_count));
+  FFB_CUDA(cudaGetLastError());
+  uint32_t total = 0, live = 0;
   FFB_CUDA(cudaMemcpyAsync(&total, dptr<uint32_t>(s.cell_start) + n_cells, sizeof total, cudaMemcpyDeviceToHost,
                            c->stream));
+  FFB_CUDA(cudaMemcpyAsync(&live, c->live_count.ptr, sizeof live, cudaMemcpyDeviceToHost, c->stream));
   FFB_CUDA(cudaStreamSynchronize(c->stream));
   if (total >= kCellEmpty)  // reference offsets must stay below the empty-cell flag
     return fail(FFB_ERR_TOO_LARGE, "%u grid references; at most %u", total, kCellEmpty - 1);
@@ -552,32 +561,11 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
       dptr<uint32_t>(s.cell_start), I.skip_empty ? dptr<uint8_t>(s.empty_dist) : nullptr, n_cells,
       dptr<uint2>(s.cell_rec));
   FFB_CUDA(cudaGetLastError());
-  // live faces: those with a non-empty binning box
   I.n_refs = total;
-  I.n_live_faces = 0;
-  {
-    std::vector<float4> lo((size_t)s.n_faces), hi((size_t)s.n_faces);
-    FFB_CUDA(cudaMemcpyAsync(lo.data(), s.box_lo.ptr, sizeof(float4) * lo.size(), cudaMemcpyDeviceToHost,
-                             c->stream));
-    FFB_CUDA(cudaMemcpyAsync(hi.data(), s.box_hi.ptr, sizeof(float4) * hi.size(), cudaMemcpyDeviceToHost,
-                             c->stream));
-    FFB_CUDA(cudaStreamSynchronize(c->stream));
-    for (int f = 0; f < s.n_faces; ++f)
-      I.n_live_faces += lo[f].x <= hi[f].x;
-  }
+  I.n_live_faces = (int)live;
   s.info = I;
   s.grid_ok = true;
   return FFB_OK;
-}
-
-// Appends the chunks of face rays [0, front + rear) of every face.
-void add_chunks(std::vector<Chunk>& out, const int32_t* front, const int32_t* rear, int n_faces)
-{
-  for (int f = 0; f < n_faces; ++f) {
-    const int nf = front[f] + rear[f];
-    for (int j0 = 0; j0 < nf; j0 += kChunkRays)
-      out.push_back(Chunk{f, j0, std::min(kChunkRays, nf - j0), front[f]});
-  }
 }
 
 // Chunk table of the emitting faces `faces` (in launch order) built on the
@@ -743,7 +731,7 @@ extern "C" void ffb_ctx_destroy(ffb_ctx* c)
                     &c->scan_sums, &c->chunks,      &c->chunk_src,    &c->rows,         &c->cursor,     &c->stats,
                     &c->tmp_in,   &c->tmp_out,      &c->tmp_out2,     &c->offsets,    &c->front_dev,
                     &c->ray_cursor, &c->ff_counts, &c->csv_tile_len, &c->csv_tile_off, &c->csv_text,
-                    &c->power_tab, &c->absorb, &c->span, &c->pack_hdr, &c->pack_pairs, &c->obj_text,
+                    &c->power_tab, &c->absorb, &c->span, &c->live_count, &c->pack_hdr, &c->pack_pairs, &c->obj_text,
                     &c->obj_chunk, &c->obj_chunk_off,
                     &c->obj_starts, &c->obj_flags, &c->obj_ords, &c->obj_vertices, &c->obj_face_idx,
                     &c->obj_face_line, &c->obj_special, &c->obj_ranges, &c->obj_faces, &c->obj_err};
@@ -2346,18 +2334,38 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
   const long long n_all = c->batch_offsets[n_scenes];
   long long total = 0;
   FFB_TRY(check_counts((int)n_all, front, rear, &total));
-  std::vector<Chunk> chunks;
-  chunks.reserve((size_t)(total / kChunkRays + n_all));
+  // The chunk table, scene after scene, written on the device from one
+  // 16-byte record per emitting face (scene-local face, front rays, rays,
+  // first chunk): the host's work and upload are linear in faces, not rays.
+  std::vector<int4> src;
+  src.reserve((size_t)n_all);
   c->batch_chunk_first.assign(n_scenes + 1, 0);
+  long long next = 0;
   for (int s = 0; s < n_scenes; ++s) {
     const long long f0 = c->batch_offsets[s];
-    c->batch_chunk_first[s] = (int)chunks.size();
-    add_chunks(chunks, front + f0, rear + f0, c->batch[s].n_faces);
+    c->batch_chunk_first[s] = (int)next;
+    for (int f = 0; f < c->batch[s].n_faces; ++f) {
+      const long long nf = (long long)front[f0 + f] + rear[f0 + f];
+      if (nf == 0)
+        continue;
+      if (nf > INT_MAX - kChunkRays)
+        return fail(FFB_ERR_TOO_LARGE, "scene %d face %d emits %lld rays; at most %d", s, f, nf,
+                    INT_MAX - kChunkRays);
+      src.push_back(make_int4(f, front[f0 + f], (int)nf, (int)next));
+      next += (nf + kChunkRays - 1) / kChunkRays;
+      if (next > INT_MAX)
+        return fail(FFB_ERR_TOO_LARGE, "more than %d work chunks", INT_MAX);
+    }
   }
-  c->batch_chunk_first[n_scenes] = (int)chunks.size();
-  c->batch_n_chunks = (int)chunks.size();
-  if (!chunks.empty())
-    FFB_TRY(upload(c, c->batch_chunks, chunks.data(), sizeof(Chunk) * chunks.size()));
+  c->batch_chunk_first[n_scenes] = (int)next;
+  c->batch_n_chunks = (int)next;
+  if (next > 0) {
+    FFB_TRY(ensure(c, c->batch_chunks, sizeof(Chunk) * (size_t)next));
+    FFB_TRY(upload(c, c->chunk_src, src.data(), sizeof(int4) * src.size()));
+    k_chunk_fill<kChunkRays><<<grid_blocks((long long)src.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+        dptr<int4>(c->chunk_src), (int)src.size(), dptr<Chunk>(c->batch_chunks));
+    FFB_CUDA(cudaGetLastError());
+  }
   std::vector<uint2> keys((size_t)n_scenes);
   for (int s = 0; s < n_scenes; ++s) {
     const uint64_t k = seeds ? seeds[s] : 1;

@@ -264,6 +264,18 @@ __global__ void k_grid_fill(BinGeom g, const float* __restrict__ faces9, const f
   });
 }
 
+// Counts the faces with a non-empty binning box (the grid's live faces):
+// one atomic per warp.
+__global__ void k_count_live(const float4* __restrict__ box_lo, const float4* __restrict__ box_hi, int n_faces,
+                             uint32_t* __restrict__ live)
+{
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = f < n_faces && box_lo[f].x <= box_hi[f].x;
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
+  if ((threadIdx.x & 31) == 0 && m)
+    atomicAdd(live, (uint32_t)__popc(m));
+}
+
 // Sorts each cell's references by triangle index (insertion sort, one thread
 // per cell): the grid is then a deterministic function of the scene.
 __global__ void k_cell_sort(const uint32_t* __restrict__ cell_start, int n_cells, int32_t* __restrict__ ref_tri)
