@@ -38,6 +38,7 @@ struct ffb_host_pool {
   std::atomic<int> next{0};
   std::vector<uint32_t*> seg;  // one zeroed 64-byte aligned scratch segment per worker
   bool avx2 = false;
+  bool avx512 = false;
 };
 
 namespace {
@@ -178,6 +179,43 @@ __attribute__((target("avx2"))) void expand_row_avx2(uint32_t* __restrict__ dst,
   }
 }
 
+template <bool kNorm, bool kNarrow>
+__attribute__((target("avx512f"))) void expand_row_avx512(uint32_t* __restrict__ dst, int n_cols,
+                                                     const uint32_t* __restrict__ pairs, uint32_t n,
+                                                     uint32_t* __restrict__ seg, float inv)
+{
+  if (kNorm && entry_bits<true>(0u, inv) != 0u)
+    return expand_row_words<kNorm, kNarrow>(dst, n_cols, pairs, n, inv);
+  uint32_t k = 0;
+  int head = (int)(((32u - ((uint32_t)(uintptr_t)dst & 31u)) & 31u) >> 2);
+  head = std::min(head, n_cols);
+  for (int i = 0; i < head; ++i)
+    dst[i] = (k < n && pair_col<kNarrow>(pairs, k) == (uint32_t)i) ? entry_bits<kNorm>(pair_val<kNarrow>(pairs, k++), inv) : 0u;
+  for (int i0 = head; i0 < n_cols; i0 += kSeg) {
+    const int len = std::min(kSeg, n_cols - i0);
+    const uint32_t k0 = k;
+    while (k < n && pair_col<kNarrow>(pairs, k) < (uint32_t)(i0 + len)) {
+      seg[pair_col<kNarrow>(pairs, k) - (uint32_t)i0] = entry_bits<kNorm>(pair_val<kNarrow>(pairs, k), inv);
+      ++k;
+    }
+    uint32_t* d = dst + i0;
+    int j = 0;
+    // 64-byte stores from a 32-byte boundary: one 32-byte store first when
+    // the destination is not 64-byte aligned
+    if (j + 8 <= len && ((uintptr_t)(d + j) & 63u) != 0) {
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(d + j),
+                          _mm256_load_si256(reinterpret_cast<const __m256i*>(seg + j)));
+      j += 8;
+    }
+    for (; j + 16 <= len; j += 16)
+      _mm512_stream_si512(reinterpret_cast<__m512i*>(d + j), _mm512_loadu_si512(seg + j));
+    for (; j < len; ++j)
+      d[j] = seg[j];
+    for (uint32_t q = k0; q < k; ++q)
+      seg[pair_col<kNarrow>(pairs, q) - (uint32_t)i0] = 0u;
+  }
+}
+
 }  // namespace
 
 ffb_host_pool* ffb_host_pool_create(int threads)
@@ -187,6 +225,7 @@ ffb_host_pool* ffb_host_pool_create(int threads)
     return nullptr;
   threads = std::max(threads, 1);
   p->avx2 = __builtin_cpu_supports("avx2");
+  p->avx512 = p->avx2 && __builtin_cpu_supports("avx512f");
   for (int i = 0; i < threads; ++i) {
     uint32_t* sg = static_cast<uint32_t*>(std::aligned_alloc(64, sizeof(uint32_t) * kSeg));
     if (!sg) {
@@ -249,7 +288,9 @@ void expand_start(ffb_host_pool* p, uint32_t* dst, int rows, int n_cols, const u
       uint32_t* d = dst + (size_t)r * (size_t)n_cols;
       const float f = kNorm ? inv[r] : 0.f;
       const uint32_t* pr = pairs + kWords * first[r];
-      if (p->avx2)
+      if (p->avx512)
+        expand_row_avx512<kNorm, kNarrow>(d, n_cols, pr, count[r], sg, f);
+      else if (p->avx2)
         expand_row_avx2<kNorm, kNarrow>(d, n_cols, pr, count[r], sg, f);
       else
         expand_row_sse2<kNorm, kNarrow>(d, n_cols, pr, count[r], sg, f);
