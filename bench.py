@@ -995,6 +995,9 @@ def ours(args):
 
     # end to end through the C ABI with host buffers
     host_counts = torch.empty(rows * n, dtype=torch.int32, pin_memory=True)
+    if world > 1:  # ranks on one node share its cores between their host threads
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        ctx.set_host_threads(max(1, min(12, cores // world)))
     e2e_steps = max(2, min(args.steps, 5))
     step(20_000, out=host_counts)
     torch.cuda.synchronize()
@@ -1014,7 +1017,7 @@ def ours(args):
     for i in range(e2e_steps):
         step(20_001 + i, out=host_counts)
     e2e_dense_s = (time.perf_counter() - t0) / e2e_steps
-    ctx.set_host_threads(-1)
+    ctx.set_host_threads(host_threads)
     t = torch.tensor([e2e_s, e2e_dense_s], device="cuda")
     d2h_t = torch.tensor([d2h_rank], dtype=torch.float64, device="cuda")
     if world > 1:
