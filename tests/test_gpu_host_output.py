@@ -227,3 +227,20 @@ def test_normalised_host_output_dense_blocks_and_meshes(ctx, scene):
 def _device_floats(n):
     import torch
     return torch.empty((n, n), dtype=torch.float32, device="cuda")
+
+
+def test_host_threads_setting(ctx):
+    """-1 is the default (min(12, hardware threads)), 0 to 256 are taken as
+    given, anything else is refused with FFB_ERR_ARG."""
+    import os
+    from form_factors_b200 import native
+    assert ctx.host_threads() == min(12, os.cpu_count())
+    for n in (0, 1, 256):
+        ctx.set_host_threads(n)
+        assert ctx.host_threads() == n
+    for bad in (-2, 257):
+        with pytest.raises(native.FFBError) as err:
+            ctx.set_host_threads(bad)
+        assert err.value.code == -301
+    ctx.set_host_threads(-1)
+    assert ctx.host_threads() == min(12, os.cpu_count())
