@@ -573,28 +573,50 @@ int grid_build(ffb_ctx* c, SceneData& s, const ffb_grid_params* params)
 // not in rays) and uploads 16 bytes per face; k_chunk_fill writes the
 // chunks.  first[i] gets the first chunk of faces[i], *n_chunks the total.
 int device_chunks(ffb_ctx* c, const std::vector<int32_t>& faces, const int32_t* front, const int32_t* rear,
-                  std::vector<long long>& first, long long* n_chunks)
+                  std::vector<long long>& first, long long* n_chunks, bool short_tail = false)
 {
-  std::vector<int4> src(faces.size());
+  // With short_tail, the faces that hold the last sixteenth of the rays get
+  // chunks of kTailRays: the launch's last chunks are short, so its warps
+  // run out of work closer together (a 256-ray chunk takes a warp about as
+  // long as 1/18 of a full-GPU launch).
+  constexpr int kTailRays = 64;
+  long long tail_from = LLONG_MAX;
+  if (short_tail) {
+    long long all = 0;
+    for (const int f : faces)
+      all += (long long)front[f] + rear[f];
+    tail_from = all - all / 16;
+  }
+  std::vector<int4> head, tail;
+  head.reserve(faces.size());
   first.resize(faces.size());
-  long long next = 0;
+  long long next = 0, rays = 0;
   for (size_t i = 0; i < faces.size(); ++i) {
     const int f = faces[i];
     const long long nf = (long long)front[f] + rear[f];
     if (nf > INT_MAX - kChunkRays)
       return fail(FFB_ERR_TOO_LARGE, "face %d emits %lld rays; at most %d", f, nf, INT_MAX - kChunkRays);
+    const int size = rays >= tail_from ? kTailRays : kChunkRays;
     first[i] = next;
-    src[i] = make_int4(f, front[f], (int)nf, (int)next);
-    next += (nf + kChunkRays - 1) / kChunkRays;
+    (size == kChunkRays ? head : tail).push_back(make_int4(f, front[f], (int)nf, (int)next));
+    next += (nf + size - 1) / size;
+    rays += nf;
     if (next > INT_MAX)
       return fail(FFB_ERR_TOO_LARGE, "more than %d work chunks", INT_MAX);
   }
   *n_chunks = next;
   if (next > 0) {
     FFB_TRY(ensure(c, c->chunks, sizeof(Chunk) * (size_t)next));
-    FFB_TRY(upload(c, c->chunk_src, src.data(), sizeof(int4) * src.size()));
-    k_chunk_fill<kChunkRays><<<grid_blocks((long long)src.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
-        dptr<int4>(c->chunk_src), (int)src.size(), dptr<Chunk>(c->chunks));
+    // one staged upload: the head's records, then the tail's
+    const size_t nh = head.size();
+    head.insert(head.end(), tail.begin(), tail.end());
+    FFB_TRY(upload(c, c->chunk_src, head.data(), sizeof(int4) * head.size()));
+    if (nh)
+      k_chunk_fill<kChunkRays><<<grid_blocks((long long)nh * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+          dptr<int4>(c->chunk_src), (int)nh, dptr<Chunk>(c->chunks));
+    if (!tail.empty())
+      k_chunk_fill<kTailRays><<<grid_blocks((long long)tail.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+          dptr<int4>(c->chunk_src) + nh, (int)tail.size(), dptr<Chunk>(c->chunks));
     FFB_CUDA(cudaGetLastError());
   }
   return FFB_OK;
@@ -1225,7 +1247,7 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
   block_pos[n_blocks] = order.size();
   std::vector<long long> face_first;
   long long n_chunks = 0;
-  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks));
+  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks, n_blocks == 1));
   std::vector<int> first(n_blocks + 1, 0);
   for (int b = 0; b <= n_blocks; ++b)
     first[b] = (int)(block_pos[b] < order.size() ? face_first[block_pos[b]] : n_chunks);
