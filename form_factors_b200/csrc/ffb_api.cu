@@ -1625,7 +1625,7 @@ extern "C" int ffb_radiance_absorption(ffb_ctx* c, const int32_t* front, const i
       order.push_back(f);
   std::vector<long long> face_first;
   long long n_chunks = 0;
-  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks));
+  FFB_TRY(device_chunks(c, order, front, rear, face_first, &n_chunks, true));
   FFB_TRY(ensure(c, c->absorb, sizeof(unsigned long long) * (size_t)n_meshes));
   FFB_CUDA(cudaMemsetAsync(c->absorb.ptr, 0, sizeof(unsigned long long) * (size_t)n_meshes, c->stream));
   FFB_TRY(ensure(c, c->stats, sizeof(unsigned long long) * kStatSlots));
