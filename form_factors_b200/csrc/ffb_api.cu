@@ -2359,13 +2359,20 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
   // The chunk table, scene after scene, written on the device from one
   // 16-byte record per emitting face (scene-local face, front rays, rays,
   // first chunk): the host's work and upload are linear in faces, not rays.
-  std::vector<int4> src;
+  // As in a single-scene launch, the faces holding the last sixteenth of a
+  // scene's rays get 64-ray chunks (its launch's tail is shorter).
+  constexpr int kTailRays = 64;
+  std::vector<int4> src, tail;
   src.reserve((size_t)n_all);
   c->batch_chunk_first.assign(n_scenes + 1, 0);
   long long next = 0;
   for (int s = 0; s < n_scenes; ++s) {
     const long long f0 = c->batch_offsets[s];
     c->batch_chunk_first[s] = (int)next;
+    long long all = 0, rays = 0;
+    for (int f = 0; f < c->batch[s].n_faces; ++f)
+      all += (long long)front[f0 + f] + rear[f0 + f];
+    const long long tail_from = all - all / 16;
     for (int f = 0; f < c->batch[s].n_faces; ++f) {
       const long long nf = (long long)front[f0 + f] + rear[f0 + f];
       if (nf == 0)
@@ -2373,8 +2380,10 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
       if (nf > INT_MAX - kChunkRays)
         return fail(FFB_ERR_TOO_LARGE, "scene %d face %d emits %lld rays; at most %d", s, f, nf,
                     INT_MAX - kChunkRays);
-      src.push_back(make_int4(f, front[f0 + f], (int)nf, (int)next));
-      next += (nf + kChunkRays - 1) / kChunkRays;
+      const int size = rays >= tail_from ? kTailRays : kChunkRays;
+      (size == kChunkRays ? src : tail).push_back(make_int4(f, front[f0 + f], (int)nf, (int)next));
+      next += (nf + size - 1) / size;
+      rays += nf;
       if (next > INT_MAX)
         return fail(FFB_ERR_TOO_LARGE, "more than %d work chunks", INT_MAX);
     }
@@ -2383,9 +2392,15 @@ extern "C" int ffb_batch_prepare(ffb_ctx* c, const int32_t* front, const int32_t
   c->batch_n_chunks = (int)next;
   if (next > 0) {
     FFB_TRY(ensure(c, c->batch_chunks, sizeof(Chunk) * (size_t)next));
+    const size_t nh = src.size();
+    src.insert(src.end(), tail.begin(), tail.end());  // one staged upload
     FFB_TRY(upload(c, c->chunk_src, src.data(), sizeof(int4) * src.size()));
-    k_chunk_fill<kChunkRays><<<grid_blocks((long long)src.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
-        dptr<int4>(c->chunk_src), (int)src.size(), dptr<Chunk>(c->batch_chunks));
+    if (nh)
+      k_chunk_fill<kChunkRays><<<grid_blocks((long long)nh * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+          dptr<int4>(c->chunk_src), (int)nh, dptr<Chunk>(c->batch_chunks));
+    if (!tail.empty())
+      k_chunk_fill<kTailRays><<<grid_blocks((long long)tail.size() * 32, 256, c->n_sm * 8), 256, 0, c->stream>>>(
+          dptr<int4>(c->chunk_src) + nh, (int)tail.size(), dptr<Chunk>(c->batch_chunks));
     FFB_CUDA(cudaGetLastError());
   }
   std::vector<uint2> keys((size_t)n_scenes);
