@@ -1259,8 +1259,9 @@ int counts_rows_impl(ffb_ctx* c, const int32_t* front, const int32_t* rear, uint
   if (n_blocks > 1)
     FFB_TRY(ensure_pipeline(c));
   // A pipelined host output moves as (column, count) pairs when host threads
-  // are enabled: per block a header (pack_header_words) and at most a
-  // quarter of its entries as pairs (2 bytes per entry instead of 4).
+  // are enabled and the rows are sparse enough: per block a header
+  // (pack_header_words) and at most a quarter of its entries as pairs (at
+  // most 1 or 2 bytes per entry with one- or two-word pairs, against 4).
   bool packed = host_out && n_blocks > 1 && host_threads(c) > 0 &&
                 sparse_enough(s.n_faces, front, rear, face_to_row, n_rows, row_begin, row_end);
   packed = packed && ensure_host_pool(c);  // without host threads the blocks are copied dense
