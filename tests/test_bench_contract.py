@@ -61,3 +61,35 @@ def test_hbm_peak_names_its_source():
     gbs, source = bench.hbm_peak()
     assert gbs > 0 and source in ("measured", "fallback")
     assert source == ("measured" if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else "fallback")
+
+
+def test_clock_sampler_with_a_fake_nvml():
+    """The timed region's clock record from NVML (read-only queries): the
+    sampler polls every 2 ms, takes the median of the loaded samples, and
+    names the clock-event reasons from their bits."""
+    import time
+
+    class FakeNvml:
+        NVML_CLOCK_SM = 1
+        calls = 0
+
+        def nvmlDeviceGetClockInfo(self, h, kind):
+            FakeNvml.calls += 1
+            return 1965 if FakeNvml.calls % 4 else 1800
+
+        def nvmlDeviceGetMaxClockInfo(self, h, kind):
+            return 1965
+
+        def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+            return 0x4 if FakeNvml.calls > 6 else 0x0  # sw_power_cap from the seventh sample on
+
+    clk = bench.Clocks(0)
+    clk._nvml_handle = lambda: (FakeNvml(), object())
+    clk.start()
+    assert clk.thread is not None
+    time.sleep(0.06)
+    rec = clk.stop()
+    assert rec["samples"] >= 10
+    assert rec["sm_mhz"] == 1965.0 and rec["sm_max_mhz"] == 1965.0 and rec["sm_min_mhz"] == 1800.0
+    assert rec["reasons"] == ["sw_power_cap"]
+    assert rec["source"].startswith("nvml")
